@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark of the LOD diffusion-decay step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 256^3 voxels x 8 substrates, dt = 0.01 min, dx = 20 um, D and
+lambda log-uniform in [1e2, 1e5] / [1e-3, 1] (seeded), U[0,1) field, no
+Dirichlet, no agents -- the configuration the FP32 >= 70 % HBM-roofline
+target is quoted on. Metric: voxel*substrate updates per second per LOD step
+(V*S*K / t). A "step" is one full LOD step (x, y and z Thomas sweeps with the
+fused Dirichlet), replayed from a CUDA graph. The 537 MB FP32 field is larger
+than the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: the path does not shard (one grid per GPU); N ranks run N
+independent replicas ("replicas only"), timed with CUDA events and reduced as
+the max over ranks. `--impl reference` times the reference's own CPU solver
+(oracle/_ref, compiled from the reference sources) on rank 0.
+
+One JSON line is printed by rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+NX = NY = NZ = 256
+S = 8
+DT = 0.01
+DX = 20.0
+SEED = 2026
+METRIC = "voxel*substrate updates/s per LOD step (256^3 voxels x 8 substrates)"
+UNIT = "voxel*substrate updates/s"
+
+
+def load_bfb():
+    pkg = ROOT / "biofvm-b_b200"
+    spec = importlib.util.spec_from_file_location("biofvm_b_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["biofvm_b_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def coefficients():
+    rng = np.random.default_rng(SEED)
+    D = np.exp(rng.uniform(np.log(1e2), np.log(1e5), S))
+    lam = np.exp(rng.uniform(np.log(1e-3), np.log(1.0), S))
+    return D, lam, rng
+
+
+def initial_field(rng):
+    return rng.random((NX, NY, NZ, S))
+
+
+def config(extra=None):
+    c = {"workload": f"LOD diffusion-decay step, {NX}^3 voxels x {S} substrates, dt={DT}, dx={DX}, "
+                     "no Dirichlet, no agents",
+         "grid": [NX, NY, NZ], "substrates": S, "dt": DT,
+         "l2": "inputs larger than L2 (field 537 MB FP32 / 1074 MB FP64 > 126 MB)",
+         "parallelism": "replicas only (one grid per GPU)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(",") for r in Path(self.path).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        j = json.loads(p.read_text())
+        return float(j["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, STREAM-style copy)"
+    return 6650.0, "fallback (6.65 TB/s)"
+
+
+def ncu_traffic(kernel_key):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    j = json.loads(p.read_text())
+    v = j.get(kernel_key)
+    return None if v is None else float(v)
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (test infrastructure under oracle/, used only here)
+# ---------------------------------------------------------------------------
+def cpu_reference_run(max_seconds, min_steps=1, steps=None):
+    """Time the reference's own CPU solver (oracle/_ref) on the workload.
+    Returns (updates/s, steps timed, threads, solver name)."""
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import REF_SO, RefEnv, RefLib
+    if not REF_SO.exists():
+        return None
+    ref = RefLib()
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    ref.lib.ref_set_threads(threads)
+    D, lam, rng = coefficients()
+    rho0 = initial_field(rng)
+    best = None
+    for solver, name in ((0, "LOD_3D"), (1, "LOD_3D_AVX256D")):
+        e = RefEnv(ref, (0, 0, 0, NX * DX, NY * DX, NZ * DX), DX, D, lam)
+        e.set_field(rho0)
+        e.set_dirichlet([0] * S)
+        e.set_solver(solver)
+        e.step(DT, 1)  # first call computes the Thomas factors; not timed
+        t0 = time.perf_counter()
+        n = 0
+        while True:
+            e.step(DT, 1)
+            n += 1
+            el = time.perf_counter() - t0
+            if steps is not None and n >= steps:
+                break
+            if max_seconds is not None and n >= min_steps and el >= max_seconds:
+                break
+        rate = NX * NY * NZ * S * n / el
+        e.close()
+        del e
+        if best is None or rate > best[0]:
+            best = (rate, n, threads, name, el)
+    return best
+
+
+def cpu_port_run(max_seconds):
+    """Fallback when the reference is not built: our oracle port, 1 thread,
+    on a 64^3 x 8 sample of the workload."""
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import Oracle
+    o = Oracle()
+    D, lam, rng = coefficients()
+    rho = rng.random((64, 64, 64, S))
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        rho = o.lod_steps(rho, DT, DX, D, lam, 1)
+        n += 1
+        if time.perf_counter() - t0 >= max_seconds:
+            break
+    el = time.perf_counter() - t0
+    return 64 ** 3 * S * n / el, n
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    warm = max(args.warmup, 1)
+    # each solver: one untimed factor-setup step, then up to K steps or
+    # args.ref_seconds of timing, whichever comes first (a bounded sample)
+    r = cpu_reference_run(args.ref_seconds, min_steps=1, steps=args.steps)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built "
+                          "(it is compiled from the reference sources by `make -C oracle ref`)"}))
+        return 0
+    rate, n, threads, name, el = r
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": warm, "ms_per_step": el / n * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded U[0,1) field, log-uniform D/lambda)",
+        "config": config({"solver": name, "threads": threads, "ranks": "1 rank x N threads (MPI unavailable)"}),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{n} of the {args.steps} requested full 256^3x8 FP64 steps (capped at "
+                                   f"{args.ref_seconds:.0f} s) after 1 factor-setup step, best of LOD_3D / AVX256D"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_our_arm(args):
+    import torch
+    rank, world, local = dist_setup(args)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    bfb = load_bfb()
+    warm = max(args.warmup, 3)
+    K = args.steps
+    V = NX * NY * NZ
+    D, lam, rng = coefficients()
+    rho0 = initial_field(rng)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    stream = torch.cuda.Stream()
+    for prec, name in ((bfb.FP32, "fp32"), (bfb.FP64, "fp64")):
+        env = bfb.Env((NX, NY, NZ), S, dx=DX, precision=prec, device=local)
+        env.set_coefficients(D, lam)
+        env.set_field(rho0)
+        env.set_stream(stream.cuda_stream)
+        env.simulate(DT, warm, bfb.STEP_DIFFUSION)
+        barrier()
+        clocks = Clocks(local)
+        if name == "fp32":
+            clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        env.simulate(DT, K, bfb.STEP_DIFFUSION)
+        e1.record(stream)
+        e1.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        clk = clocks.stop() if name == "fp32" else None
+        barrier()
+        # per-kernel device time (events around every launch, same stream)
+        prof = env.profile_steps(DT, min(K, 50), bfb.STEP_DIFFUSION)
+        nprof = min(K, 50)
+        results[name] = dict(ms=ms, clocks=clk, prof=prof, nprof=nprof, env=env, elem=4 if prec == bfb.FP32 else 8)
+        if name == "fp64":
+            env.close()
+
+    # end to end through the C ABI with reference-facing host buffers
+    env = results["fp32"]["env"]
+    host = torch.from_numpy(rho0.reshape(-1).copy()).pin_memory()
+    K_e2e = max(1, min(K, 20))
+    env.step_host_ptr(host.data_ptr(), DT, 1)  # warm
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K_e2e):
+        env.step_host_ptr(host.data_ptr(), DT, 1)
+    e1.record(stream)
+    e1.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    env.close()
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    r32, r64 = results["fp32"], results["fp64"]
+    value = world * V * S * K / (r32["ms"] / 1e3)
+    value64 = world * V * S * K / (r64["ms"] / 1e3)
+    peak, peak_src = measured_peak()
+    phases = ["sweep_x", "sweep_y", "sweep_z"]
+    per = r32["prof"][:3] / r32["nprof"]  # ms per launch
+    dom = int(np.argmax(per))
+    bytes_launch = 2.0 * V * S * 4  # one read + one write of the field
+    achieved = bytes_launch / (per[dom] / 1e3) / 1e9
+    step_bytes = 6.0 * V * S * 4
+    ms_step = r32["ms"] / K
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_run(args.cpu_seconds, min_steps=1)
+        if r is not None:
+            rate, n, threads, sname, el = r
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{n} full 256^3x8 FP64 steps ({el:.1f} s) of the reference {sname} "
+                             "(faster of LOD_3D / AVX256D), after one factor-setup step"}
+        else:
+            rate, n = cpu_port_run(args.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"{n} steps of a 64^3x8 sample with the oracle port (reference not built)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warm,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded U[0,1) field, log-uniform D/lambda)",
+        "config": config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": ncu_traffic(f"fp32_{phases[dom]}"), "kernel": phases[dom],
+                     "algorithmic_bytes_per_launch": bytes_launch, "peak_source": peak_src,
+                     "ms_per_launch": float(per[dom])},
+        "step_roofline": {"achieved": step_bytes / (ms_step / 1e3) / 1e9, "frac": step_bytes / (ms_step / 1e3) / 1e9 / peak,
+                          "algorithmic_bytes_per_step": step_bytes},
+        "kernel_ms_per_launch": {p: float(x) for p, x in zip(phases, per)},
+        "fp64": {"value": value64, "ms_per_step": r64["ms"] / K,
+                 "step_roofline_frac": 6.0 * V * S * 8 / (r64["ms"] / K / 1e3) / 1e9 / peak,
+                 "kernel_ms_per_launch": {p: float(x) for p, x in zip(phases, r64["prof"][:3] / r64["nprof"])}},
+        "fp32_over_fp64": value / value64,
+        "clocks": r32["clocks"],
+        "e2e": {"value": world * V * S * K_e2e / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": V * S * 8,
+                "d2h_bytes_per_step": V * S * 8, "steps": K_e2e,
+                "path": "bfb_step_host: pinned FP64 host field -> device (FP32) -> 1 LOD step -> host"},
+        "gpu_launches": 3 * K,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=60.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,275 @@
+"""Python binding of the B200 BioFVM-B diffusion-decay library (C ABI over ctypes).
+
+The product is the C ABI in include/biofvm_b200.h, implemented by
+lib/libbiofvm_b200.so (CUDA, sm_100a). This module only loads that library
+and wraps its calls; there is no CPU fallback: if the library is missing or
+no CUDA device is present, every call raises.
+
+The package directory is named ``biofvm-b_b200`` and is imported by path:
+
+    import importlib.util, sys
+    spec = importlib.util.spec_from_file_location(
+        "biofvm_b_b200", "biofvm-b_b200/__init__.py",
+        submodule_search_locations=["biofvm-b_b200"])
+    bfb = importlib.util.module_from_spec(spec); sys.modules["biofvm_b_b200"] = bfb
+    spec.loader.exec_module(bfb)
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libbiofvm_b200.so"
+
+FP64 = 0
+FP32 = 1
+STEP_BULK = 1
+STEP_DIFFUSION = 2
+STEP_CELLS = 4
+OPT_FREEZE_FACTORS = 1
+OPT_USE_GRAPHS = 2
+
+ERRORS = {
+    -1: "BFB_ERR_INVALID_ARG",
+    -2: "BFB_ERR_SIZE",
+    -3: "BFB_ERR_OOM",
+    -4: "BFB_ERR_CUDA",
+    -5: "BFB_ERR_STATE",
+    -6: "BFB_ERR_WATCHDOG",
+    -7: "BFB_ERR_UNSUPPORTED",
+}
+
+# Every symbol declared in include/biofvm_b200.h (checked by the CPU tests).
+EXPORTS = [
+    "bfb_last_error", "bfb_version", "bfb_create", "bfb_create_domain", "bfb_destroy", "bfb_get_shape",
+    "bfb_set_stream", "bfb_set_option", "bfb_synchronize", "bfb_set_coefficients", "bfb_set_field",
+    "bfb_get_field", "bfb_set_field_raw", "bfb_get_field_raw", "bfb_field_device_ptr", "bfb_set_dirichlet",
+    "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
+    "bfb_set_agents", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
+    "bfb_checksum",
+]
+
+
+class BFBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_up = ctypes.POINTER(ctypes.c_uint8)
+
+
+def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is missing: build it with `python biofvm-b_b200/build.py`")
+    L = ctypes.CDLL(str(path))
+    L.bfb_last_error.restype = ctypes.c_char_p
+    sig = {
+        "bfb_create": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                       ctypes.c_int, ctypes.c_int],
+        "bfb_create_domain": [ctypes.POINTER(_vp)] + [ctypes.c_double] * 7 + [ctypes.c_int] * 3,
+        "bfb_destroy": [_vp],
+        "bfb_get_shape": [_vp, _ip, _ip, _ip, _ip],
+        "bfb_set_stream": [_vp, _vp],
+        "bfb_set_option": [_vp, ctypes.c_int, ctypes.c_int],
+        "bfb_synchronize": [_vp],
+        "bfb_set_coefficients": [_vp, _dp, _dp],
+        "bfb_set_field": [_vp, _vp],
+        "bfb_get_field": [_vp, _vp],
+        "bfb_set_field_raw": [_vp, _vp],
+        "bfb_get_field_raw": [_vp, _vp],
+        "bfb_field_device_ptr": [_vp, ctypes.POINTER(_vp)],
+        "bfb_set_dirichlet": [_vp, _vp, _vp, _vp],
+        "bfb_set_dirichlet_uniform": [_vp, _vp, _vp, _vp],
+        "bfb_apply_dirichlet": [_vp],
+        "bfb_diffusion_step": [_vp, ctypes.c_double, ctypes.c_int],
+        "bfb_set_bulk": [_vp, _vp, _vp, _vp],
+        "bfb_bulk_step": [_vp, ctypes.c_double],
+        "bfb_set_agents": [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double],
+        "bfb_agent_voxels": [_vp, _vp],
+        "bfb_cells_step": [_vp, ctypes.c_double],
+        "bfb_simulate": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
+        "bfb_step_host": [_vp, _vp, ctypes.c_double, ctypes.c_int],
+        "bfb_profile_steps": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp],
+        "bfb_checksum": [_vp, _dp],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(code: int):
+    if code != 0:
+        raise BFBError(code, _lib.bfb_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _u8(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.uint8)
+
+
+class Env:
+    """One device-resident microenvironment (a ``bfb_env``)."""
+
+    def __init__(self, shape, n_substrates, dx=20.0, precision=FP64, device=0, domain=None):
+        L = load_library()
+        h = _vp()
+        if domain is not None:
+            x0, x1, y0, y1, z0, z1 = domain
+            _check(L.bfb_create_domain(ctypes.byref(h), x0, x1, y0, y1, z0, z1, dx, n_substrates, precision, device))
+        else:
+            nx, ny, nz = shape
+            _check(L.bfb_create(ctypes.byref(h), nx, ny, nz, n_substrates, dx, precision, device))
+        self.h = h
+        self.L = L
+        a = [ctypes.c_int() for _ in range(4)]
+        _check(L.bfb_get_shape(h, *[ctypes.byref(x) for x in a]))
+        self.nx, self.ny, self.nz, self.S = (x.value for x in a)
+        self.precision = precision
+        self.dx = dx
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz, self.S)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bfb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- configuration --------------------------------------------------
+    def set_stream(self, stream_handle: int):
+        _check(self.L.bfb_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def set_option(self, opt, value):
+        _check(self.L.bfb_set_option(self.h, opt, int(value)))
+
+    def set_coefficients(self, D, lam):
+        D, lam = _f64(D), _f64(lam)
+        assert D.size == self.S and lam.size == self.S
+        _check(self.L.bfb_set_coefficients(self.h, D.ctypes.data_as(_dp), lam.ctypes.data_as(_dp)))
+
+    def set_dirichlet(self, activation, values=None, face_mask=None):
+        act = _u8(activation)
+        v = None if values is None else _f64(values)
+        if v is not None:
+            assert v.size == self.nx * self.ny * self.nz * self.S
+        fm = _u8(face_mask)
+        _check(self.L.bfb_set_dirichlet(self.h, _ptr(v), _ptr(act), _ptr(fm)))
+
+    def set_dirichlet_uniform(self, activation, value_per_substrate, face_mask=None):
+        _check(self.L.bfb_set_dirichlet_uniform(self.h, _ptr(_f64(value_per_substrate)), _ptr(_u8(activation)),
+                                                _ptr(_u8(face_mask))))
+
+    def apply_dirichlet(self):
+        _check(self.L.bfb_apply_dirichlet(self.h))
+
+    def set_bulk(self, S_rate=None, T_target=None, U_rate=None):
+        if S_rate is None:
+            _check(self.L.bfb_set_bulk(self.h, None, None, None))
+            return
+        a, b, c = _f64(S_rate), _f64(T_target), _f64(U_rate)
+        _check(self.L.bfb_set_bulk(self.h, _ptr(a), _ptr(b), _ptr(c)))
+
+    def set_agents(self, pos, volume, secretion, uptake, saturation, dt, active=None):
+        pos, volume = _f64(pos), _f64(volume)
+        sec, upt, sat = _f64(secretion), _f64(uptake), _f64(saturation)
+        n = pos.shape[0]
+        _check(self.L.bfb_set_agents(self.h, n, _ptr(pos), _ptr(volume), _ptr(sec), _ptr(upt), _ptr(sat),
+                                     _ptr(_u8(active)), dt))
+        self.n_agents = n
+
+    def agent_voxels(self):
+        out = np.zeros(getattr(self, "n_agents", 0), dtype=np.int32)
+        _check(self.L.bfb_agent_voxels(self.h, _ptr(out)))
+        return out
+
+    # -- data -----------------------------------------------------------
+    def set_field(self, rho):
+        rho = _f64(rho)
+        assert rho.size == self.nx * self.ny * self.nz * self.S
+        _check(self.L.bfb_set_field(self.h, _ptr(rho)))
+
+    def get_field(self):
+        out = np.empty(self.shape, dtype=np.float64)
+        _check(self.L.bfb_get_field(self.h, _ptr(out)))
+        return out
+
+    def set_field_raw(self, rho):
+        dt = np.float64 if self.precision == FP64 else np.float32
+        rho = np.ascontiguousarray(rho, dtype=dt)
+        _check(self.L.bfb_set_field_raw(self.h, _ptr(rho)))
+
+    def get_field_raw(self):
+        dt = np.float64 if self.precision == FP64 else np.float32
+        out = np.empty(self.shape, dtype=dt)
+        _check(self.L.bfb_get_field_raw(self.h, _ptr(out)))
+        return out
+
+    def field_device_ptr(self) -> int:
+        p = _vp()
+        _check(self.L.bfb_field_device_ptr(self.h, ctypes.byref(p)))
+        return p.value
+
+    # -- stepping -------------------------------------------------------
+    def diffusion_step(self, dt, n=1):
+        _check(self.L.bfb_diffusion_step(self.h, dt, n))
+
+    def bulk_step(self, dt):
+        _check(self.L.bfb_bulk_step(self.h, dt))
+
+    def cells_step(self, dt):
+        _check(self.L.bfb_cells_step(self.h, dt))
+
+    def simulate(self, dt, n, flags=STEP_DIFFUSION):
+        _check(self.L.bfb_simulate(self.h, dt, n, flags))
+
+    def step_host_ptr(self, host_ptr: int, dt, n=1):
+        _check(self.L.bfb_step_host(self.h, ctypes.c_void_p(host_ptr), dt, n))
+
+    def synchronize(self):
+        _check(self.L.bfb_synchronize(self.h))
+
+    def profile_steps(self, dt, n, flags=STEP_DIFFUSION):
+        """Milliseconds per phase over n steps: x, y, z, bulk, cells."""
+        out = np.zeros(5)
+        _check(self.L.bfb_profile_steps(self.h, dt, n, flags, out.ctypes.data_as(_dp)))
+        return out
+
+    def checksum(self):
+        out = np.zeros(self.S)
+        _check(self.L.bfb_checksum(self.h, out.ctypes.data_as(_dp)))
+        return out

@@ -1,0 +1,319 @@
+// bfb_aux.cu -- agents (secretion/uptake), checksum and precision conversion.
+#include "bfb_aux.cuh"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+namespace bfb {
+
+// ---------------------------------------------------------------------------
+// Conversions
+// ---------------------------------------------------------------------------
+__global__ void d2f_kernel(const double *__restrict__ s, float *__restrict__ d, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        d[e] = __double2float_rn(s[e]);
+}
+__global__ void f2d_kernel(const float *__restrict__ s, double *__restrict__ d, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        d[e] = (double)s[e];
+}
+static unsigned grid_for(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 32); }
+
+int launch_convert_d2f(const double *src, float *dst, long long n, cudaStream_t s) {
+    if (n <= 0) return BFB_OK;
+    d2f_kernel<<<grid_for(n), 256, 0, s>>>(src, dst, n);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+int launch_convert_f2d(const float *src, double *dst, long long n, cudaStream_t s) {
+    if (n <= 0) return BFB_OK;
+    f2d_kernel<<<grid_for(n), 256, 0, s>>>(src, dst, n);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Agent binning and constants.
+//
+// Binning restates Basic_Agent::assign_position -> update_voxel_index ->
+// Cartesian_Mesh::nearest_voxel_local_index at one rank
+// (BioFVM_basic_agent.cpp:112-153, BioFVM_parallel.cpp:418-522,
+//  BioFVM_mesh.cpp:204-213):
+//   invalid position (outside the closed box)  -> position rejected, the
+//                                                agent keeps voxel 0
+//   v = (int)floor((p - lo)/h) clamped to [0, (int)((hi - lo)/h) - 1]
+//   index = x*lny*lnz + y*lnz + z with lny/lnz the truncated extents,
+//   clamped to [0, V-1].
+// Constants restate set_internal_uptake_constants (BioFVM_basic_agent.cpp:
+// 155-176) with the reference build's fused axpy:
+//   c = (dt*volume)/dV, t1 = (S*rho*)*c, t2 = fma(c, U, fma(c, S, 1)).
+// ---------------------------------------------------------------------------
+struct BinGeom {
+    double lo[3], hi[3], h[3];
+    int V;
+    double dV;
+};
+
+__device__ __forceinline__ int bin_axis(double p, double lo, double hi, double h) {
+    int v = (int)floor(__ddiv_rn(__dsub_rn(p, lo), h));
+    const int g = (int)__ddiv_rn(__dsub_rn(hi, lo), h);
+    if (v >= g) v = g - 1;
+    if (v < 0) v = 0;
+    return v;
+}
+
+__global__ void bin_agents_kernel(int n, int S, const double *__restrict__ pos, const double *__restrict__ vol,
+                                  const double *__restrict__ sec, const double *__restrict__ upt,
+                                  const double *__restrict__ sat, double dt, BinGeom g, int *__restrict__ voxel,
+                                  double *__restrict__ t1, double *__restrict__ t2) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const double x = pos[3 * a], y = pos[3 * a + 1], z = pos[3 * a + 2];
+    int idx = 0;  // a freshly created agent's current_voxel_index
+    const bool valid = !(x < g.lo[0] || x > g.hi[0] || y < g.lo[1] || y > g.hi[1] || z < g.lo[2] || z > g.hi[2]);
+    if (valid) {
+        const int xi = bin_axis(x, g.lo[0], g.hi[0], g.h[0]);
+        const int yi = bin_axis(y, g.lo[1], g.hi[1], g.h[1]);
+        const int zi = bin_axis(z, g.lo[2], g.hi[2], g.h[2]);
+        const int lny = (int)__ddiv_rn(__dsub_rn(g.hi[1], g.lo[1]), g.h[1]);
+        const int lnz = (int)__ddiv_rn(__dsub_rn(g.hi[2], g.lo[2]), g.h[2]);
+        idx = xi * lny * lnz + yi * lnz + zi;
+        if (idx < 0) idx = 0;
+        if (idx >= g.V) idx = g.V - 1;
+    }
+    voxel[a] = idx;
+    const double c = __ddiv_rn(__dmul_rn(dt, vol[a]), g.dV);
+    for (int d = 0; d < S; ++d) {
+        const size_t e = (size_t)a * S + d;
+        t1[e] = __dmul_rn(__dmul_rn(sec[e], sat[e]), c);
+        t2[e] = __fma_rn(c, upt[e], __fma_rn(c, sec[e], 1.0));
+    }
+}
+
+template <typename T>
+__global__ void gather_constants_kernel(int n_active, int S, const int *__restrict__ order,
+                                        const double *__restrict__ t1, const double *__restrict__ t2,
+                                        T *__restrict__ o1, T *__restrict__ o2) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)n_active * S) return;
+    const int r = (int)(e / S), d = (int)(e % S);
+    const int a = order[r];
+    o1[e] = (T)t1[(size_t)a * S + d];
+    o2[e] = (T)t2[(size_t)a * S + d];
+}
+
+// BioFVM_basic_agent.cpp:291-296 for all agents of one voxel, in list order.
+template <typename T>
+__global__ void cells_kernel(T *__restrict__ f, int S, int n_occ, const int *__restrict__ seg_start,
+                             const int *__restrict__ seg_voxel, const T *__restrict__ t1, const T *__restrict__ t2) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)n_occ * S) return;
+    const int s = (int)(e / S), d = (int)(e % S);
+    const size_t fe = (size_t)seg_voxel[s] * S + d;
+    T x = f[fe];
+    const int a1 = seg_start[s + 1];
+    for (int a = seg_start[s]; a < a1; ++a) {
+        const size_t q = (size_t)a * S + d;
+        if constexpr (sizeof(T) == 8)
+            x = __ddiv_rn(__dadd_rn(x, t1[q]), t2[q]);
+        else
+            x = __fdiv_rn(__fadd_rn(x, t1[q]), t2[q]);
+    }
+    f[fe] = x;
+}
+
+void agents_free(bfb_env_s *env) {
+    cudaFree(env->agent_voxel);
+    cudaFree(env->seg_start);
+    cudaFree(env->seg_voxel);
+    cudaFree(env->ag_t1);
+    cudaFree(env->ag_t2);
+    env->agent_voxel = env->seg_start = env->seg_voxel = nullptr;
+    env->ag_t1 = env->ag_t2 = nullptr;
+    env->n_agents = env->n_occ = env->n_active = 0;
+}
+
+namespace {
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { cudaFree(p); }
+    cudaError_t alloc(size_t bytes) { return cudaMalloc(&p, bytes ? bytes : 1); }
+    template <typename U>
+    U *as() { return static_cast<U *>(p); }
+};
+}  // namespace
+
+int agents_build(bfb_env_s *env, int n, const double *pos, const double *volume, const double *sec,
+                 const double *upt, const double *sat, const uint8_t *active, double dt) {
+    agents_free(env);
+    if (n == 0) return BFB_OK;
+    const int S = env->S;
+    cudaStream_t s = env->stream;
+    DevBuf d_pos, d_vol, d_sec, d_upt, d_sat, d_t1, d_t2, d_keys, d_keys_sorted, d_idx, d_idx_sorted, d_unique,
+        d_counts, d_nruns, d_tmp;
+    BFB_CUDA(d_pos.alloc(sizeof(double) * 3 * n));
+    BFB_CUDA(d_vol.alloc(sizeof(double) * n));
+    BFB_CUDA(d_sec.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_upt.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_sat.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_t1.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_t2.alloc(sizeof(double) * n * S));
+    BFB_CUDA(cudaMalloc(&env->agent_voxel, sizeof(int) * n));
+    BFB_CUDA(cudaMemcpyAsync(d_pos.p, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_vol.p, volume, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_sec.p, sec, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_upt.p, upt, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_sat.p, sat, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+
+    BinGeom g;
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = env->bbox[a];
+        g.hi[a] = env->bbox[3 + a];
+        g.h[a] = env->dx;
+    }
+    g.V = (int)env->V;
+    g.dV = (env->dx * env->dx) * env->dx;
+    bin_agents_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, S, d_pos.as<double>(), d_vol.as<double>(),
+                                                      d_sec.as<double>(), d_upt.as<double>(), d_sat.as<double>(), dt,
+                                                      g, env->agent_voxel, d_t1.as<double>(), d_t2.as<double>());
+    BFB_CUDA(cudaGetLastError());
+
+    // Keys of active agents (list order kept as the value); inactive agents
+    // take no part in secretion/uptake (BioFVM_basic_agent.cpp:282-283).
+    std::vector<int> h_vox(n);
+    BFB_CUDA(cudaMemcpyAsync(h_vox.data(), env->agent_voxel, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    BFB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> keys, idx;
+    keys.reserve(n);
+    idx.reserve(n);
+    for (int a = 0; a < n; ++a)
+        if (!active || active[a]) {
+            keys.push_back(h_vox[a]);
+            idx.push_back(a);
+        }
+    const int na = (int)keys.size();
+    env->n_agents = n;
+    env->n_active = na;
+    if (na == 0) return BFB_OK;
+    BFB_CUDA(d_keys.alloc(sizeof(int) * na));
+    BFB_CUDA(d_keys_sorted.alloc(sizeof(int) * na));
+    BFB_CUDA(d_idx.alloc(sizeof(int) * na));
+    BFB_CUDA(d_idx_sorted.alloc(sizeof(int) * na));
+    BFB_CUDA(d_unique.alloc(sizeof(int) * na));
+    BFB_CUDA(d_counts.alloc(sizeof(int) * na));
+    BFB_CUDA(d_nruns.alloc(sizeof(int)));
+    BFB_CUDA(cudaMemcpyAsync(d_keys.p, keys.data(), sizeof(int) * na, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_idx.p, idx.data(), sizeof(int) * na, cudaMemcpyHostToDevice, s));
+
+    // Stable LSD radix sort by voxel: agents of one voxel stay in list order.
+    int end_bit = 1;
+    while (end_bit < 31 && (1LL << end_bit) < env->V) ++end_bit;
+    size_t tmp_sort = 0, tmp_rle = 0;
+    BFB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_sort, d_keys.as<int>(), d_keys_sorted.as<int>(),
+                                             d_idx.as<int>(), d_idx_sorted.as<int>(), na, 0, end_bit, s));
+    BFB_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, tmp_rle, d_keys_sorted.as<int>(), d_unique.as<int>(),
+                                                d_counts.as<int>(), d_nruns.as<int>(), na, s));
+    BFB_CUDA(d_tmp.alloc(std::max(tmp_sort, tmp_rle)));
+    BFB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp.p, tmp_sort, d_keys.as<int>(), d_keys_sorted.as<int>(),
+                                             d_idx.as<int>(), d_idx_sorted.as<int>(), na, 0, end_bit, s));
+    BFB_CUDA(cub::DeviceRunLengthEncode::Encode(d_tmp.p, tmp_rle, d_keys_sorted.as<int>(), d_unique.as<int>(),
+                                                d_counts.as<int>(), d_nruns.as<int>(), na, s));
+    int n_occ = 0;
+    BFB_CUDA(cudaMemcpyAsync(&n_occ, d_nruns.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BFB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> counts(n_occ), starts(n_occ + 1, 0);
+    BFB_CUDA(cudaMemcpy(counts.data(), d_counts.p, sizeof(int) * n_occ, cudaMemcpyDeviceToHost));
+    for (int q = 0; q < n_occ; ++q) starts[q + 1] = starts[q] + counts[q];
+    BFB_CUDA(cudaMalloc(&env->seg_start, sizeof(int) * (n_occ + 1)));
+    BFB_CUDA(cudaMalloc(&env->seg_voxel, sizeof(int) * std::max(1, n_occ)));
+    BFB_CUDA(cudaMemcpyAsync(env->seg_start, starts.data(), sizeof(int) * (n_occ + 1), cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(env->seg_voxel, d_unique.p, sizeof(int) * n_occ, cudaMemcpyDeviceToDevice, s));
+    env->n_occ = n_occ;
+
+    BFB_CUDA(cudaMalloc(&env->ag_t1, env->elem * (size_t)na * S));
+    BFB_CUDA(cudaMalloc(&env->ag_t2, env->elem * (size_t)na * S));
+    const long long tot = (long long)na * S;
+    const unsigned gb = (unsigned)((tot + 255) / 256);
+    if (env->precision == BFB_FP64)
+        gather_constants_kernel<double><<<gb, 256, 0, s>>>(na, S, d_idx_sorted.as<int>(), d_t1.as<double>(),
+                                                           d_t2.as<double>(), (double *)env->ag_t1,
+                                                           (double *)env->ag_t2);
+    else
+        gather_constants_kernel<float><<<gb, 256, 0, s>>>(na, S, d_idx_sorted.as<int>(), d_t1.as<double>(),
+                                                          d_t2.as<double>(), (float *)env->ag_t1, (float *)env->ag_t2);
+    BFB_CUDA(cudaGetLastError());
+    BFB_CUDA(cudaStreamSynchronize(s));  // temporaries are freed on return
+    return BFB_OK;
+}
+
+int launch_cells(bfb_env_s *env, cudaStream_t s) {
+    if (env->n_occ == 0) return BFB_OK;
+    const long long tot = (long long)env->n_occ * env->S;
+    const unsigned gb = (unsigned)((tot + 255) / 256);
+    if (env->precision == BFB_FP64)
+        cells_kernel<double><<<gb, 256, 0, s>>>((double *)env->field, env->S, env->n_occ, env->seg_start,
+                                                env->seg_voxel, (const double *)env->ag_t1, (const double *)env->ag_t2);
+    else
+        cells_kernel<float><<<gb, 256, 0, s>>>((float *)env->field, env->S, env->n_occ, env->seg_start,
+                                               env->seg_voxel, (const float *)env->ag_t1, (const float *)env->ag_t2);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checksum: fixed partition of voxels per block, block tree sums in FP64,
+// then one block adds the partials in block order -> deterministic.
+// ---------------------------------------------------------------------------
+constexpr int kSumBlocks = 296;  // 2 x 148 SMs
+constexpr int kSumThreads = 256;
+constexpr int kMaxSumS = 64;
+
+template <typename T>
+__global__ void checksum_partial_kernel(const T *__restrict__ f, long long V, int S, double *__restrict__ partials) {
+    __shared__ double red[kSumThreads];
+    const long long per = (V + gridDim.x - 1) / gridDim.x;
+    const long long v0 = (long long)blockIdx.x * per, v1 = min(V, v0 + per);
+    for (int d = 0; d < S; ++d) {
+        double acc = 0.0;
+        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) acc += (double)f[(size_t)v * S + d];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * S + d] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void checksum_final_kernel(const double *__restrict__ partials, int nblocks, int S, double *__restrict__ out) {
+    const int d = threadIdx.x;
+    if (d >= S) return;
+    double acc = 0.0;
+    for (int b = 0; b < nblocks; ++b) acc += partials[(size_t)b * S + d];
+    out[d] = acc;
+}
+
+int checksum_prepare(bfb_env_s *env) {
+    if (env->partials) return BFB_OK;
+    BFB_CUDA(cudaMalloc(&env->partials, sizeof(double) * (kSumBlocks * (size_t)env->S + env->S)));
+    env->partial_blocks = kSumBlocks;
+    return BFB_OK;
+}
+
+int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s) {
+    if (env->S > kMaxSumS) return fail(BFB_ERR_UNSUPPORTED, "checksum supports at most 64 substrates");
+    if (env->precision == BFB_FP64)
+        checksum_partial_kernel<double><<<kSumBlocks, kSumThreads, 0, s>>>((const double *)env->field, env->V, env->S,
+                                                                         env->partials);
+    else
+        checksum_partial_kernel<float><<<kSumBlocks, kSumThreads, 0, s>>>((const float *)env->field, env->V, env->S,
+                                                                        env->partials);
+    checksum_final_kernel<<<1, kMaxSumS, 0, s>>>(env->partials, kSumBlocks, env->S, out_dev);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+
+}  // namespace bfb

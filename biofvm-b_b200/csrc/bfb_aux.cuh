@@ -1,0 +1,24 @@
+// bfb_aux.cuh -- agents, reductions and conversions.
+#pragma once
+#include "bfb_internal.cuh"
+
+namespace bfb {
+
+// Field precision conversion (device).
+int launch_convert_d2f(const double *src, float *dst, long long n, cudaStream_t s);
+int launch_convert_f2d(const float *src, double *dst, long long n, cudaStream_t s);
+
+// Agents: binning + cached constants (FP64, bit-exact with the reference),
+// then a stable voxel sort and per-voxel segments. All device memory of the
+// previous agent set is released first.
+int agents_build(bfb_env_s *env, int n, const double *pos, const double *volume, const double *sec,
+                 const double *upt, const double *sat, const uint8_t *active, double dt);
+void agents_free(bfb_env_s *env);
+int launch_cells(bfb_env_s *env, cudaStream_t s);
+
+// Per-substrate FP64 sums of the field. Writes S doubles to out_dev. Uses
+// env->partials (allocated on demand, outside any stream capture).
+int checksum_prepare(bfb_env_s *env);
+int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s);
+
+}  // namespace bfb

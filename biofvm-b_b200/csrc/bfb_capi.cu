@@ -1,0 +1,705 @@
+// bfb_capi.cu -- the C ABI (include/biofvm_b200.h): handles, coefficients,
+// Dirichlet, bulk, agents, step sequencing and CUDA-graph replay.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bfb_aux.cuh"
+#include "bfb_internal.cuh"
+#include "bfb_sweeps.cuh"
+
+namespace bfb {
+
+static thread_local std::string g_last_error = "no error";
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int code, const std::string &msg) {
+    set_error(msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    set_error(std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") in " + what);
+    return e == cudaErrorMemoryAllocation ? BFB_ERR_OOM : BFB_ERR_CUDA;
+}
+
+void sweeps_prepare_device();  // bfb_sweeps.cu
+
+// ---------------------------------------------------------------------------
+// Thomas factors, host FP64, in the reference's operation order
+// (BioFVM_parallel.cpp:780-912). The reference build fuses the axpy
+// `denom[m] += c1*c[m-1]` (g++ -ffp-contract=fast); std::fma does the same.
+// This file is compiled with -ffp-contract=off so nothing else is fused.
+// ---------------------------------------------------------------------------
+static void axis_factors(int n, int S, double dt, double dx, const double *D, const double *lam,
+                         std::vector<double> &den, std::vector<double> &c, std::vector<double> &c1v) {
+    den.assign((size_t)n * S, 0.0);
+    c.assign((size_t)n * S, 0.0);
+    c1v.assign(S, 0.0);
+    for (int d = 0; d < S; ++d) {
+        double c1 = D[d] * dt;
+        c1 /= dx;
+        c1 /= dx;
+        double c2 = lam[d] * dt;
+        c2 /= 3.0;
+        double c3 = 1.0;
+        c3 += c1;
+        c3 += c1;
+        c3 += c2;
+        double c3a = 1.0;
+        c3a += c1;
+        c3a += c2;
+        c1v[d] = c1;
+        for (int m = 0; m < n; ++m) {
+            c[(size_t)m * S + d] = -c1;
+            den[(size_t)m * S + d] = c3;
+        }
+        den[d] = c3a;
+        den[(size_t)(n - 1) * S + d] = c3a;
+        if (n == 1) den[d] = 1.0 + c2;
+        c[d] /= den[d];
+        for (int m = 1; m < n; ++m) {
+            den[(size_t)m * S + d] = std::fma(c1, c[(size_t)(m - 1) * S + d], den[(size_t)m * S + d]);
+            c[(size_t)m * S + d] /= den[(size_t)m * S + d];
+        }
+    }
+}
+
+static int upload_table(bfb_env_s *env, void *dst, const std::vector<double> &v, bool reciprocal) {
+    if (env->precision == BFB_FP64) {
+        BFB_CUDA(cudaMemcpy(dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(v.size());
+        for (size_t q = 0; q < v.size(); ++q) f[q] = (float)(reciprocal ? 1.0 / v[q] : v[q]);
+        BFB_CUDA(cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return BFB_OK;
+}
+
+static int ensure_factors(bfb_env_s *env, double dt) {
+    if (env->factors_valid && (env->freeze_factors || env->factor_dt == dt)) return BFB_OK;
+    const int ns[3] = {env->nx, env->ny, env->nz};
+    std::vector<double> den, c, c1;
+    // the factor tables are only read by kernels on env->stream
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    for (int a = 0; a < 3; ++a) {
+        axis_factors(ns[a], env->S, dt, env->dx, env->D.data(), env->lambda.data(), den, c, c1);
+        int st = upload_table(env, env->fac_den[a], den, true);
+        if (st) return st;
+        st = upload_table(env, env->fac_cb[a], c, false);
+        if (st) return st;
+    }
+    int st = upload_table(env, env->c1, c1, false);
+    if (st) return st;
+    env->factors_valid = true;
+    env->factor_dt = dt;
+    env->epoch++;
+    return BFB_OK;
+}
+
+template <typename T>
+static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
+    SweepArgs<T> a;
+    a.f = static_cast<T *>(env->field);
+    a.nx = env->nx;
+    a.ny = env->ny;
+    a.nz = env->nz;
+    a.S = env->S;
+    a.fac.den = static_cast<const T *>(env->fac_den[axis]);
+    a.fac.cb = static_cast<const T *>(env->fac_cb[axis]);
+    a.c1 = static_cast<const T *>(env->c1);
+    for (int f = 0; f < 6; ++f) a.dir.face[f] = static_cast<const T *>(env->faces[f]);
+    a.dir.mask = env->d_mask;
+    a.dir.nx = env->nx;
+    a.dir.ny = env->ny;
+    a.dir.nz = env->nz;
+    a.dir.S = env->S;
+    a.dir.any = env->dir_any;
+    a.bulk.A = static_cast<const T *>(env->bulkA);
+    a.bulk.B = static_cast<const T *>(env->bulkB);
+    a.bulk.dt = (T)dt;
+    a.bulk.on = bulk && env->bulk_on;
+    return a;
+}
+
+// One LOD diffusion step; `bulk` fuses a preceding bulk source/sink update
+// into the x-sweep load.
+template <typename T>
+static int run_diffusion(bfb_env_s *env, double dt, bool bulk, cudaStream_t s) {
+    int st = launch_strided<T>(make_args<T>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, s);
+    if (st) return st;
+    st = launch_strided<T>(make_args<T>(env, 1, false, dt), 1, false, env->tuning.warps_y, s);
+    if (st) return st;
+    return launch_contig<T>(make_args<T>(env, 2, false, dt), env->tuning.warps_z, s);
+}
+
+template <typename T>
+static int run_steps(bfb_env_s *env, double dt, int n, int flags, cudaStream_t s) {
+    for (int q = 0; q < n; ++q) {
+        int st = BFB_OK;
+        if (flags & BFB_STEP_DIFFUSION) {
+            st = run_diffusion<T>(env, dt, (flags & BFB_STEP_BULK) != 0, s);
+        } else if (flags & BFB_STEP_BULK) {
+            st = launch_bulk<T>(make_args<T>(env, 0, true, dt), env->N, s);
+        }
+        if (st) return st;
+        if (flags & BFB_STEP_CELLS) {
+            st = launch_cells(env, s);
+            if (st) return st;
+        }
+    }
+    return BFB_OK;
+}
+
+static int run_steps_any(bfb_env_s *env, double dt, int n, int flags, cudaStream_t s) {
+    return env->precision == BFB_FP64 ? run_steps<double>(env, dt, n, flags, s) : run_steps<float>(env, dt, n, flags, s);
+}
+
+static void drop_graph(bfb_env_s *env) {
+    if (env->graph_exec) cudaGraphExecDestroy(env->graph_exec);
+    env->graph_exec = nullptr;
+    env->graph_flags = -1;
+}
+
+static int check_env(bfb_env_s *env) {
+    if (!env) return fail(BFB_ERR_INVALID_ARG, "null bfb_env");
+    BFB_CUDA(cudaSetDevice(env->device));
+    return BFB_OK;
+}
+
+static int bulk_tabulate(bfb_env_s *env, const double *Sr, const double *T, const double *U) {
+    // A = T*S and B = U + S as the reference rounds them
+    // (BioFVM_microenvironment.cpp:1131-1142).
+    const size_t N = env->N;
+    std::vector<double> A(N), B(N);
+    for (size_t e = 0; e < N; ++e) {
+        A[e] = T[e] * Sr[e];
+        B[e] = U[e] + Sr[e];
+    }
+    if (!env->bulkA) BFB_CUDA(cudaMalloc(&env->bulkA, env->elem * N));
+    if (!env->bulkB) BFB_CUDA(cudaMalloc(&env->bulkB, env->elem * N));
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    int st = upload_table(env, env->bulkA, A, false);
+    if (st) return st;
+    return upload_table(env, env->bulkB, B, false);
+}
+
+}  // namespace bfb
+
+using namespace bfb;
+
+// ===========================================================================
+extern "C" {
+
+BFB_API const char *bfb_last_error(void) { return g_last_error.c_str(); }
+BFB_API int bfb_version(void) { return 100; }
+
+BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, double dx, int precision, int device) {
+    if (!out) return fail(BFB_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (nx < 1 || ny < 1 || nz < 1 || n_substrates < 1)
+        return fail(BFB_ERR_SIZE, "grid sizes and substrate count must be >= 1");
+    if (!(dx > 0)) return fail(BFB_ERR_INVALID_ARG, "dx must be > 0");
+    if (precision != BFB_FP64 && precision != BFB_FP32) return fail(BFB_ERR_INVALID_ARG, "precision must be BFB_FP64 or BFB_FP32");
+    const long long V = (long long)nx * ny * nz;
+    if (V > 0x7fffffffLL) return fail(BFB_ERR_SIZE, "more than 2^31-1 voxels");
+    int ndev = 0;
+    BFB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(BFB_ERR_INVALID_ARG, "no such CUDA device");
+    BFB_CUDA(cudaSetDevice(device));
+    sweeps_prepare_device();
+
+    bfb_env_s *env = new bfb_env_s();
+    env->device = device;
+    env->precision = precision;
+    env->nx = nx;
+    env->ny = ny;
+    env->nz = nz;
+    env->S = n_substrates;
+    env->dx = dx;
+    env->bbox[0] = env->bbox[1] = env->bbox[2] = 0.0;
+    env->bbox[3] = nx * dx;
+    env->bbox[4] = ny * dx;
+    env->bbox[5] = nz * dx;
+    env->elem = precision == BFB_FP64 ? 8 : 4;
+    env->V = V;
+    env->N = V * n_substrates;
+    env->D.assign(n_substrates, 0.0);
+    env->lambda.assign(n_substrates, 0.0);
+    env->activation.assign(n_substrates, 0);
+    env->face_mask.assign(6 * (size_t)n_substrates, 0);
+    int st = BFB_OK;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (st) return;
+        cudaError_t e = cudaMalloc(p, bytes ? bytes : 1);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMalloc");
+    };
+    alloc(&env->field, env->elem * env->N);
+    const int ns[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        alloc(&env->fac_den[a], env->elem * (size_t)ns[a] * n_substrates);
+        alloc(&env->fac_cb[a], env->elem * (size_t)ns[a] * n_substrates);
+    }
+    alloc(&env->c1, env->elem * n_substrates);
+    alloc((void **)&env->d_mask, n_substrates);
+    if (!st) {
+        cudaError_t e = cudaStreamCreateWithFlags(&env->own_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaStreamCreateWithFlags");
+        env->stream = env->own_stream;
+    }
+    if (!st) {
+        cudaError_t e = cudaMemset(env->field, 0, env->elem * env->N);
+        if (e == cudaSuccess) e = cudaMemset(env->d_mask, 0, n_substrates);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemset");
+    }
+    if (st) {
+        bfb_destroy(env);
+        return st;
+    }
+    *out = env;
+    return BFB_OK;
+}
+
+BFB_API int bfb_create_domain(bfb_env *out, double x0, double x1, double y0, double y1, double z0, double z1,
+                              double dx, int n_substrates, int precision, int device) {
+    if (!(dx > 0)) return fail(BFB_ERR_INVALID_ARG, "dx must be > 0");
+    // BioFVM_parallel.cpp:100-102
+    const double eps = 1e-16;
+    const int nx = (int)std::ceil(eps + (x1 - x0) / dx);
+    const int ny = (int)std::ceil(eps + (y1 - y0) / dx);
+    const int nz = (int)std::ceil(eps + (z1 - z0) / dx);
+    int st = bfb_create(out, nx, ny, nz, n_substrates, dx, precision, device);
+    if (st) return st;
+    bfb_env_s *env = *out;
+    env->bbox[0] = x0;
+    env->bbox[1] = y0;
+    env->bbox[2] = z0;
+    env->bbox[3] = x1;
+    env->bbox[4] = y1;
+    env->bbox[5] = z1;
+    return BFB_OK;
+}
+
+BFB_API int bfb_destroy(bfb_env env) {
+    if (!env) return BFB_OK;
+    cudaSetDevice(env->device);
+    if (env->stream) cudaStreamSynchronize(env->stream);
+    drop_graph(env);
+    agents_free(env);
+    cudaFree(env->field);
+    cudaFree(env->staging);
+    for (int a = 0; a < 3; ++a) {
+        cudaFree(env->fac_den[a]);
+        cudaFree(env->fac_cb[a]);
+    }
+    cudaFree(env->c1);
+    for (int f = 0; f < 6; ++f) cudaFree(env->faces[f]);
+    cudaFree(env->d_mask);
+    cudaFree(env->bulkA);
+    cudaFree(env->bulkB);
+    cudaFree(env->partials);
+    if (env->own_stream) cudaStreamDestroy(env->own_stream);
+    delete env;
+    return BFB_OK;
+}
+
+BFB_API int bfb_get_shape(bfb_env env, int *nx, int *ny, int *nz, int *S) {
+    if (!env) return fail(BFB_ERR_INVALID_ARG, "null bfb_env");
+    if (nx) *nx = env->nx;
+    if (ny) *ny = env->ny;
+    if (nz) *nz = env->nz;
+    if (S) *S = env->S;
+    return BFB_OK;
+}
+
+BFB_API int bfb_set_stream(bfb_env env, void *stream) {
+    int st = check_env(env);
+    if (st) return st;
+    // NULL selects the env's own stream again
+    cudaStream_t want = stream ? (cudaStream_t)stream : env->own_stream;
+    if (env->stream != want) {
+        BFB_CUDA(cudaStreamSynchronize(env->stream));
+        drop_graph(env);
+    }
+    env->stream = want;
+    return BFB_OK;
+}
+
+BFB_API int bfb_set_option(bfb_env env, int option, int value) {
+    if (!env) return fail(BFB_ERR_INVALID_ARG, "null bfb_env");
+    switch (option) {
+    case BFB_OPT_FREEZE_FACTORS: env->freeze_factors = value != 0; break;
+    case BFB_OPT_USE_GRAPHS:
+        env->use_graphs = value != 0;
+        drop_graph(env);
+        break;
+    default: return fail(BFB_ERR_INVALID_ARG, "unknown option");
+    }
+    return BFB_OK;
+}
+
+BFB_API int bfb_synchronize(bfb_env env) {
+    int st = check_env(env);
+    if (st) return st;
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_set_coefficients(bfb_env env, const double *D, const double *lambda) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!D || !lambda) return fail(BFB_ERR_INVALID_ARG, "D and lambda must not be NULL");
+    env->D.assign(D, D + env->S);
+    env->lambda.assign(lambda, lambda + env->S);
+    env->factors_valid = false;
+    return BFB_OK;
+}
+
+static int ensure_staging(bfb_env_s *env) {
+    if (env->staging) return BFB_OK;
+    BFB_CUDA(cudaMalloc(&env->staging, sizeof(double) * env->N));
+    return BFB_OK;
+}
+
+BFB_API int bfb_set_field(bfb_env env, const double *host) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
+    if (env->precision == BFB_FP64) {
+        BFB_CUDA(cudaMemcpyAsync(env->field, host, sizeof(double) * env->N, cudaMemcpyHostToDevice, env->stream));
+    } else {
+        if ((st = ensure_staging(env))) return st;
+        BFB_CUDA(cudaMemcpyAsync(env->staging, host, sizeof(double) * env->N, cudaMemcpyHostToDevice, env->stream));
+        if ((st = launch_convert_d2f((const double *)env->staging, (float *)env->field, env->N, env->stream))) return st;
+    }
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_get_field(bfb_env env, double *host) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
+    if (env->precision == BFB_FP64) {
+        BFB_CUDA(cudaMemcpyAsync(host, env->field, sizeof(double) * env->N, cudaMemcpyDeviceToHost, env->stream));
+    } else {
+        if ((st = ensure_staging(env))) return st;
+        if ((st = launch_convert_f2d((const float *)env->field, (double *)env->staging, env->N, env->stream))) return st;
+        BFB_CUDA(cudaMemcpyAsync(host, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, env->stream));
+    }
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_set_field_raw(bfb_env env, const void *host) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
+    BFB_CUDA(cudaMemcpyAsync(env->field, host, env->elem * env->N, cudaMemcpyHostToDevice, env->stream));
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_get_field_raw(bfb_env env, void *host) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
+    BFB_CUDA(cudaMemcpyAsync(host, env->field, env->elem * env->N, cudaMemcpyDeviceToHost, env->stream));
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_field_device_ptr(bfb_env env, void **dptr) {
+    if (!env || !dptr) return fail(BFB_ERR_INVALID_ARG, "null argument");
+    *dptr = env->field;
+    return BFB_OK;
+}
+
+// Dirichlet: cut the six face arrays out of per-voxel values.
+static int dirichlet_install(bfb_env_s *env, const std::vector<double> *faces_host /* 6 arrays or null */,
+                             const uint8_t *activation, const uint8_t *face_mask) {
+    const int S = env->S;
+    if (activation) env->activation.assign(activation, activation + S);
+    for (int f = 0; f < 6; ++f)
+        for (int d = 0; d < S; ++d) {
+            const uint8_t base = face_mask ? face_mask[f * S + d] : 1;
+            env->face_mask[f * S + d] = (base && env->activation[d]) ? 1 : 0;
+        }
+    std::vector<uint8_t> bits(S, 0);
+    int any = 0;
+    for (int d = 0; d < S; ++d) {
+        for (int f = 0; f < 6; ++f)
+            if (env->face_mask[f * S + d]) bits[d] |= (uint8_t)(1u << f);
+        any |= bits[d];
+    }
+    const size_t fsz[6] = {(size_t)env->ny * env->nz, (size_t)env->ny * env->nz, (size_t)env->nx * env->nz,
+                           (size_t)env->nx * env->nz, (size_t)env->nx * env->ny, (size_t)env->nx * env->ny};
+    for (int f = 0; f < 6; ++f)
+        if (!env->faces[f]) {
+            BFB_CUDA(cudaMalloc(&env->faces[f], env->elem * fsz[f] * S));
+            BFB_CUDA(cudaMemset(env->faces[f], 0, env->elem * fsz[f] * S));
+        }
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    if (faces_host)
+        for (int f = 0; f < 6; ++f) {
+            int st = upload_table(env, env->faces[f], faces_host[f], false);
+            if (st) return st;
+        }
+    BFB_CUDA(cudaMemcpy(env->d_mask, bits.data(), S, cudaMemcpyHostToDevice));
+    env->dir_any = any != 0;
+    env->epoch++;
+    return BFB_OK;
+}
+
+BFB_API int bfb_set_dirichlet(bfb_env env, const double *values, const uint8_t *activation, const uint8_t *face_mask) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!activation) return fail(BFB_ERR_INVALID_ARG, "activation must not be NULL");
+    if (!values) return dirichlet_install(env, nullptr, activation, face_mask);
+    const int nx = env->nx, ny = env->ny, nz = env->nz, S = env->S;
+    std::vector<double> F[6];
+    F[0].resize((size_t)ny * nz * S);
+    F[1].resize((size_t)ny * nz * S);
+    F[2].resize((size_t)nx * nz * S);
+    F[3].resize((size_t)nx * nz * S);
+    F[4].resize((size_t)nx * ny * S);
+    F[5].resize((size_t)nx * ny * S);
+    auto at = [&](int i, int j, int k, int d) { return values[(((size_t)i * ny + j) * nz + k) * S + d]; };
+    for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k)
+            for (int d = 0; d < S; ++d) {
+                F[0][((size_t)j * nz + k) * S + d] = at(0, j, k, d);
+                F[1][((size_t)j * nz + k) * S + d] = at(nx - 1, j, k, d);
+            }
+    for (int i = 0; i < nx; ++i)
+        for (int k = 0; k < nz; ++k)
+            for (int d = 0; d < S; ++d) {
+                F[2][((size_t)i * nz + k) * S + d] = at(i, 0, k, d);
+                F[3][((size_t)i * nz + k) * S + d] = at(i, ny - 1, k, d);
+            }
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int d = 0; d < S; ++d) {
+                F[4][((size_t)i * ny + j) * S + d] = at(i, j, 0, d);
+                F[5][((size_t)i * ny + j) * S + d] = at(i, j, nz - 1, d);
+            }
+    return dirichlet_install(env, F, activation, face_mask);
+}
+
+BFB_API int bfb_set_dirichlet_uniform(bfb_env env, const double *value_per_substrate, const uint8_t *activation,
+                                      const uint8_t *face_mask) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!activation) return fail(BFB_ERR_INVALID_ARG, "activation must not be NULL");
+    if (!value_per_substrate) return dirichlet_install(env, nullptr, activation, face_mask);
+    const int nx = env->nx, ny = env->ny, nz = env->nz, S = env->S;
+    const size_t fsz[6] = {(size_t)ny * nz, (size_t)ny * nz, (size_t)nx * nz, (size_t)nx * nz, (size_t)nx * ny,
+                           (size_t)nx * ny};
+    std::vector<double> F[6];
+    for (int f = 0; f < 6; ++f) {
+        F[f].resize(fsz[f] * S);
+        for (size_t q = 0; q < fsz[f]; ++q)
+            for (int d = 0; d < S; ++d) F[f][q * S + d] = value_per_substrate[d];
+    }
+    return dirichlet_install(env, F, activation, face_mask);
+}
+
+BFB_API int bfb_apply_dirichlet(bfb_env env) {
+    int st = check_env(env);
+    if (st) return st;
+    st = env->precision == BFB_FP64 ? launch_dirichlet<double>(make_args<double>(env, 0, false, 0), env->stream)
+                                    : launch_dirichlet<float>(make_args<float>(env, 0, false, 0), env->stream);
+    return st;
+}
+
+BFB_API int bfb_diffusion_step(bfb_env env, double dt, int n_steps) {
+    int st = check_env(env);
+    if (st) return st;
+    if (n_steps < 0) return fail(BFB_ERR_INVALID_ARG, "n_steps < 0");
+    if (!(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0");
+    if ((st = ensure_factors(env, dt))) return st;
+    return run_steps_any(env, dt, n_steps, BFB_STEP_DIFFUSION, env->stream);
+}
+
+
+BFB_API int bfb_set_bulk(bfb_env env, const double *supply_rate, const double *target, const double *uptake) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!supply_rate && !target && !uptake) {
+        env->bulk_on = 0;
+        env->epoch++;
+        return BFB_OK;
+    }
+    if (!supply_rate || !target || !uptake) return fail(BFB_ERR_INVALID_ARG, "bulk: give all three arrays or none");
+    if ((st = bulk_tabulate(env, supply_rate, target, uptake))) return st;
+    env->bulk_on = 1;
+    env->epoch++;
+    return BFB_OK;
+}
+
+BFB_API int bfb_bulk_step(bfb_env env, double dt) {
+    int st = check_env(env);
+    if (st) return st;
+    return run_steps_any(env, dt, 1, BFB_STEP_BULK, env->stream);
+}
+
+BFB_API int bfb_set_agents(bfb_env env, int n, const double *pos, const double *volume, const double *secretion,
+                           const double *uptake, const double *saturation, const uint8_t *active, double dt) {
+    int st = check_env(env);
+    if (st) return st;
+    if (n < 0) return fail(BFB_ERR_INVALID_ARG, "n < 0");
+    if (n > 0 && (!pos || !volume || !secretion || !uptake || !saturation))
+        return fail(BFB_ERR_INVALID_ARG, "agent arrays must not be NULL");
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    st = agents_build(env, n, pos, volume, secretion, uptake, saturation, active, dt);
+    env->epoch++;
+    return st;
+}
+
+BFB_API int bfb_agent_voxels(bfb_env env, int *out) {
+    int st = check_env(env);
+    if (st) return st;
+    if (env->n_agents == 0) return BFB_OK;
+    if (!out) return fail(BFB_ERR_INVALID_ARG, "out is NULL");
+    BFB_CUDA(cudaMemcpy(out, env->agent_voxel, sizeof(int) * env->n_agents, cudaMemcpyDeviceToHost));
+    return BFB_OK;
+}
+
+BFB_API int bfb_cells_step(bfb_env env, double dt) {
+    (void)dt;  // constants are cached by bfb_set_agents, as set_internal_uptake_constants does
+    int st = check_env(env);
+    if (st) return st;
+    return launch_cells(env, env->stream);
+}
+
+BFB_API int bfb_simulate(bfb_env env, double dt, int n_steps, int flags) {
+    int st = check_env(env);
+    if (st) return st;
+    if (n_steps < 0) return fail(BFB_ERR_INVALID_ARG, "n_steps < 0");
+    if (!(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0");
+    if (flags & ~(BFB_STEP_BULK | BFB_STEP_DIFFUSION | BFB_STEP_CELLS)) return fail(BFB_ERR_INVALID_ARG, "bad flags");
+    if (flags & BFB_STEP_DIFFUSION)
+        if ((st = ensure_factors(env, dt))) return st;
+    if (n_steps == 0) return BFB_OK;
+    if (!env->use_graphs || env->stream == nullptr) return run_steps_any(env, dt, n_steps, flags, env->stream);
+    // One step captured as a graph, replayed n_steps times.
+    if (!env->graph_exec || env->graph_flags != flags || env->graph_dt != dt || env->graph_epoch != env->epoch) {
+        drop_graph(env);
+        cudaGraph_t graph = nullptr;
+        BFB_CUDA(cudaStreamBeginCapture(env->stream, cudaStreamCaptureModeThreadLocal));
+        int cst = run_steps_any(env, dt, 1, flags, env->stream);
+        cudaError_t e = cudaStreamEndCapture(env->stream, &graph);
+        if (cst) {
+            if (graph) cudaGraphDestroy(graph);
+            return cst;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&env->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            env->graph_exec = nullptr;
+            return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        env->graph_flags = flags;
+        env->graph_dt = dt;
+        env->graph_epoch = env->epoch;
+    }
+    for (int q = 0; q < n_steps; ++q) BFB_CUDA(cudaGraphLaunch(env->graph_exec, env->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_steps) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!host_field) return fail(BFB_ERR_INVALID_ARG, "host_field is NULL");
+    if ((st = ensure_factors(env, dt))) return st;
+    cudaStream_t s = env->stream;
+    if (env->precision == BFB_FP64) {
+        BFB_CUDA(cudaMemcpyAsync(env->field, host_field, sizeof(double) * env->N, cudaMemcpyHostToDevice, s));
+    } else {
+        if ((st = ensure_staging(env))) return st;
+        BFB_CUDA(cudaMemcpyAsync(env->staging, host_field, sizeof(double) * env->N, cudaMemcpyHostToDevice, s));
+        if ((st = launch_convert_d2f((const double *)env->staging, (float *)env->field, env->N, s))) return st;
+    }
+    if ((st = run_steps_any(env, dt, n_steps, BFB_STEP_DIFFUSION, s))) return st;
+    if (env->precision == BFB_FP64) {
+        BFB_CUDA(cudaMemcpyAsync(host_field, env->field, sizeof(double) * env->N, cudaMemcpyDeviceToHost, s));
+    } else {
+        if ((st = launch_convert_f2d((const float *)env->field, (double *)env->staging, env->N, s))) return st;
+        BFB_CUDA(cudaMemcpyAsync(host_field, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, s));
+    }
+    BFB_CUDA(cudaStreamSynchronize(s));
+    return BFB_OK;
+}
+
+// Per-phase device time, the counterpart of the reference's -DTIMING CSV
+// (BioFVM_parallel.cpp:695-697, 1259-1392): events around every launch.
+BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, double *ms_out) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!ms_out || n_steps < 1) return fail(BFB_ERR_INVALID_ARG, "ms_out NULL or n_steps < 1");
+    if (!(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0");
+    if (flags & BFB_STEP_DIFFUSION)
+        if ((st = ensure_factors(env, dt))) return st;
+    for (int q = 0; q < BFB_PROFILE_PHASES; ++q) ms_out[q] = 0.0;
+    cudaStream_t s = env->stream;
+    cudaEvent_t ev[BFB_PROFILE_PHASES + 1];
+    for (auto &e : ev) BFB_CUDA(cudaEventCreate(&e));
+    auto phase_ms = [&](int ph, auto &&launch) -> int {
+        BFB_CUDA(cudaEventRecord(ev[0], s));
+        int r = launch();
+        if (r) return r;
+        BFB_CUDA(cudaEventRecord(ev[1], s));
+        BFB_CUDA(cudaEventSynchronize(ev[1]));
+        float ms = 0;
+        BFB_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        ms_out[ph] += ms;
+        return BFB_OK;
+    };
+    for (int q = 0; q < n_steps && !st; ++q) {
+        const bool fp64 = env->precision == BFB_FP64;
+        if (flags & BFB_STEP_DIFFUSION) {
+            const bool bulk = (flags & BFB_STEP_BULK) != 0;
+            st = phase_ms(0, [&] {
+                return fp64 ? launch_strided<double>(make_args<double>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, s)
+                            : launch_strided<float>(make_args<float>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, s);
+            });
+            if (!st)
+                st = phase_ms(1, [&] {
+                    return fp64 ? launch_strided<double>(make_args<double>(env, 1, false, dt), 1, false, env->tuning.warps_y, s)
+                                : launch_strided<float>(make_args<float>(env, 1, false, dt), 1, false, env->tuning.warps_y, s);
+                });
+            if (!st)
+                st = phase_ms(2, [&] {
+                    return fp64 ? launch_contig<double>(make_args<double>(env, 2, false, dt), env->tuning.warps_z, s)
+                                : launch_contig<float>(make_args<float>(env, 2, false, dt), env->tuning.warps_z, s);
+                });
+        } else if (flags & BFB_STEP_BULK) {
+            st = phase_ms(3, [&] {
+                return fp64 ? launch_bulk<double>(make_args<double>(env, 0, true, dt), env->N, s)
+                            : launch_bulk<float>(make_args<float>(env, 0, true, dt), env->N, s);
+            });
+        }
+        if (!st && (flags & BFB_STEP_CELLS)) st = phase_ms(4, [&] { return launch_cells(env, s); });
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return st;
+}
+
+BFB_API int bfb_checksum(bfb_env env, double *out) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!out) return fail(BFB_ERR_INVALID_ARG, "out is NULL");
+    if ((st = checksum_prepare(env))) return st;
+    double *dout = env->partials + (size_t)env->partial_blocks * env->S;
+    if ((st = launch_checksum(env, dout, env->stream))) return st;
+    BFB_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * env->S, cudaMemcpyDeviceToHost, env->stream));
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    return BFB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,132 @@
+// bfb_internal.cuh -- shared types of the B200 diffusion-decay library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "biofvm_b200.h"
+
+namespace bfb {
+
+// ---------------------------------------------------------------------------
+// Error plumbing: every C entry point returns a status and records a message.
+// ---------------------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define BFB_CUDA(call)                                        \
+    do {                                                      \
+        cudaError_t _e = (call);                              \
+        if (_e != cudaSuccess) return ::bfb::cuda_fail(_e, #call); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Dirichlet faces on the device.
+//   faces[f] holds the values of face f for every substrate:
+//     f = 0/1 (x-lo/hi): [ny][nz][S]   f = 2/3 (y-lo/hi): [nx][nz][S]
+//     f = 4/5 (z-lo/hi): [nx][ny][S]
+//   mask[d] bit f set <=> face f is active for substrate d.
+// A voxel on several faces (edges, corners) has the same value in every face
+// array, because all are cut from one per-voxel array.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DirFaces {
+    const T *face[6];
+    const uint8_t *mask;  // [S]
+    int nx, ny, nz, S;
+    int any;              // 0: no active face for any substrate
+};
+
+// Thomas factors of one axis on the device.
+//   den[m*S+d]: FP64 path: the reference's denominators (divided by);
+//               FP32 path: their reciprocals 1/den, computed in FP64, rounded once.
+//   cb[m*S+d]:  back-substitution coefficients c[m] (negative numbers).
+template <typename T>
+struct AxisFactors {
+    const T *den;
+    const T *cb;
+};
+
+// Bulk source/sink terms fused into the x-sweep load.
+//   A = S*T (rounded once), B = U + S (rounded once); rho <- (rho + dt*A) / (B*dt + 1)
+template <typename T>
+struct BulkTerms {
+    const T *A;
+    const T *B;
+    T dt;
+    int on;
+};
+
+// Launch configuration chosen by the autotuner (or defaults).
+struct SweepTuning {
+    int warps_x = 2;   // warps per CTA of the strided kernels (x and y)
+    int warps_y = 2;
+    int warps_z = 2;   // warps per CTA of the contiguous kernel (z)
+};
+
+}  // namespace bfb
+
+// ---------------------------------------------------------------------------
+// The environment handle.
+// ---------------------------------------------------------------------------
+struct bfb_env_s {
+    int device = 0;
+    int precision = BFB_FP64;
+    int nx = 0, ny = 0, nz = 0, S = 0;
+    double dx = 0;
+    double bbox[6] = {0, 0, 0, 0, 0, 0};  // x0, y0, z0, x1, y1, z1
+    cudaStream_t stream = nullptr;       // stream all device work is issued on
+    cudaStream_t own_stream = nullptr;   // created by bfb_create, used unless bfb_set_stream overrides
+    size_t elem = 8;                     // bytes per field element
+    int64_t V = 0;                       // voxels
+    int64_t N = 0;                       // V * S
+
+    void *field = nullptr;               // device, N elements
+    void *staging = nullptr;             // device, N doubles (host double <-> env precision)
+
+    // coefficients and cached factors
+    std::vector<double> D, lambda;
+    bool factors_valid = false;
+    double factor_dt = 0;
+    int freeze_factors = 1;
+    void *fac_den[3] = {nullptr, nullptr, nullptr};
+    void *fac_cb[3] = {nullptr, nullptr, nullptr};
+    void *c1 = nullptr;                  // [S]
+
+    // Dirichlet
+    std::vector<uint8_t> activation;     // [S]
+    std::vector<uint8_t> face_mask;      // [6*S], already ANDed with activation
+    void *faces[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint8_t *d_mask = nullptr;           // [S]
+    int dir_any = 0;
+
+    // bulk
+    int bulk_on = 0;
+    void *bulkA = nullptr, *bulkB = nullptr;
+
+    // agents
+    int n_agents = 0;
+    int n_occ = 0;                       // occupied voxels with >= 1 active agent
+    int *agent_voxel = nullptr;          // [n_agents], list order (current_voxel_index)
+    int *seg_start = nullptr;            // [n_occ + 1]
+    int *seg_voxel = nullptr;            // [n_occ]
+    void *ag_t1 = nullptr, *ag_t2 = nullptr;  // [n_active][S] in voxel-sorted, list-stable order
+    int n_active = 0;
+
+    // scratch for reductions
+    double *partials = nullptr;
+    int partial_blocks = 0;
+
+    // CUDA graph of bfb_simulate
+    int use_graphs = 1;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_flags = -1;
+    double graph_dt = 0;
+    uint64_t graph_epoch = 0;            // bumps whenever captured state changes
+    uint64_t epoch = 1;
+
+    bfb::SweepTuning tuning;
+};

@@ -1,0 +1,73 @@
+// bfb_sweeps.cuh -- LOD Thomas sweeps for sm_100a.
+//
+// One LOD step of the reference (BioFVM_parallel.cpp:693-1395) is
+//     Dir, X-sweep, Dir, Y-sweep, Dir, Z-sweep, Dir
+// where every sweep solves, for each grid line and substrate, the symmetric
+// tridiagonal system tridiag(-c1, diag, -c1) y = u with precomputed Thomas
+// factors (forward: y0 = u0/den0, ym = (um + c1*y(m-1))/den_m; back:
+// ym -= c_m * y(m+1)), and Dir overwrites the active outer faces.
+//
+// Field layout rho[((i*ny + j)*nz + k)*S + d]: z (with d) is contiguous, x is
+// the slowest axis. So:
+//   * x- and y-sweeps are STRIDED: a line's elements are P = ny*nz*S (x) or
+//     nz*S (y) elements apart, and P consecutive lines form a contiguous row.
+//     A warp owns 32 adjacent lines ("columns"); its n x 32 tile is staged
+//     into shared memory with cp.async (16-byte copies when aligned), one lane
+//     per line runs the recurrence in shared memory, and the back substitution
+//     stores straight to global memory, 128 B (FP32) / 256 B (FP64) per warp
+//     store. One read and one write of the field per sweep.
+//   * the z-sweep is CONTIGUOUS: a line lives inside one (i,j) row of nz*S
+//     contiguous elements. A warp stages R = 32/S whole rows (one contiguous
+//     block of global memory) into padded shared rows, lane (r, d) solves line
+//     (row r, substrate d) in place, and the warp copies the rows back out.
+// Dirichlet is fused: the pre-X Dir (and, if enabled, the bulk source/sink
+// update that precedes the step) on the X-sweep load, and each post-sweep Dir
+// on that sweep's store. Because Dir is a pure overwrite of fixed positions
+// and each sweep rewrites every element of its line, this is exactly the
+// reference's sequence. The recurrence keeps the un-overwritten values.
+#pragma once
+#include "bfb_internal.cuh"
+
+namespace bfb {
+
+struct StridedGeom {
+    int n;                 // line length
+    long long P;           // lines per slab == element stride between line elements
+    long long slab_stride; // elements between slabs
+    int n_slabs;
+    int ncb;               // 32-column blocks per slab
+    int axis;              // 0 = x, 1 = y
+};
+
+struct ContigGeom {
+    int nz;
+    long long nrows;       // nx * ny rows of nz*S elements
+    int R;                 // rows per warp tile
+    int RS;                // shared-memory row stride (elements), RS = S (mod 32)
+};
+
+template <typename T>
+struct SweepArgs {
+    T *f;
+    int nx, ny, nz, S;
+    AxisFactors<T> fac;
+    const T *c1;           // [S]
+    DirFaces<T> dir;
+    BulkTerms<T> bulk;
+};
+
+// launchers (bfb_sweeps.cu)
+template <typename T>
+int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, cudaStream_t s);
+template <typename T>
+int launch_contig(const SweepArgs<T> &a, int warps, cudaStream_t s);
+template <typename T>
+int launch_dirichlet(const SweepArgs<T> &a, cudaStream_t s);
+template <typename T>
+int launch_bulk(const SweepArgs<T> &a, long long N, cudaStream_t s);
+
+// shared-memory bytes a strided / contiguous CTA needs (0 if it does not fit)
+size_t strided_smem(int n, int elem, int warps);
+size_t contig_smem(int nz, int S, int elem, int warps, int *R, int *RS);
+
+}  // namespace bfb

@@ -1,0 +1,176 @@
+/*
+ * biofvm_b200.h -- C ABI of the B200-native BioFVM-B diffusion-decay path.
+ *
+ * One `bfb_env` is one device-resident microenvironment: a uniform Cartesian
+ * voxel grid (nx, ny, nz) of edge dx holding S substrates, stored on the GPU in
+ * the reference's layout  rho[((i*ny + j)*nz + k)*S + d]  (voxel-major,
+ * substrate-inner; BioFVM_mesh.cpp:659-665), in FP64 or FP32.
+ *
+ * Every entry point returns an int status (BFB_OK = 0, negative on error) and
+ * never aborts; bfb_last_error() gives the calling thread's last message.
+ * Handles are not thread-safe; all device work of a handle is issued on its
+ * stream (bfb_set_stream), so calls may be captured in a CUDA graph by the
+ * caller. Host pointers are plain host memory (pinned memory makes the copies
+ * asynchronous-capable but is not required). No torch types cross this line.
+ *
+ * Reference interfaces replaced (reference paths, file:line):
+ *   - the swappable solver pointer  void (*diffusion_decay_solver)(Microenvironment&,
+ *     double dt, int, int, int*, int*, MPI_Comm)   BioFVM_microenvironment.h:164,
+ *     its callers simulate_diffusion_decay         BioFVM_microenvironment.cpp:1018-1029,
+ *     and the solvers behind it                    BioFVM_parallel.cpp:693-1395 / 1411-2326
+ *   - apply_dirichlet_conditions + Dirichlet setters
+ *                                                  BioFVM_microenvironment.cpp:226-484
+ *   - simulate_bulk_sources_and_sinks              BioFVM_microenvironment.cpp:1110-1153
+ *   - simulate_cell_sources_and_sinks / Basic_Agent::simulate_secretion_and_uptake
+ *                                                  BioFVM_microenvironment.cpp:1155-1169,
+ *                                                  BioFVM_basic_agent.cpp:279-300
+ */
+#ifndef BIOFVM_B200_H
+#define BIOFVM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BFB_API __attribute__((visibility("default")))
+#else
+#define BFB_API
+#endif
+
+typedef struct bfb_env_s *bfb_env;
+
+/* status codes */
+#define BFB_OK 0
+#define BFB_ERR_INVALID_ARG (-1)
+#define BFB_ERR_SIZE (-2)
+#define BFB_ERR_OOM (-3)
+#define BFB_ERR_CUDA (-4)
+#define BFB_ERR_STATE (-5)
+#define BFB_ERR_WATCHDOG (-6)
+#define BFB_ERR_UNSUPPORTED (-7)
+
+/* field precision */
+#define BFB_FP64 0
+#define BFB_FP32 1
+
+/* options (bfb_set_option) */
+#define BFB_OPT_FREEZE_FACTORS 1 /* 1 (default): Thomas factors are computed on the first step
+                                    and kept, as BioFVM_parallel.cpp:714,913 does; 0: recomputed
+                                    whenever dt differs from the cached one */
+#define BFB_OPT_USE_GRAPHS 2     /* 1 (default): bfb_simulate replays a captured CUDA graph */
+
+/* bfb_simulate flags: per step, in the order of examples/3D_tumor_example_X.cpp:346-348 */
+#define BFB_STEP_BULK 1
+#define BFB_STEP_DIFFUSION 2
+#define BFB_STEP_CELLS 4
+
+/* Thread-local text of the last error (never NULL). */
+BFB_API const char *bfb_last_error(void);
+BFB_API int bfb_version(void);
+
+/* Create a grid of nx*ny*nz voxels of edge dx with S substrates whose domain
+ * starts at the origin. Replaces Microenvironment() + resize_space_uniform()
+ * (BioFVM_microenvironment.cpp:140-216, BioFVM_parallel.cpp:18-59) at one rank.
+ * All D and lambda start at 0; no Dirichlet face is active (see
+ * bfb_set_dirichlet for the reference's defaults). */
+BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, double dx,
+                       int precision, int device);
+
+/* Same, from a domain box, with the reference's node count
+ * n = (int)ceil(1e-16 + (hi - lo)/dx) per axis (BioFVM_parallel.cpp:100-102).
+ * The box is also the one agent positions are binned against. */
+BFB_API int bfb_create_domain(bfb_env *out, double x0, double x1, double y0, double y1,
+                              double z0, double z1, double dx, int n_substrates, int precision,
+                              int device);
+
+BFB_API int bfb_destroy(bfb_env env);
+BFB_API int bfb_get_shape(bfb_env env, int *nx, int *ny, int *nz, int *n_substrates);
+/* Every env owns a non-blocking stream; bfb_set_stream(env, s) issues its
+ * work on the caller's stream s instead (NULL: back to the env's own). */
+BFB_API int bfb_set_stream(bfb_env env, void *cuda_stream);
+BFB_API int bfb_set_option(bfb_env env, int option, int value);
+BFB_API int bfb_synchronize(bfb_env env);
+
+/* Per-substrate diffusion coefficients and decay rates (the public vectors
+ * diffusion_coefficients / decay_rates, BioFVM_microenvironment.h:151-152).
+ * Invalidates the cached Thomas factors. */
+BFB_API int bfb_set_coefficients(bfb_env env, const double *D, const double *lambda);
+
+/* Field transfer, V*S values in the reference layout. The double variants
+ * convert to/from the env's precision on the device; the _raw variants copy
+ * the env's own element type (double for FP64, float for FP32). */
+BFB_API int bfb_set_field(bfb_env env, const double *host);
+BFB_API int bfb_get_field(bfb_env env, double *host);
+BFB_API int bfb_set_field_raw(bfb_env env, const void *host);
+BFB_API int bfb_get_field_raw(bfb_env env, void *host);
+/* Device pointer of the field (env precision); valid until bfb_destroy. */
+BFB_API int bfb_field_device_ptr(bfb_env env, void **dptr);
+
+/* Dirichlet conditions on the outer faces.
+ *   values     V*S per-voxel values like the reference's dirichlet_value_vectors
+ *              (only outer-face voxels are read), or NULL to keep the current ones
+ *   activation S flags, dirichlet_activation_vector (BioFVM_microenvironment.cpp:328-332)
+ *   face_mask  6*S flags [face][d] (faces x-lo, x-hi, y-lo, y-hi, z-lo, z-hi), or
+ *              NULL for the reference's rule: all six faces follow activation[d]
+ *              (BioFVM_microenvironment.cpp:381-484). A non-NULL mask is ANDed
+ *              with activation and extends the reference (e.g. x-faces only).
+ * A new env has every face inactive and all values 0; the reference's own
+ * constructor defaults (activation true, value 100.0 after resize,
+ * BioFVM_parallel.cpp:56) are applied by the C++ facade. */
+BFB_API int bfb_set_dirichlet(bfb_env env, const double *values, const uint8_t *activation,
+                              const uint8_t *face_mask);
+/* set_substrate_dirichlet_value(d, v) for every d at once
+ * (BioFVM_microenvironment.cpp:334-359): one value per substrate on all faces. */
+BFB_API int bfb_set_dirichlet_uniform(bfb_env env, const double *value_per_substrate,
+                                      const uint8_t *activation, const uint8_t *face_mask);
+/* apply_dirichlet_conditions(rank, size) at one rank. */
+BFB_API int bfb_apply_dirichlet(bfb_env env);
+
+/* n_steps LOD diffusion-decay steps (Dir, X, Dir, Y, Dir, Z, Dir each),
+ * the work of diffusion_decay_solver__constant_coefficients_LOD_3D. */
+BFB_API int bfb_diffusion_step(bfb_env env, double dt, int n_steps);
+
+/* Bulk sources and sinks: S (supply rate), T (target density), U (uptake
+ * rate), V*S each, as the three bulk callbacks would write them
+ * (BioFVM_microenvironment.h:165-167). Pass all NULL to disable. */
+BFB_API int bfb_set_bulk(bfb_env env, const double *supply_rate, const double *target,
+                         const double *uptake);
+BFB_API int bfb_bulk_step(bfb_env env, double dt);
+
+/* Agents (Basic_Agent): n agents in list order, pos n*3, volume n, rates n*S,
+ * active n flags (NULL = all active). Binning, the cached constants of
+ * set_internal_uptake_constants(dt) and the voxel sort run on the device. */
+BFB_API int bfb_set_agents(bfb_env env, int n, const double *pos, const double *volume,
+                           const double *secretion, const double *uptake,
+                           const double *saturation, const uint8_t *active, double dt);
+/* current_voxel_index of each agent (list order). */
+BFB_API int bfb_agent_voxels(bfb_env env, int *out);
+BFB_API int bfb_cells_step(bfb_env env, double dt);
+
+/* n_steps composite steps, each [bulk] -> [diffusion] -> [cells] by flags. */
+BFB_API int bfb_simulate(bfb_env env, double dt, int n_steps, int flags);
+
+/* Host-buffer step for reference-facing callers: copies host (V*S doubles)
+ * to the device, runs n_steps diffusion steps, copies the result back. */
+BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_steps);
+
+/* Device time per phase, the counterpart of the reference's -DTIMING per-sweep
+ * CSV (BioFVM_parallel.cpp:695-697, 1259-1392): runs n_steps steps like
+ * bfb_simulate (without a graph) with CUDA events around every launch and
+ * adds the milliseconds of each phase to ms_out[BFB_PROFILE_PHASES]:
+ * 0 x-sweep (with the fused pre-x Dirichlet / bulk), 1 y-sweep, 2 z-sweep,
+ * 3 standalone bulk, 4 cells. */
+#define BFB_PROFILE_PHASES 5
+BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, double *ms_out);
+
+/* Per-substrate FP64 sum of the field over all voxels (mass checksum). */
+BFB_API int bfb_checksum(bfb_env env, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

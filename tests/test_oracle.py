@@ -1,0 +1,151 @@
+"""CPU tests: the oracle restatement is pinned to the reference.
+
+* against the committed golden fixtures (made by the reference library), bit-exact;
+* against the live reference library when it is built here (oracle/_ref), bit-exact;
+* the adjoint restatement against central finite differences.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import log_uniform
+from oracle.oracle import REF_SO, RefEnv, RefLib, face_mask_all
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def golden(name):
+    return dict(np.load(GOLD / f"{name}.npz"))
+
+
+def test_config1_golden_bitexact(oracle):
+    g = golden("config1_15cube")
+    S = 1
+    vals = np.broadcast_to(np.asarray(g["dir_value"], float), g["rho0"].shape)
+    out = oracle.lod_steps(g["rho0"], float(g["dt"]), float(g["dx"]), g["D"], g["lam"], int(g["steps"]),
+                           vals, face_mask_all(g["activation"]))
+    assert np.array_equal(out, g["out"])
+    # the reference's AVX2 solver gives the same bits (both fuse the axpy)
+    assert np.array_equal(g["out_avx"], g["out"])
+    assert S == g["rho0"].shape[-1]
+
+
+@pytest.mark.parametrize("name", ["multi_7x5x9_S3", "multi_1x4x6_S2", "multi_2x3x1_S2", "multi_17x3x33_S5"])
+def test_multi_golden_bitexact(oracle, name):
+    g = golden(name)
+    out = oracle.lod_steps(g["rho0"], float(g["dt"]), float(g["dx"]), g["D"], g["lam"], int(g["steps"]),
+                           g["dir_values"], face_mask_all(g["activation"]))
+    assert np.array_equal(out, g["out"])
+
+
+def test_bulk_golden_bitexact(oracle):
+    g = golden("bulk_9x8x7_S3")
+    rho = g["rho0"]
+    S = rho.shape[-1]
+    for _ in range(3):
+        rho = oracle.bulk_step(rho, float(g["dt"]), g["S_rate"], g["T_target"], g["U_rate"])
+        rho = oracle.lod_steps(rho, float(g["dt"]), float(g["dx"]), g["D"], g["lam"], 1, None,
+                               np.zeros((6, S), np.uint8))
+    assert np.array_equal(rho, g["out"])
+
+
+def test_agents_golden_bitexact(oracle):
+    g = golden("agents_12x10x9_S2")
+    rho = g["rho0"]
+    S = rho.shape[-1]
+    dt, dx = float(g["dt"]), float(g["dx"])
+    vox = oracle.bin_agents(g["pos"], g["bbox"], dx, rho.shape[:3])
+    # rejected positions keep a new agent's voxel 0
+    assert np.array_equal(np.where(vox < 0, 0, vox), g["voxels"])
+    assert (vox < 0).sum() == 2
+    t1, t2 = oracle.agent_constants(dt, dx, g["vol"], g["sec"], g["upt"], g["sat"])
+    for _ in range(3):
+        rho = oracle.lod_steps(rho, dt, dx, g["D"], g["lam"], 1, None, np.zeros((6, S), np.uint8))
+        rho = oracle.cells_step(rho, np.where(vox < 0, 0, vox), t1, t2)
+    assert np.array_equal(rho, g["out"])
+
+
+needs_ref = pytest.mark.skipif(not REF_SO.exists(), reason="reference library not built here")
+
+
+@needs_ref
+@pytest.mark.parametrize("shape,S", [((5, 6, 7), 4), ((3, 1, 2), 1), ((11, 4, 2), 6), ((2, 2, 2), 3)])
+def test_live_reference_bitexact(oracle, rng, shape, S):
+    ref = RefLib()
+    dx, dt = 20.0, 0.01
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    e = RefEnv(ref, (0, 0, 0, *(np.array(shape) * dx)), dx, D, lam)
+    rho0 = rng.random(e.shape)
+    act = (rng.random(S) < 0.5).astype(np.uint8)
+    vals = rng.random(e.shape) * 10
+    e.set_field(rho0)
+    e.set_dirichlet(act, face_values=vals)
+    e.step(dt, 3)
+    out = oracle.lod_steps(rho0, dt, dx, D, lam, 3, vals, face_mask_all(act))
+    assert np.array_equal(out, e.field())
+
+
+@needs_ref
+def test_live_reference_default_dirichlet_is_100(oracle):
+    """dirichlet_test's 'should be 100' (examples/dirichlet_test.cpp:277): after
+    resize the reference's Dirichlet value is 100.0 with activation true."""
+    ref = RefLib()
+    e = RefEnv(ref, (0, 0, 0, 100, 100, 100), 20.0, [1e3], [0.1])
+    e.set_field(np.zeros(e.shape))
+    e.apply_dirichlet()
+    f = e.field()
+    assert f[0, 0, 0, 0] == 100.0 and f[2, 2, 2, 0] == 0.0
+
+
+@needs_ref
+def test_live_reference_non_multiple_domain_binning(oracle, rng):
+    """Domain length not a multiple of dx: the node count uses ceil while the
+    binning extents truncate (BioFVM_parallel.cpp:100-102 vs 440-446)."""
+    ref = RefLib()
+    dx = 20.0
+    box = (0.0, 0.0, 0.0, 105.0, 93.0, 71.0)
+    e = RefEnv(ref, box, dx, [1e3, 1e4], [0.1, 0.2])
+    pos = rng.uniform(-5, 110, (500, 3))
+    vol = np.ones(500)
+    z = np.zeros((500, 2))
+    e.add_agents(pos, vol, z, z, z, 0.01)
+    ov = oracle.bin_agents(pos, box, dx, e.shape[:3])
+    assert np.array_equal(np.where(ov < 0, 0, ov), e.agent_voxels())
+
+
+def test_adjoint_oracle_matches_finite_differences(oracle, rng):
+    shape, S = (4, 3, 5), 2
+    dx, dt = 20.0, 0.01
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-2, 1.0, S)
+    rho = rng.random((*shape, S))
+    vals = rng.random((*shape, S))
+    fm = np.zeros((6, S), np.uint8)
+    fm[0, 0] = fm[1, 0] = 1
+    w = rng.random((*shape, S))
+
+    def loss(r, Dv, lv):
+        return float((oracle.lod_steps(r, dt, dx, Dv, lv, 1, vals, fm) * w).sum())
+
+    g_rho, gD, gL = oracle.lod_step_adjoint(rho, w, dt, dx, D, lam, vals, fm)
+    for q in range(S):
+        h = D[q] * 1e-6
+        Dp, Dm = D.copy(), D.copy()
+        Dp[q] += h
+        Dm[q] -= h
+        fd = (loss(rho, Dp, lam) - loss(rho, Dm, lam)) / (2 * h)
+        assert abs(fd - gD[q]) <= 1e-6 * max(1.0, abs(fd))
+        h = lam[q] * 1e-6
+        Lp, Lm = lam.copy(), lam.copy()
+        Lp[q] += h
+        Lm[q] -= h
+        fd = (loss(rho, D, Lp) - loss(rho, D, Lm)) / (2 * h)
+        assert abs(fd - gL[q]) <= 1e-6 * max(1.0, abs(fd))
+    # the step is affine in rho: the gradient is exact up to rounding
+    for idx in [(0, 0, 0, 0), (1, 2, 3, 1), (3, 1, 4, 0), (2, 1, 2, 1)]:
+        e = np.zeros_like(rho)
+        e[idx] = 1.0
+        fd = (loss(rho + e, D, lam) - loss(rho - e, D, lam)) / 2
+        assert abs(fd - g_rho[idx]) <= 1e-10
