@@ -48,7 +48,7 @@ EXPORTS = [
     "bfb_set_stream", "bfb_set_option", "bfb_synchronize", "bfb_set_coefficients", "bfb_set_field",
     "bfb_get_field", "bfb_set_field_raw", "bfb_get_field_raw", "bfb_field_device_ptr", "bfb_set_dirichlet",
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
-    "bfb_set_agents", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
+    "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
     "bfb_checksum",
 ]
 
@@ -97,6 +97,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_set_bulk": [_vp, _vp, _vp, _vp],
         "bfb_bulk_step": [_vp, ctypes.c_double],
         "bfb_set_agents": [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double],
+        "bfb_set_agent_constants": [_vp, ctypes.c_int, _vp, _vp, _vp, _vp],
         "bfb_agent_voxels": [_vp, _vp],
         "bfb_cells_step": [_vp, ctypes.c_double],
         "bfb_simulate": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
@@ -211,6 +212,12 @@ class Env:
         _check(self.L.bfb_set_agents(self.h, n, _ptr(pos), _ptr(volume), _ptr(sec), _ptr(upt), _ptr(sat),
                                      _ptr(_u8(active)), dt))
         self.n_agents = n
+
+    def set_agent_constants(self, voxel, temp1, temp2, active=None):
+        vox = np.ascontiguousarray(voxel, dtype=np.int32)
+        t1, t2 = _f64(temp1), _f64(temp2)
+        _check(self.L.bfb_set_agent_constants(self.h, vox.size, _ptr(vox), _ptr(t1), _ptr(t2), _ptr(_u8(active))))
+        self.n_agents = vox.size
 
     def agent_voxels(self):
         out = np.zeros(getattr(self, "n_agents", 0), dtype=np.int32)

@@ -35,7 +35,8 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     LIB_DIR.mkdir(exist_ok=True)
     obj_dir = PKG / "_build"
     obj_dir.mkdir(exist_ok=True)
-    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "biofvm_b200.h"]
+    deps = ([CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "biofvm_b200.h"] +
+            list((PKG / "host").rglob("*.cpp")) + list((PKG / "host").glob("*.h")))
     newest = max(p.stat().st_mtime for p in deps)
     if LIB.exists() and LIB.stat().st_mtime >= newest and not force:
         return LIB
@@ -46,7 +47,23 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
         _run([NVCC, *ARCH, *FLAGS, *extra, "-c", CSRC / s, "-o", o])
         objs.append(o)
     _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs])
+    build_host()
     return LIB
+
+
+HOST_LIB = LIB_DIR / "libbiofvm_b200_host.so"
+DEMO = LIB_DIR / "facade_demo"
+CXX = "/usr/bin/g++"
+
+
+def build_host() -> None:
+    """The C++ facade (host/) over the C ABI, and its example driver."""
+    inc = [f"-I{ROOT / 'include'}", f"-I{PKG / 'host'}"]
+    flags = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall"]
+    _run([CXX, *flags, *inc, "-shared", "-o", HOST_LIB, PKG / "host" / "BioFVM_B200.cpp", f"-L{LIB_DIR}",
+          "-lbiofvm_b200", "-Wl,-rpath,$ORIGIN"])
+    _run([CXX, *flags, *inc, "-o", DEMO, PKG / "host" / "examples" / "facade_demo.cpp", f"-L{LIB_DIR}",
+          "-lbiofvm_b200_host", "-lbiofvm_b200", "-Wl,-rpath,$ORIGIN"])
 
 
 if __name__ == "__main__":

@@ -144,58 +144,30 @@ struct DevBuf {
 };
 }  // namespace
 
-int agents_build(bfb_env_s *env, int n, const double *pos, const double *volume, const double *sec,
-                 const double *upt, const double *sat, const uint8_t *active, double dt) {
-    agents_free(env);
-    if (n == 0) return BFB_OK;
+// Sort the active agents by voxel (stable: list order within a voxel) and
+// build the per-voxel segments the cells kernel walks. d_vox/d_t1/d_t2 are
+// device arrays in list order (d_t1/d_t2 FP64, [n][S]); active may be NULL.
+static int index_agents(bfb_env_s *env, int n, const int *d_vox, const double *d_t1, const double *d_t2,
+                        const uint8_t *active) {
     const int S = env->S;
     cudaStream_t s = env->stream;
-    DevBuf d_pos, d_vol, d_sec, d_upt, d_sat, d_t1, d_t2, d_keys, d_keys_sorted, d_idx, d_idx_sorted, d_unique,
-        d_counts, d_nruns, d_tmp;
-    BFB_CUDA(d_pos.alloc(sizeof(double) * 3 * n));
-    BFB_CUDA(d_vol.alloc(sizeof(double) * n));
-    BFB_CUDA(d_sec.alloc(sizeof(double) * n * S));
-    BFB_CUDA(d_upt.alloc(sizeof(double) * n * S));
-    BFB_CUDA(d_sat.alloc(sizeof(double) * n * S));
-    BFB_CUDA(d_t1.alloc(sizeof(double) * n * S));
-    BFB_CUDA(d_t2.alloc(sizeof(double) * n * S));
-    BFB_CUDA(cudaMalloc(&env->agent_voxel, sizeof(int) * n));
-    BFB_CUDA(cudaMemcpyAsync(d_pos.p, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-    BFB_CUDA(cudaMemcpyAsync(d_vol.p, volume, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    BFB_CUDA(cudaMemcpyAsync(d_sec.p, sec, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
-    BFB_CUDA(cudaMemcpyAsync(d_upt.p, upt, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
-    BFB_CUDA(cudaMemcpyAsync(d_sat.p, sat, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
-
-    BinGeom g;
-    for (int a = 0; a < 3; ++a) {
-        g.lo[a] = env->bbox[a];
-        g.hi[a] = env->bbox[3 + a];
-        g.h[a] = env->dx;
-    }
-    g.V = (int)env->V;
-    g.dV = (env->dx * env->dx) * env->dx;
-    bin_agents_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, S, d_pos.as<double>(), d_vol.as<double>(),
-                                                      d_sec.as<double>(), d_upt.as<double>(), d_sat.as<double>(), dt,
-                                                      g, env->agent_voxel, d_t1.as<double>(), d_t2.as<double>());
-    BFB_CUDA(cudaGetLastError());
-
-    // Keys of active agents (list order kept as the value); inactive agents
-    // take no part in secretion/uptake (BioFVM_basic_agent.cpp:282-283).
     std::vector<int> h_vox(n);
-    BFB_CUDA(cudaMemcpyAsync(h_vox.data(), env->agent_voxel, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    BFB_CUDA(cudaMemcpyAsync(h_vox.data(), d_vox, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
     BFB_CUDA(cudaStreamSynchronize(s));
     std::vector<int> keys, idx;
     keys.reserve(n);
     idx.reserve(n);
-    for (int a = 0; a < n; ++a)
+    for (int a = 0; a < n; ++a) {
         if (!active || active[a]) {
+            if (h_vox[a] < 0 || h_vox[a] >= env->V) return fail(BFB_ERR_INVALID_ARG, "agent voxel index out of range");
             keys.push_back(h_vox[a]);
             idx.push_back(a);
         }
+    }
     const int na = (int)keys.size();
-    env->n_agents = n;
     env->n_active = na;
     if (na == 0) return BFB_OK;
+    DevBuf d_keys, d_keys_sorted, d_idx, d_idx_sorted, d_unique, d_counts, d_nruns, d_tmp;
     BFB_CUDA(d_keys.alloc(sizeof(int) * na));
     BFB_CUDA(d_keys_sorted.alloc(sizeof(int) * na));
     BFB_CUDA(d_idx.alloc(sizeof(int) * na));
@@ -236,15 +208,68 @@ int agents_build(bfb_env_s *env, int n, const double *pos, const double *volume,
     const long long tot = (long long)na * S;
     const unsigned gb = (unsigned)((tot + 255) / 256);
     if (env->precision == BFB_FP64)
-        gather_constants_kernel<double><<<gb, 256, 0, s>>>(na, S, d_idx_sorted.as<int>(), d_t1.as<double>(),
-                                                           d_t2.as<double>(), (double *)env->ag_t1,
-                                                           (double *)env->ag_t2);
+        gather_constants_kernel<double><<<gb, 256, 0, s>>>(na, S, d_idx_sorted.as<int>(), d_t1, d_t2,
+                                                           (double *)env->ag_t1, (double *)env->ag_t2);
     else
-        gather_constants_kernel<float><<<gb, 256, 0, s>>>(na, S, d_idx_sorted.as<int>(), d_t1.as<double>(),
-                                                          d_t2.as<double>(), (float *)env->ag_t1, (float *)env->ag_t2);
+        gather_constants_kernel<float><<<gb, 256, 0, s>>>(na, S, d_idx_sorted.as<int>(), d_t1, d_t2,
+                                                          (float *)env->ag_t1, (float *)env->ag_t2);
     BFB_CUDA(cudaGetLastError());
     BFB_CUDA(cudaStreamSynchronize(s));  // temporaries are freed on return
     return BFB_OK;
+}
+
+int agents_build(bfb_env_s *env, int n, const double *pos, const double *volume, const double *sec,
+                 const double *upt, const double *sat, const uint8_t *active, double dt) {
+    agents_free(env);
+    if (n == 0) return BFB_OK;
+    const int S = env->S;
+    cudaStream_t s = env->stream;
+    DevBuf d_pos, d_vol, d_sec, d_upt, d_sat, d_t1, d_t2;
+    BFB_CUDA(d_pos.alloc(sizeof(double) * 3 * n));
+    BFB_CUDA(d_vol.alloc(sizeof(double) * n));
+    BFB_CUDA(d_sec.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_upt.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_sat.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_t1.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_t2.alloc(sizeof(double) * n * S));
+    BFB_CUDA(cudaMalloc(&env->agent_voxel, sizeof(int) * n));
+    BFB_CUDA(cudaMemcpyAsync(d_pos.p, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_vol.p, volume, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_sec.p, sec, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_upt.p, upt, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_sat.p, sat, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+
+    BinGeom g;
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = env->bbox[a];
+        g.hi[a] = env->bbox[3 + a];
+        g.h[a] = env->dx;
+    }
+    g.V = (int)env->V;
+    g.dV = (env->dx * env->dx) * env->dx;
+    bin_agents_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, S, d_pos.as<double>(), d_vol.as<double>(),
+                                                      d_sec.as<double>(), d_upt.as<double>(), d_sat.as<double>(), dt,
+                                                      g, env->agent_voxel, d_t1.as<double>(), d_t2.as<double>());
+    BFB_CUDA(cudaGetLastError());
+    env->n_agents = n;
+    return index_agents(env, n, env->agent_voxel, d_t1.as<double>(), d_t2.as<double>(), active);
+}
+
+int agents_build_constants(bfb_env_s *env, int n, const int *voxel, const double *t1, const double *t2,
+                           const uint8_t *active) {
+    agents_free(env);
+    if (n == 0) return BFB_OK;
+    const int S = env->S;
+    cudaStream_t s = env->stream;
+    DevBuf d_t1, d_t2;
+    BFB_CUDA(d_t1.alloc(sizeof(double) * n * S));
+    BFB_CUDA(d_t2.alloc(sizeof(double) * n * S));
+    BFB_CUDA(cudaMalloc(&env->agent_voxel, sizeof(int) * n));
+    BFB_CUDA(cudaMemcpyAsync(env->agent_voxel, voxel, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_t1.p, t1, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+    BFB_CUDA(cudaMemcpyAsync(d_t2.p, t2, sizeof(double) * n * S, cudaMemcpyHostToDevice, s));
+    env->n_agents = n;
+    return index_agents(env, n, env->agent_voxel, d_t1.as<double>(), d_t2.as<double>(), active);
 }
 
 int launch_cells(bfb_env_s *env, cudaStream_t s) {

@@ -13,6 +13,10 @@ int launch_convert_f2d(const float *src, double *dst, long long n, cudaStream_t 
 // previous agent set is released first.
 int agents_build(bfb_env_s *env, int n, const double *pos, const double *volume, const double *sec,
                  const double *upt, const double *sat, const uint8_t *active, double dt);
+// Same, from the constants an agent already caches (current_voxel_index,
+// temp1, temp2 in list order), as the reference's Basic_Agent holds them.
+int agents_build_constants(bfb_env_s *env, int n, const int *voxel, const double *t1, const double *t2,
+                           const uint8_t *active);
 void agents_free(bfb_env_s *env);
 int launch_cells(bfb_env_s *env, cudaStream_t s);
 

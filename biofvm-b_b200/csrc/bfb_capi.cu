@@ -27,7 +27,6 @@ int cuda_fail(cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? BFB_ERR_OOM : BFB_ERR_CUDA;
 }
 
-void sweeps_prepare_device();  // bfb_sweeps.cu
 
 // ---------------------------------------------------------------------------
 // Thomas factors, host FP64, in the reference's operation order
@@ -69,14 +68,72 @@ static void axis_factors(int n, int S, double dt, double dx, const double *D, co
     }
 }
 
-static int upload_table(bfb_env_s *env, void *dst, const std::vector<double> &v, bool reciprocal) {
+static int upload_table(bfb_env_s *env, void *dst, const std::vector<double> &v) {
     if (env->precision == BFB_FP64) {
         BFB_CUDA(cudaMemcpy(dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
     } else {
         std::vector<float> f(v.size());
-        for (size_t q = 0; q < v.size(); ++q) f[q] = (float)(reciprocal ? 1.0 / v[q] : v[q]);
+        for (size_t q = 0; q < v.size(); ++q) f[q] = (float)v[q];
         BFB_CUDA(cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
+    return BFB_OK;
+}
+
+// First row from which every table is bitwise constant up to row n-2, over
+// all substrates (at least 1; n-1 when there is no such tail).
+static int tail_start(const std::vector<std::vector<double>> &tabs, int n, int S) {
+    int m0 = 1;
+    for (const auto &t : tabs)
+        for (int d = 0; d < S; ++d) {
+            int m = n - 2;
+            if (m < 1) return std::max(1, n - 1);
+            while (m > 1 && t[(size_t)(m - 1) * S + d] == t[(size_t)(n - 2) * S + d]) --m;
+            m0 = std::max(m0, m);
+        }
+    return m0;
+}
+
+// The device tables for one axis from the reference's factors (den, c).
+//   FP64: den and c as they are.
+//   FP32: 1/den as a hi+lo pair of floats, c1/den and c rounded once; the
+//         deviation form of the FP32 kernels (bfb_sweeps.cuh) needs no c1.
+static int upload_factors(bfb_env_s *env, int axis, int n, const std::vector<double> &den,
+                          const std::vector<double> &c, const std::vector<double> &c1) {
+    const int S = env->S;
+    const size_t nS = (size_t)n * S;
+    std::vector<std::vector<double>> tabs;
+    if (env->precision == BFB_FP64) {
+        tabs = {den, c};
+    } else {
+        std::vector<double> rh(nS), rl(nS), a(nS), cf(nS);
+        for (int m = 0; m < n; ++m)
+            for (int d = 0; d < S; ++d) {
+                const size_t q = (size_t)m * S + d;
+                const double r = 1.0 / den[q];
+                rh[q] = (double)(float)r;
+                rl[q] = (double)(float)(r - rh[q]);
+                a[q] = (double)(float)(c1[d] / den[q]);
+                cf[q] = (double)(float)c[q];
+            }
+        tabs = {rh, rl, a, cf};
+    }
+    const int m0 = tail_start(tabs, n, S);
+    std::vector<double> flat, tail(4 * (size_t)S, 0.0);
+    flat.reserve(4 * nS);
+    for (size_t k = 0; k < 4; ++k) {
+        if (k < tabs.size()) {
+            flat.insert(flat.end(), tabs[k].begin(), tabs[k].end());
+            if (m0 <= n - 2)
+                for (int d = 0; d < S; ++d) tail[k * S + d] = tabs[k][(size_t)m0 * S + d];
+        } else {
+            flat.insert(flat.end(), nS, 0.0);
+        }
+    }
+    int st = upload_table(env, env->fac_tab[axis], flat);
+    if (st) return st;
+    st = upload_table(env, env->fac_tail[axis], tail);
+    if (st) return st;
+    env->fac_m0[axis] = m0;
     return BFB_OK;
 }
 
@@ -88,13 +145,21 @@ static int ensure_factors(bfb_env_s *env, double dt) {
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     for (int a = 0; a < 3; ++a) {
         axis_factors(ns[a], env->S, dt, env->dx, env->D.data(), env->lambda.data(), den, c, c1);
-        int st = upload_table(env, env->fac_den[a], den, true);
-        if (st) return st;
-        st = upload_table(env, env->fac_cb[a], c, false);
+        int st = upload_factors(env, a, ns[a], den, c, c1);
         if (st) return st;
     }
-    int st = upload_table(env, env->c1, c1, false);
+    int st = upload_table(env, env->c1, c1);
     if (st) return st;
+    // g = 1/(1 + c2), c2 = dt*lambda/3 (BioFVM_parallel.cpp:793-794), as hi, lo
+    std::vector<double> g(2 * (size_t)env->S);
+    for (int d = 0; d < env->S; ++d) {
+        double c2 = env->lambda[d] * dt;
+        c2 /= 3.0;
+        const double gv = 1.0 / (1.0 + c2);
+        g[d] = (double)(float)gv;
+        g[env->S + d] = (double)(float)(gv - g[d]);
+    }
+    if ((st = upload_table(env, env->g, g))) return st;
     env->factors_valid = true;
     env->factor_dt = dt;
     env->epoch++;
@@ -109,9 +174,17 @@ static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
     a.ny = env->ny;
     a.nz = env->nz;
     a.S = env->S;
-    a.fac.den = static_cast<const T *>(env->fac_den[axis]);
-    a.fac.cb = static_cast<const T *>(env->fac_cb[axis]);
+    const int ns[3] = {env->nx, env->ny, env->nz};
+    const size_t nS = (size_t)ns[axis] * env->S;
+    const T *tab = static_cast<const T *>(env->fac_tab[axis]);
+    a.fac.t0 = tab;
+    a.fac.t1 = tab + nS;
+    a.fac.t2 = tab + 2 * nS;
+    a.fac.t3 = tab + 3 * nS;
+    a.fac.tail = static_cast<const T *>(env->fac_tail[axis]);
+    a.fac.m0 = env->fac_m0[axis];
     a.c1 = static_cast<const T *>(env->c1);
+    a.g = static_cast<const T *>(env->g);
     for (int f = 0; f < 6; ++f) a.dir.face[f] = static_cast<const T *>(env->faces[f]);
     a.dir.mask = env->d_mask;
     a.dir.nx = env->nx;
@@ -183,9 +256,9 @@ static int bulk_tabulate(bfb_env_s *env, const double *Sr, const double *T, cons
     if (!env->bulkA) BFB_CUDA(cudaMalloc(&env->bulkA, env->elem * N));
     if (!env->bulkB) BFB_CUDA(cudaMalloc(&env->bulkB, env->elem * N));
     BFB_CUDA(cudaStreamSynchronize(env->stream));
-    int st = upload_table(env, env->bulkA, A, false);
+    int st = upload_table(env, env->bulkA, A);
     if (st) return st;
-    return upload_table(env, env->bulkB, B, false);
+    return upload_table(env, env->bulkB, B);
 }
 
 }  // namespace bfb
@@ -241,10 +314,11 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
     alloc(&env->field, env->elem * env->N);
     const int ns[3] = {nx, ny, nz};
     for (int a = 0; a < 3; ++a) {
-        alloc(&env->fac_den[a], env->elem * (size_t)ns[a] * n_substrates);
-        alloc(&env->fac_cb[a], env->elem * (size_t)ns[a] * n_substrates);
+        alloc(&env->fac_tab[a], env->elem * 4 * (size_t)ns[a] * n_substrates);
+        alloc(&env->fac_tail[a], env->elem * 4 * (size_t)n_substrates);
     }
     alloc(&env->c1, env->elem * n_substrates);
+    alloc(&env->g, env->elem * 2 * n_substrates);
     alloc((void **)&env->d_mask, n_substrates);
     if (!st) {
         cudaError_t e = cudaStreamCreateWithFlags(&env->own_stream, cudaStreamNonBlocking);
@@ -293,10 +367,11 @@ BFB_API int bfb_destroy(bfb_env env) {
     cudaFree(env->field);
     cudaFree(env->staging);
     for (int a = 0; a < 3; ++a) {
-        cudaFree(env->fac_den[a]);
-        cudaFree(env->fac_cb[a]);
+        cudaFree(env->fac_tab[a]);
+        cudaFree(env->fac_tail[a]);
     }
     cudaFree(env->c1);
+    cudaFree(env->g);
     for (int f = 0; f < 6; ++f) cudaFree(env->faces[f]);
     cudaFree(env->d_mask);
     cudaFree(env->bulkA);
@@ -446,7 +521,7 @@ static int dirichlet_install(bfb_env_s *env, const std::vector<double> *faces_ho
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     if (faces_host)
         for (int f = 0; f < 6; ++f) {
-            int st = upload_table(env, env->faces[f], faces_host[f], false);
+            int st = upload_table(env, env->faces[f], faces_host[f]);
             if (st) return st;
         }
     BFB_CUDA(cudaMemcpy(env->d_mask, bits.data(), S, cudaMemcpyHostToDevice));
@@ -556,6 +631,18 @@ BFB_API int bfb_set_agents(bfb_env env, int n, const double *pos, const double *
         return fail(BFB_ERR_INVALID_ARG, "agent arrays must not be NULL");
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     st = agents_build(env, n, pos, volume, secretion, uptake, saturation, active, dt);
+    env->epoch++;
+    return st;
+}
+
+BFB_API int bfb_set_agent_constants(bfb_env env, int n, const int *voxel, const double *temp1, const double *temp2,
+                                    const uint8_t *active) {
+    int st = check_env(env);
+    if (st) return st;
+    if (n < 0) return fail(BFB_ERR_INVALID_ARG, "n < 0");
+    if (n > 0 && (!voxel || !temp1 || !temp2)) return fail(BFB_ERR_INVALID_ARG, "agent arrays must not be NULL");
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    st = agents_build_constants(env, n, voxel, temp1, temp2, active);
     env->epoch++;
     return st;
 }

@@ -40,16 +40,6 @@ struct DirFaces {
     int any;              // 0: no active face for any substrate
 };
 
-// Thomas factors of one axis on the device.
-//   den[m*S+d]: FP64 path: the reference's denominators (divided by);
-//               FP32 path: their reciprocals 1/den, computed in FP64, rounded once.
-//   cb[m*S+d]:  back-substitution coefficients c[m] (negative numbers).
-template <typename T>
-struct AxisFactors {
-    const T *den;
-    const T *cb;
-};
-
 // Bulk source/sink terms fused into the x-sweep load.
 //   A = S*T (rounded once), B = U + S (rounded once); rho <- (rho + dt*A) / (B*dt + 1)
 template <typename T>
@@ -92,9 +82,13 @@ struct bfb_env_s {
     bool factors_valid = false;
     double factor_dt = 0;
     int freeze_factors = 1;
-    void *fac_den[3] = {nullptr, nullptr, nullptr};
-    void *fac_cb[3] = {nullptr, nullptr, nullptr};
-    void *c1 = nullptr;                  // [S]
+    // per axis: tables [4][n*S] (FP64 uses 2: den, c; FP32 uses 4: 1/den hi,
+    // 1/den lo, c1/den, c) and tail values [4][S] for rows [m0, n-2]
+    void *fac_tab[3] = {nullptr, nullptr, nullptr};
+    void *fac_tail[3] = {nullptr, nullptr, nullptr};
+    int fac_m0[3] = {1, 1, 1};
+    void *c1 = nullptr;                  // [S] (FP64)
+    void *g = nullptr;                   // [2*S] (FP32): 1/(1 + c2) as hi, lo
 
     // Dirichlet
     std::vector<uint8_t> activation;     // [S]

@@ -10,41 +10,6 @@ constexpr int kMaxSmem = 227 * 1024;  // opt-in dynamic shared memory per CTA on
 constexpr int kChunks = 4;            // cp.async commit groups per strided tile
 
 // ---------------------------------------------------------------------------
-// Arithmetic. FP64 reproduces the reference build exactly: the fused
-// `u += c1*u_prev` / `u -= c*u_next` of g++ -ffp-contract=fast and the IEEE
-// division by the denominator (the library is compiled with --fmad=false so
-// nothing else is fused). FP32 multiplies by 1/den (computed in FP64, rounded
-// once) and uses FMAs throughout.
-// ---------------------------------------------------------------------------
-template <typename T>
-struct Arith;
-
-template <>
-struct Arith<double> {
-    static __device__ __forceinline__ double first(double x, double den) { return __ddiv_rn(x, den); }
-    static __device__ __forceinline__ double fwd(double x, double prev, double c1, double den) {
-        return __ddiv_rn(__fma_rn(c1, prev, x), den);
-    }
-    static __device__ __forceinline__ double back(double y, double next, double c) { return __fma_rn(-c, next, y); }
-    // BioFVM_microenvironment.cpp:1131-1148: (rho + dt*A) / ((B*dt) + 1), first product fused
-    static __device__ __forceinline__ double bulk(double r, double A, double B, double dt) {
-        return __ddiv_rn(__fma_rn(dt, A, r), __dadd_rn(__dmul_rn(B, dt), 1.0));
-    }
-};
-
-template <>
-struct Arith<float> {
-    static __device__ __forceinline__ float first(float x, float rden) { return __fmul_rn(x, rden); }
-    static __device__ __forceinline__ float fwd(float x, float prev, float c1, float rden) {
-        return __fmul_rn(__fmaf_rn(c1, prev, x), rden);
-    }
-    static __device__ __forceinline__ float back(float y, float next, float c) { return __fmaf_rn(-c, next, y); }
-    static __device__ __forceinline__ float bulk(float r, float A, float B, float dt) {
-        return __fdiv_rn(__fmaf_rn(dt, A, r), __fmaf_rn(B, dt, 1.0f));
-    }
-};
-
-// ---------------------------------------------------------------------------
 // cp.async helpers (LDGSTS: global -> shared without staging in registers)
 // ---------------------------------------------------------------------------
 template <int BYTES>
@@ -86,10 +51,246 @@ __device__ __forceinline__ bool on_active_face(unsigned m, int i, int j, int k, 
 }
 
 // ---------------------------------------------------------------------------
-// Strided sweep (x: axis 0, y: axis 1). One warp = one 32-column tile.
+// Bulk source/sink update (BioFVM_microenvironment.cpp:1131-1148):
+//   rho = (rho + dt*A) / ((B*dt) + 1) with A = S*T, B = U + S; the first
+//   product is fused as in the reference build.
 // ---------------------------------------------------------------------------
-template <typename T, int VB, bool FUSE_PRE>
-__global__ void sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
+__device__ __forceinline__ double bulk_update(double r, double A, double B, double dt) {
+    return __ddiv_rn(__fma_rn(dt, A, r), __dadd_rn(__dmul_rn(B, dt), 1.0));
+}
+__device__ __forceinline__ float bulk_update(float r, float A, float B, float dt) {
+    return __fdiv_rn(__fmaf_rn(dt, A, r), __fmaf_rn(B, dt, 1.0f));
+}
+
+// ---------------------------------------------------------------------------
+// One line, at line[m*ls] (m = 0..n-1), in shared or global memory.
+//   pre(m, x)   input transform (bulk / pre-sweep Dirichlet), identity otherwise
+//   out(m, y)   writes the result of row m (Dirichlet applied by the caller)
+//   ready(r)    called before row r is first read; lets the strided kernel
+//               wait for the cp.async group holding row r
+// The per-lane factor pointers are already offset by the substrate d. The
+// line pointer and stride are 64-bit so the global fallbacks can use it too.
+// ---------------------------------------------------------------------------
+struct LineFactors64 {
+    const double *den, *cb;
+    double den_t, cb_t, c1;
+    int S, m0;
+};
+
+template <class Pre, class Out, class Ready>
+__device__ __forceinline__ void solve_line(double *line, long long ls, int n, const LineFactors64 &F, Pre pre,
+                                           Out out, Ready ready) {
+    ready(0);
+    double prev = __ddiv_rn(pre(0, line[0]), F.den[0]);
+    line[0] = prev;
+    const int hb = min(F.m0, n - 1);  // head rows [1, hb) read the tables
+    for (int r = 1; r < hb; ++r) {
+        ready(r);
+        prev = __ddiv_rn(__fma_rn(F.c1, prev, pre(r, line[r * ls])), F.den[(size_t)r * F.S]);
+        line[r * ls] = prev;
+    }
+#pragma unroll 4
+    for (int r = max(hb, 1); r < n - 1; ++r) {  // tail rows use register factors
+        ready(r);
+        prev = __ddiv_rn(__fma_rn(F.c1, prev, pre(r, line[r * ls])), F.den_t);
+        line[r * ls] = prev;
+    }
+    if (n > 1) {
+        ready(n - 1);
+        prev = __ddiv_rn(__fma_rn(F.c1, prev, pre(n - 1, line[(n - 1) * ls])), F.den[(size_t)(n - 1) * F.S]);
+    }
+    double next = prev;
+    out(n - 1, next);
+    const int tl = max(F.m0, 0);
+#pragma unroll 4
+    for (int r = n - 2; r >= tl; --r) {
+        next = __fma_rn(-F.cb_t, next, line[r * ls]);
+        out(r, next);
+    }
+    for (int r = min(tl, n - 1) - 1; r >= 0; --r) {
+        next = __fma_rn(-F.cb[(size_t)r * F.S], next, line[r * ls]);
+        out(r, next);
+    }
+}
+
+struct LineFactors32 {
+    const float *rh, *rl, *a, *cb;
+    float rh_t, rl_t, a_t, cb_t;
+    float gh, gl;
+    int S, m0;
+};
+
+template <class Pre, class Out, class Ready>
+__device__ __forceinline__ void solve_line(float *line, long long ls, int n, const LineFactors32 &F, Pre pre, Out out,
+                                           Ready ready) {
+    ready(0);
+    const float xb = pre(0, line[0]);  // deviation reference: the line's first value
+    float p = 0.0f;                     // z_0 = (u_0 - xb)/den_0 = 0
+    line[0] = 0.0f;
+    const int hb = min(F.m0, n - 1);
+    for (int r = 1; r < hb; ++r) {
+        ready(r);
+        const float dlt = __fsub_rn(pre(r, line[r * ls]), xb);
+        const size_t q = (size_t)r * F.S;
+        p = __fmaf_rn(F.a[q], p, __fmaf_rn(dlt, F.rh[q], __fmul_rn(dlt, F.rl[q])));
+        line[r * ls] = p;
+    }
+#pragma unroll 4
+    for (int r = max(hb, 1); r < n - 1; ++r) {
+        ready(r);
+        const float dlt = __fsub_rn(pre(r, line[r * ls]), xb);
+        p = __fmaf_rn(F.a_t, p, __fmaf_rn(dlt, F.rh_t, __fmul_rn(dlt, F.rl_t)));
+        line[r * ls] = p;
+    }
+    if (n > 1) {
+        ready(n - 1);
+        const float dlt = __fsub_rn(pre(n - 1, line[(n - 1) * ls]), xb);
+        const size_t q = (size_t)(n - 1) * F.S;
+        p = __fmaf_rn(F.a[q], p, __fmaf_rn(dlt, F.rh[q], __fmul_rn(dlt, F.rl[q])));
+    }
+    // y = g*xb + z, with g*xb added as (hi, lo) around the deviation
+    float next = p;
+    out(n - 1, __fmaf_rn(xb, F.gh, __fmaf_rn(xb, F.gl, next)));
+    const int tl = max(F.m0, 0);
+#pragma unroll 4
+    for (int r = n - 2; r >= tl; --r) {
+        next = __fmaf_rn(-F.cb_t, next, line[r * ls]);
+        out(r, __fmaf_rn(xb, F.gh, __fmaf_rn(xb, F.gl, next)));
+    }
+    for (int r = min(tl, n - 1) - 1; r >= 0; --r) {
+        next = __fmaf_rn(-F.cb[(size_t)r * F.S], next, line[r * ls]);
+        out(r, __fmaf_rn(xb, F.gh, __fmaf_rn(xb, F.gl, next)));
+    }
+}
+
+__device__ __forceinline__ LineFactors64 line_factors(const SweepArgs<double> &a, int d) {
+    LineFactors64 F;
+    F.den = a.fac.t0 + d;
+    F.cb = a.fac.t1 + d;
+    F.S = a.S;
+    F.m0 = a.fac.m0;
+    F.c1 = a.c1[d];
+    F.den_t = a.fac.tail[d];
+    F.cb_t = a.fac.tail[a.S + d];
+    return F;
+}
+
+__device__ __forceinline__ LineFactors32 line_factors(const SweepArgs<float> &a, int d) {
+    LineFactors32 F;
+    F.rh = a.fac.t0 + d;
+    F.rl = a.fac.t1 + d;
+    F.a = a.fac.t2 + d;
+    F.cb = a.fac.t3 + d;
+    F.S = a.S;
+    F.m0 = a.fac.m0;
+    F.rh_t = a.fac.tail[d];
+    F.rl_t = a.fac.tail[a.S + d];
+    F.a_t = a.fac.tail[2 * a.S + d];
+    F.cb_t = a.fac.tail[3 * a.S + d];
+    F.gh = a.g[d];
+    F.gl = a.g[a.S + d];
+    return F;
+}
+
+// ---------------------------------------------------------------------------
+// Lean per-lane recurrences for the shared-memory kernels. fwd<TAIL> /
+// bwd<TAIL> read the factor tables only when TAIL is false (rows < m0 and the
+// last row); TAIL rows use the register copies.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct LineSolver;
+
+template <>
+struct LineSolver<double> {
+    const double *den, *cb;
+    double den_t, cb_t, c1;
+    int S;
+    double prev, next;
+    __device__ __forceinline__ LineSolver(const SweepArgs<double> &a, int d) {
+        den = a.fac.t0 + d;
+        cb = a.fac.t1 + d;
+        den_t = a.fac.tail[d];
+        cb_t = a.fac.tail[a.S + d];
+        c1 = a.c1[d];
+        S = a.S;
+    }
+    // returns the value stored for the backward pass
+    __device__ __forceinline__ double first(double x0) {
+        prev = __ddiv_rn(x0, den[0]);
+        return prev;
+    }
+    template <bool TAIL>
+    __device__ __forceinline__ double fwd(double x, int r) {
+        prev = __ddiv_rn(__fma_rn(c1, prev, x), TAIL ? den_t : den[(size_t)r * S]);
+        return prev;
+    }
+    __device__ __forceinline__ double out_last() {
+        next = prev;
+        return next;
+    }
+    template <bool TAIL>
+    __device__ __forceinline__ double bwd(double z, int r) {
+        next = __fma_rn(-(TAIL ? cb_t : cb[(size_t)r * S]), next, z);
+        return next;
+    }
+};
+
+template <>
+struct LineSolver<float> {
+    const float *rh, *rl, *a, *cb;
+    float rh_t, rl_t, a_t, cb_t, gh, gl;
+    int S;
+    float xb, p, next;
+    __device__ __forceinline__ LineSolver(const SweepArgs<float> &A, int d) {
+        rh = A.fac.t0 + d;
+        rl = A.fac.t1 + d;
+        a = A.fac.t2 + d;
+        cb = A.fac.t3 + d;
+        rh_t = A.fac.tail[d];
+        rl_t = A.fac.tail[A.S + d];
+        a_t = A.fac.tail[2 * A.S + d];
+        cb_t = A.fac.tail[3 * A.S + d];
+        gh = A.g[d];
+        gl = A.g[A.S + d];
+        S = A.S;
+    }
+    __device__ __forceinline__ float first(float x0) {
+        xb = x0;  // deviation reference; z_0 = (u_0 - xb)/den_0 = 0
+        p = 0.0f;
+        return 0.0f;
+    }
+    template <bool TAIL>
+    __device__ __forceinline__ float fwd(float x, int r) {
+        const float dlt = __fsub_rn(x, xb);
+        if (TAIL) {
+            p = __fmaf_rn(a_t, p, __fmaf_rn(dlt, rh_t, __fmul_rn(dlt, rl_t)));
+        } else {
+            const size_t q = (size_t)r * S;
+            p = __fmaf_rn(a[q], p, __fmaf_rn(dlt, rh[q], __fmul_rn(dlt, rl[q])));
+        }
+        return p;
+    }
+    __device__ __forceinline__ float y(float v) const { return __fmaf_rn(xb, gh, __fmaf_rn(xb, gl, v)); }
+    __device__ __forceinline__ float out_last() {
+        next = p;
+        return y(next);
+    }
+    template <bool TAIL>
+    __device__ __forceinline__ float bwd(float z, int r) {
+        next = __fmaf_rn(-(TAIL ? cb_t : cb[(size_t)r * S]), next, z);
+        return y(next);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Strided sweep (x: axis 0, y: axis 1). One warp = one 32-column tile.
+//   FUSE_PRE: x-sweep; applies the step's leading Dirichlet to rows 0 / n-1
+//   BULK:     x-sweep; applies the bulk source/sink update on load
+// The hot loops carry no Dirichlet test: rows 0 and n-1 are peeled, and a
+// column lying wholly on an active face is overwritten after its solve.
+// ---------------------------------------------------------------------------
+template <typename T, int VB, bool FUSE_PRE, bool BULK>
+__global__ void __launch_bounds__(128) sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -99,11 +300,13 @@ __global__ void sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
     const long long col0 = (tile % g.ncb) * 32;
     const int ncols = (int)min((long long)32, g.P - col0);
     const int n = g.n;
+    const long long P = g.P;
     T *__restrict__ sm = reinterpret_cast<T *>(smem_raw) + (size_t)warp * n * 32;
     T *__restrict__ base = a.f + (size_t)slab * g.slab_stride + col0;
 
     // ---- stage the tile: kChunks commit groups of rows
     const int crow = (n + kChunks - 1) / kChunks;
+    const int nch = (n + crow - 1) / crow;  // non-empty groups
     constexpr int EPV = VB / (int)sizeof(T);  // elements per copy
     const bool vec = (VB > (int)sizeof(T)) && ncols == 32;
 #pragma unroll 1
@@ -114,17 +317,27 @@ __global__ void sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
             const int total = (r1 - r0) * VPR;
             for (int v = lane; v < total; v += 32) {
                 const int r = r0 + v / VPR, q = (v % VPR) * EPV;
-                cp_async<VB>(sm + r * 32 + q, base + (size_t)r * g.P + q);
+                cp_async<VB>(sm + r * 32 + q, base + (size_t)r * P + q);
             }
         } else if (lane < ncols) {
-            for (int r = r0; r < r1; ++r) cp_async<sizeof(T)>(sm + r * 32 + lane, base + (size_t)r * g.P + lane);
+            for (int r = r0; r < r1; ++r) cp_async<sizeof(T)>(sm + r * 32 + lane, base + (size_t)r * P + lane);
         }
         cp_commit();
+    }
+    // Group ch has landed for the whole warp after wait(ch). Every lane takes
+    // the same nch waits: one lane's 16-byte copies fill rows other lanes read.
+    auto wait = [&](int ch) {
+        cp_wait_dyn(kChunks - 1 - ch);
+        __syncwarp();
+    };
+    const bool valid = lane < ncols;
+    if (!valid) {
+        for (int ch = 0; ch < nch; ++ch) wait(ch);
+        return;
     }
 
     // ---- line coordinates of this lane
     const long long col = col0 + lane;
-    const bool valid = lane < ncols;
     const int S = a.S;
     const int d = (int)(col % S);
     int ci, cj, ck;  // voxel coordinates with the line coordinate left at 0
@@ -138,99 +351,7 @@ __global__ void sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
         ci = slab;
         cj = 0;
     }
-    unsigned m = 0;
-    if (a.dir.any && valid) m = a.dir.mask[d];
-    bool col_dir, lo_dir, hi_dir;
-    if (g.axis == 0) {
-        col_dir = ((m & 4u) && cj == 0) || ((m & 8u) && cj == a.ny - 1) || ((m & 16u) && ck == 0) ||
-                  ((m & 32u) && ck == a.nz - 1);
-        lo_dir = m & 1u;
-        hi_dir = m & 2u;
-    } else {
-        col_dir = ((m & 1u) && ci == 0) || ((m & 2u) && ci == a.nx - 1) || ((m & 16u) && ck == 0) ||
-                  ((m & 32u) && ck == a.nz - 1);
-        lo_dir = m & 4u;
-        hi_dir = m & 8u;
-    }
-    const T c1 = valid ? a.c1[d] : T(0);
-    const T *__restrict__ den = a.fac.den + d;
-    const T *__restrict__ cb = a.fac.cb + d;
-    auto vox_dir = [&](int mm) -> T {
-        return g.axis == 0 ? dir_value(a.dir, mm, cj, ck, d) : dir_value(a.dir, ci, mm, ck, d);
-    };
-
-    // ---- forward elimination in shared memory, chunk by chunk as copies land
-    T prev = T(0);
-#pragma unroll 1
-    for (int ch = 0; ch < kChunks; ++ch) {
-        cp_wait_dyn(kChunks - 1 - ch);
-        __syncwarp();
-        const int r0 = min(n, ch * crow), r1 = min(n, r0 + crow);
-        if (valid) {
-            int r = r0;
-            if (r == 0 && r1 > 0) {
-                T x = sm[lane];
-                if (FUSE_PRE) {
-                    if (a.bulk.on) x = Arith<T>::bulk(x, a.bulk.A[(size_t)slab * g.slab_stride + col],
-                                                      a.bulk.B[(size_t)slab * g.slab_stride + col], a.bulk.dt);
-                    if (lo_dir) x = vox_dir(0);
-                    if (hi_dir && n == 1) x = vox_dir(0);
-                }
-                prev = Arith<T>::first(x, den[0]);
-                sm[lane] = prev;
-                r = 1;
-            }
-#pragma unroll 4
-            for (; r < r1; ++r) {
-                T x = sm[r * 32 + lane];
-                if (FUSE_PRE) {
-                    if (a.bulk.on) {
-                        const size_t e = (size_t)slab * g.slab_stride + (size_t)r * g.P + col;
-                        x = Arith<T>::bulk(x, a.bulk.A[e], a.bulk.B[e], a.bulk.dt);
-                    }
-                    if (r == n - 1 && hi_dir) x = vox_dir(r);
-                }
-                prev = Arith<T>::fwd(x, prev, c1, den[(size_t)r * S]);
-                sm[r * 32 + lane] = prev;
-            }
-        }
-    }
-    if (!valid) return;
-
-    // ---- back substitution, Dirichlet on the store, straight to global memory
-    T next = prev;
-    base[(size_t)(n - 1) * g.P + lane] = (col_dir || hi_dir || (lo_dir && n == 1)) ? vox_dir(n - 1) : next;
-#pragma unroll 4
-    for (int r = n - 2; r >= 0; --r) {
-        const T y = sm[r * 32 + lane];
-        next = Arith<T>::back(y, next, cb[(size_t)r * S]);
-        base[(size_t)r * g.P + lane] = (col_dir || (r == 0 && lo_dir)) ? vox_dir(r) : next;
-    }
-}
-
-// Fallback for lines too long for shared memory: thread per line, the forward
-// pass writes its intermediate values back to the field (two reads and two
-// writes per sweep).
-template <typename T, bool FUSE_PRE>
-__global__ void sweep_strided_global_kernel(SweepArgs<T> a, StridedGeom g) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)g.n_slabs * g.P) return;
-    const int slab = (int)(t / g.P);
-    const long long col = t % g.P;
-    const int S = a.S, n = g.n;
-    const int d = (int)(col % S);
-    int ci, cj, ck;
-    if (g.axis == 0) {
-        const long long q = col / S;
-        ck = (int)(q % a.nz);
-        cj = (int)(q / a.nz);
-        ci = 0;
-    } else {
-        ck = (int)(col / S);
-        ci = slab;
-        cj = 0;
-    }
-    unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
+    const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
     bool col_dir, lo_dir, hi_dir;
     if (g.axis == 0) {
         col_dir = ((m & 4u) && cj == 0) || ((m & 8u) && cj == a.ny - 1) || ((m & 16u) && ck == 0) ||
@@ -246,34 +367,75 @@ __global__ void sweep_strided_global_kernel(SweepArgs<T> a, StridedGeom g) {
     auto vox_dir = [&](int mm) -> T {
         return g.axis == 0 ? dir_value(a.dir, mm, cj, ck, d) : dir_value(a.dir, ci, mm, ck, d);
     };
-    T *base = a.f + (size_t)slab * g.slab_stride + col;
-    const T c1 = a.c1[d];
-    T prev = T(0);
-    for (int r = 0; r < n; ++r) {
-        T x = base[(size_t)r * g.P];
-        if (FUSE_PRE) {
-            if (a.bulk.on) {
-                const size_t e = (size_t)slab * g.slab_stride + (size_t)r * g.P + col;
-                x = Arith<T>::bulk(x, a.bulk.A[e], a.bulk.B[e], a.bulk.dt);
-            }
-            if ((r == 0 && lo_dir) || (r == n - 1 && hi_dir)) x = vox_dir(r);
-        }
-        prev = r == 0 ? Arith<T>::first(x, a.fac.den[d]) : Arith<T>::fwd(x, prev, c1, a.fac.den[(size_t)r * S + d]);
-        base[(size_t)r * g.P] = prev;
+    const T *bA = nullptr, *bB = nullptr;
+    if constexpr (BULK) {
+        bA = a.bulk.A + (size_t)slab * g.slab_stride + col;
+        bB = a.bulk.B + (size_t)slab * g.slab_stride + col;
     }
-    T next = prev;
-    base[(size_t)(n - 1) * g.P] = (col_dir || hi_dir || (lo_dir && n == 1)) ? vox_dir(n - 1) : next;
-    for (int r = n - 2; r >= 0; --r) {
-        next = Arith<T>::back(base[(size_t)r * g.P], next, a.fac.cb[(size_t)r * S + d]);
-        base[(size_t)r * g.P] = (col_dir || (r == 0 && lo_dir)) ? vox_dir(r) : next;
+    auto load = [&](int r) -> T {
+        T x = sm[r * 32 + lane];
+        if constexpr (BULK) x = bulk_update(x, bA[(size_t)r * P], bB[(size_t)r * P], a.bulk.dt);
+        return x;
+    };
+
+    LineSolver<T> L(a, d);
+    const int m0 = a.fac.m0;
+
+    // ---- forward elimination in shared memory, group by group as copies land
+    wait(0);
+    {
+        T x0 = load(0);
+        if (FUSE_PRE && (lo_dir || (hi_dir && n == 1))) x0 = vox_dir(0);
+        sm[lane] = L.first(x0);
     }
+    int r = 1;
+    for (int ch = 0; ch < nch; ++ch) {
+        if (ch > 0) wait(ch);
+        const int rend = min(n - 1, (ch + 1) * crow);
+        const int hend = min(rend, m0);
+        for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(load(r), r);
+#pragma unroll 8
+        for (; r < rend; ++r) sm[r * 32 + lane] = L.template fwd<true>(load(r), r);
+    }
+    if (n > 1) {
+        T x = load(n - 1);
+        if (FUSE_PRE && hi_dir) x = vox_dir(n - 1);
+        L.template fwd<false>(x, n - 1);
+    }
+
+    // ---- back substitution straight to global memory
+    T *gp = base + lane + (size_t)(n - 1) * P;
+    {
+        T y = L.out_last();
+        if (hi_dir || (lo_dir && n == 1)) y = vox_dir(n - 1);
+        *gp = y;
+    }
+    const int tl = max(m0, 1);
+    r = n - 2;
+#pragma unroll 8
+    for (; r >= tl; --r) {
+        gp -= P;
+        *gp = L.template bwd<true>(sm[r * 32 + lane], r);
+    }
+    for (; r >= 1; --r) {
+        gp -= P;
+        *gp = L.template bwd<false>(sm[r * 32 + lane], r);
+    }
+    if (n > 1) {
+        T y = L.template bwd<false>(sm[lane], 0);
+        if (lo_dir) y = vox_dir(0);
+        gp -= P;
+        *gp = y;
+    }
+    if (col_dir)  // the whole column is on an active face of another axis
+        for (int q = 0; q < n; ++q) base[lane + (size_t)q * P] = vox_dir(q);
 }
 
 // ---------------------------------------------------------------------------
 // Contiguous sweep (z). One warp = R consecutive (i,j) rows of nz*S elements.
 // ---------------------------------------------------------------------------
 template <typename T, int VB>
-__global__ void sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
+__global__ void __launch_bounds__(128) sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -301,6 +463,7 @@ __global__ void sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
     }
 
     // ---- lane (r, d) solves line (row0 + r, d) in place
+    const int m0 = a.fac.m0;
     for (int t = lane; t < nr * S; t += 32) {
         const int r = t / S, d = t - r * S;
         const long long row = row0 + r;
@@ -310,23 +473,29 @@ __global__ void sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
                               ((m & 8u) && j == a.ny - 1);
         const bool lo_dir = m & 16u, hi_dir = m & 32u;
         T *line = sm + (size_t)r * g.RS + d;
-        const T c1 = a.c1[d];
-        const T *__restrict__ den = a.fac.den + d;
-        const T *__restrict__ cb = a.fac.cb + d;
-        T prev = Arith<T>::first(line[0], den[0]);
-        line[0] = prev;
-#pragma unroll 4
-        for (int k = 1; k < nz; ++k) {
-            prev = Arith<T>::fwd(line[k * S], prev, c1, den[(size_t)k * S]);
-            line[k * S] = prev;
+        LineSolver<T> Ls(a, d);
+        line[0] = Ls.first(line[0]);
+        const int hend = min(nz - 1, m0);
+        int k = 1;
+        for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(line[k * S], k);
+#pragma unroll 8
+        for (; k < nz - 1; ++k) line[k * S] = Ls.template fwd<true>(line[k * S], k);
+        if (nz > 1) Ls.template fwd<false>(line[(nz - 1) * S], nz - 1);
+        {
+            const T y = Ls.out_last();  // also seeds the back substitution
+            line[(nz - 1) * S] = (hi_dir || (lo_dir && nz == 1)) ? dir_value(a.dir, i, j, nz - 1, d) : y;
         }
-        T next = prev;
-        if (line_dir || hi_dir || (lo_dir && nz == 1)) line[(nz - 1) * S] = dir_value(a.dir, i, j, nz - 1, d);
-#pragma unroll 4
-        for (int k = nz - 2; k >= 0; --k) {
-            next = Arith<T>::back(line[k * S], next, cb[(size_t)k * S]);
-            line[k * S] = (line_dir || (k == 0 && lo_dir)) ? dir_value(a.dir, i, j, k, d) : next;
+        const int tl = max(m0, 1);
+        k = nz - 2;
+#pragma unroll 8
+        for (; k >= tl; --k) line[k * S] = Ls.template bwd<true>(line[k * S], k);
+        for (; k >= 1; --k) line[k * S] = Ls.template bwd<false>(line[k * S], k);
+        if (nz > 1) {
+            const T y = Ls.template bwd<false>(line[0], 0);
+            line[0] = lo_dir ? dir_value(a.dir, i, j, 0, d) : y;
         }
+        if (line_dir)
+            for (int q = 0; q < nz; ++q) line[q * S] = dir_value(a.dir, i, j, q, d);
     }
     __syncwarp();
 
@@ -349,7 +518,66 @@ __global__ void sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
     }
 }
 
-// Fallback for rows too long for shared memory: thread per (row, d).
+// ---------------------------------------------------------------------------
+// Fallbacks for lines too long for shared memory: thread per line, the line
+// read and written in place in global memory (the forward pass stores its
+// intermediate values, so two reads and two writes per sweep).
+// ---------------------------------------------------------------------------
+template <typename T, bool FUSE_PRE>
+__global__ void sweep_strided_global_kernel(SweepArgs<T> a, StridedGeom g) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)g.n_slabs * g.P) return;
+    const int slab = (int)(t / g.P);
+    const long long col = t % g.P;
+    const int S = a.S, n = g.n;
+    const int d = (int)(col % S);
+    int ci, cj, ck;
+    if (g.axis == 0) {
+        const long long q = col / S;
+        ck = (int)(q % a.nz);
+        cj = (int)(q / a.nz);
+        ci = 0;
+    } else {
+        ck = (int)(col / S);
+        ci = slab;
+        cj = 0;
+    }
+    const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
+    bool col_dir, lo_dir, hi_dir;
+    if (g.axis == 0) {
+        col_dir = ((m & 4u) && cj == 0) || ((m & 8u) && cj == a.ny - 1) || ((m & 16u) && ck == 0) ||
+                  ((m & 32u) && ck == a.nz - 1);
+        lo_dir = m & 1u;
+        hi_dir = m & 2u;
+    } else {
+        col_dir = ((m & 1u) && ci == 0) || ((m & 2u) && ci == a.nx - 1) || ((m & 16u) && ck == 0) ||
+                  ((m & 32u) && ck == a.nz - 1);
+        lo_dir = m & 4u;
+        hi_dir = m & 8u;
+    }
+    auto vox_dir = [&](int mm) -> T {
+        return g.axis == 0 ? dir_value(a.dir, mm, cj, ck, d) : dir_value(a.dir, ci, mm, ck, d);
+    };
+    T *line = a.f + (size_t)slab * g.slab_stride + col;
+    const long long P = g.P;
+    auto pre = [&](int r, T x) -> T {
+        if constexpr (FUSE_PRE) {
+            if (a.bulk.on) {
+                const size_t e = (size_t)slab * g.slab_stride + (size_t)r * P + col;
+                x = bulk_update(x, a.bulk.A[e], a.bulk.B[e], a.bulk.dt);
+            }
+            if ((r == 0 && lo_dir) || (r == n - 1 && hi_dir)) x = vox_dir(r);
+        }
+        return x;
+    };
+    auto out = [&](int r, T y) {
+        if (col_dir || (r == 0 && lo_dir) || (r == n - 1 && hi_dir)) y = vox_dir(r);
+        line[(size_t)r * P] = y;
+    };
+    auto ready = [](int) {};
+    solve_line(line, P, n, line_factors(a, d), pre, out, ready);
+}
+
 template <typename T>
 __global__ void sweep_contig_global_kernel(SweepArgs<T> a, long long nrows) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -363,19 +591,13 @@ __global__ void sweep_contig_global_kernel(SweepArgs<T> a, long long nrows) {
                           ((m & 8u) && j == a.ny - 1);
     const bool lo_dir = m & 16u, hi_dir = m & 32u;
     T *line = a.f + (size_t)row * nz * S + d;
-    const T c1 = a.c1[d];
-    T prev = Arith<T>::first(line[0], a.fac.den[d]);
-    line[0] = prev;
-    for (int k = 1; k < nz; ++k) {
-        prev = Arith<T>::fwd(line[(size_t)k * S], prev, c1, a.fac.den[(size_t)k * S + d]);
-        line[(size_t)k * S] = prev;
-    }
-    T next = prev;
-    if (line_dir || hi_dir || (lo_dir && nz == 1)) line[(size_t)(nz - 1) * S] = dir_value(a.dir, i, j, nz - 1, d);
-    for (int k = nz - 2; k >= 0; --k) {
-        next = Arith<T>::back(line[(size_t)k * S], next, a.fac.cb[(size_t)k * S + d]);
-        line[(size_t)k * S] = (line_dir || (k == 0 && lo_dir)) ? dir_value(a.dir, i, j, k, d) : next;
-    }
+    auto pre = [](int, T x) -> T { return x; };
+    auto out = [&](int k, T y) {
+        if (line_dir || (k == 0 && lo_dir) || (k == nz - 1 && hi_dir)) y = dir_value(a.dir, i, j, k, d);
+        line[(size_t)k * S] = y;
+    };
+    auto ready = [](int) {};
+    solve_line(line, S, nz, line_factors(a, d), pre, out, ready);
 }
 
 // ---------------------------------------------------------------------------
@@ -419,7 +641,7 @@ __global__ void dirichlet_kernel(SweepArgs<T> a) {
 template <typename T>
 __global__ void bulk_kernel(T *f, const T *A, const T *B, T dt, long long N) {
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (long long)gridDim.x * blockDim.x)
-        f[e] = Arith<T>::bulk(f[e], A[e], B[e], dt);
+        f[e] = bulk_update(f[e], A[e], B[e], dt);
 }
 
 // ---------------------------------------------------------------------------
@@ -445,10 +667,12 @@ size_t contig_smem(int nz, int S, int elem, int warps, int *R, int *RS) {
 
 template <typename T, int VB, bool FP>
 static int go_strided(const SweepArgs<T> &a, const StridedGeom &g, int warps, size_t smem, cudaStream_t s) {
-    auto k = sweep_strided_kernel<T, VB, FP>;
     const long long tiles = (long long)g.n_slabs * g.ncb;
     const long long blocks = (tiles + warps - 1) / warps;
-    k<<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
+    if (FP && a.bulk.on)
+        sweep_strided_kernel<T, VB, FP, FP><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
+    else
+        sweep_strided_kernel<T, VB, FP, false><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
 }
@@ -469,7 +693,9 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, cu
         g.n_slabs = a.nx;
     }
     g.ncb = (int)((g.P + 31) / 32);
-    const size_t smem = strided_smem(g.n, sizeof(T), warps);
+    warps = std::max(1, std::min(warps, 4));
+    size_t smem = strided_smem(g.n, sizeof(T), warps);
+    while (smem == 0 && warps > 1) smem = strided_smem(g.n, sizeof(T), --warps);
     if (smem == 0) {
         const long long threads = (long long)g.n_slabs * g.P;
         const unsigned blocks = (unsigned)((threads + 127) / 128);
@@ -492,10 +718,9 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, cu
 
 template <typename T, int VB>
 static int go_contig(const SweepArgs<T> &a, const ContigGeom &g, int warps, size_t smem, cudaStream_t s) {
-    auto k = sweep_contig_kernel<T, VB>;
     const long long tiles = (g.nrows + g.R - 1) / g.R;
     const long long blocks = (tiles + warps - 1) / warps;
-    k<<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
+    sweep_contig_kernel<T, VB><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
 }
@@ -505,7 +730,9 @@ int launch_contig(const SweepArgs<T> &a, int warps, cudaStream_t s) {
     ContigGeom g;
     g.nz = a.nz;
     g.nrows = (long long)a.nx * a.ny;
-    const size_t smem = contig_smem(a.nz, a.S, sizeof(T), warps, &g.R, &g.RS);
+    warps = std::max(1, std::min(warps, 4));
+    size_t smem = contig_smem(a.nz, a.S, sizeof(T), warps, &g.R, &g.RS);
+    while (smem == 0 && warps > 1) smem = contig_smem(a.nz, a.S, sizeof(T), --warps, &g.R, &g.RS);
     if (smem == 0) {
         const long long threads = g.nrows * a.S;
         sweep_contig_global_kernel<T><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, g.nrows);
@@ -540,6 +767,13 @@ int launch_bulk(const SweepArgs<T> &a, long long N, cudaStream_t s) {
 
 // Opt every shared-memory kernel into the full 227 KB once per device, before
 // any launch (so that nothing configures a kernel inside a stream capture).
+template <typename K>
+static void opt_in(K k) {
+    cudaFuncSetAttribute((const void *)k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+}
+
 void sweeps_prepare_device() {
     static std::mutex mu;
     static unsigned long long done = 0;  // one bit per device
@@ -547,20 +781,23 @@ void sweeps_prepare_device() {
     if (cudaGetDevice(&dev) != cudaSuccess) return;
     std::lock_guard<std::mutex> lock(mu);
     if (done & (1ull << (dev & 63))) return;
-    const int b = kMaxSmem;
-    cudaFuncSetAttribute(sweep_strided_kernel<double, 16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_strided_kernel<double, 16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_strided_kernel<double, 8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_strided_kernel<double, 8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_strided_kernel<float, 16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_strided_kernel<float, 16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_strided_kernel<float, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_strided_kernel<float, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_contig_kernel<double, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_contig_kernel<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_contig_kernel<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_contig_kernel<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(sweep_contig_kernel<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    opt_in(sweep_strided_kernel<double, 16, true, true>);
+    opt_in(sweep_strided_kernel<double, 16, true, false>);
+    opt_in(sweep_strided_kernel<double, 16, false, false>);
+    opt_in(sweep_strided_kernel<double, 8, true, true>);
+    opt_in(sweep_strided_kernel<double, 8, true, false>);
+    opt_in(sweep_strided_kernel<double, 8, false, false>);
+    opt_in(sweep_strided_kernel<float, 16, true, true>);
+    opt_in(sweep_strided_kernel<float, 16, true, false>);
+    opt_in(sweep_strided_kernel<float, 16, false, false>);
+    opt_in(sweep_strided_kernel<float, 4, true, true>);
+    opt_in(sweep_strided_kernel<float, 4, true, false>);
+    opt_in(sweep_strided_kernel<float, 4, false, false>);
+    opt_in(sweep_contig_kernel<double, 16>);
+    opt_in(sweep_contig_kernel<double, 8>);
+    opt_in(sweep_contig_kernel<float, 16>);
+    opt_in(sweep_contig_kernel<float, 8>);
+    opt_in(sweep_contig_kernel<float, 4>);
     done |= 1ull << (dev & 63);
 }
 

@@ -3,8 +3,8 @@
 // One LOD step of the reference (BioFVM_parallel.cpp:693-1395) is
 //     Dir, X-sweep, Dir, Y-sweep, Dir, Z-sweep, Dir
 // where every sweep solves, for each grid line and substrate, the symmetric
-// tridiagonal system tridiag(-c1, diag, -c1) y = u with precomputed Thomas
-// factors (forward: y0 = u0/den0, ym = (um + c1*y(m-1))/den_m; back:
+// tridiagonal system A y = u, A = tridiag(-c1, diag, -c1), with precomputed
+// Thomas factors (forward: y0 = u0/den0, ym = (um + c1*y(m-1))/den_m; back:
 // ym -= c_m * y(m+1)), and Dir overwrites the active outer faces.
 //
 // Field layout rho[((i*ny + j)*nz + k)*S + d]: z (with d) is contiguous, x is
@@ -25,10 +25,51 @@
 // on that sweep's store. Because Dir is a pure overwrite of fixed positions
 // and each sweep rewrites every element of its line, this is exactly the
 // reference's sequence. The recurrence keeps the un-overwritten values.
+//
+// Factor tails: den_m and c_m converge to a floating-point fixed point after a
+// few rows (den_m = c3 - c1^2/den_(m-1) contracts by (c1/den)^2 < 1/4), so
+// every table is bitwise constant on rows [m0, n-2]. The host finds m0 per axis
+// and the kernels keep those values in registers; only rows < m0 and row n-1
+// read the tables. This is exact, not an approximation.
+//
+// Arithmetic:
+//   FP64 -- the reference's operations in its order, bit for bit: the fused
+//     u += c1*u_prev and u -= c*u_next of its -ffp-contract=fast build and an
+//     IEEE division by den_m.
+//   FP32 -- FP32 storage and FP32 arithmetic, in "deviation" form. With
+//     xb = u_0 of the line and g = 1/(1 + c2), A*1 = (1 + c2)*1 exactly (every
+//     row of A sums to 1 + c2), so  A^{-1} u = g*xb + A^{-1}(u - xb).
+//     The recurrence runs on u - xb with the reciprocal form
+//     z_m = (u_m - xb)*r_m + a_m*z_(m-1)  (r = 1/den, a = c1/den), r and g
+//     carried as hi+lo FP32 pairs. Rounding of the coefficients then acts only
+//     on the deviation, which smooths out as the field diffuses, instead of on
+//     the whole field, which makes plain FP32 Thomas drift ~1e-4 in 1000 steps.
 #pragma once
 #include "bfb_internal.cuh"
 
 namespace bfb {
+
+// Per-axis factor tables on the device (see bfb_capi.cu: upload_factors).
+//   FP64: t0 = den, t1 = c (back-substitution coefficient)
+//   FP32: t0 = 1/den (hi), t1 = 1/den (lo), t2 = c1/den, t3 = c
+// tail[q*S + d] = value of table q on rows [m0, n-2] (valid when m0 <= n-2).
+template <typename T>
+struct Factors {
+    const T *t0, *t1, *t2, *t3;
+    const T *tail;
+    int m0;
+};
+
+template <typename T>
+struct SweepArgs {
+    T *f;
+    int nx, ny, nz, S;
+    Factors<T> fac;
+    const T *c1;   // FP64: [S] c1 = dt*D/dx^2
+    const T *g;    // FP32: [2*S] g = 1/(1 + c2) as hi, lo
+    DirFaces<T> dir;
+    BulkTerms<T> bulk;
+};
 
 struct StridedGeom {
     int n;                 // line length
@@ -46,16 +87,6 @@ struct ContigGeom {
     int RS;                // shared-memory row stride (elements), RS = S (mod 32)
 };
 
-template <typename T>
-struct SweepArgs {
-    T *f;
-    int nx, ny, nz, S;
-    AxisFactors<T> fac;
-    const T *c1;           // [S]
-    DirFaces<T> dir;
-    BulkTerms<T> bulk;
-};
-
 // launchers (bfb_sweeps.cu)
 template <typename T>
 int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, cudaStream_t s);
@@ -69,5 +100,8 @@ int launch_bulk(const SweepArgs<T> &a, long long N, cudaStream_t s);
 // shared-memory bytes a strided / contiguous CTA needs (0 if it does not fit)
 size_t strided_smem(int n, int elem, int warps);
 size_t contig_smem(int nz, int S, int elem, int warps, int *R, int *RS);
+
+// Opt the shared-memory kernels into 227 KB, once per device.
+void sweeps_prepare_device();
 
 }  // namespace bfb

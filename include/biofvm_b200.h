@@ -147,6 +147,14 @@ BFB_API int bfb_bulk_step(bfb_env env, double dt);
 BFB_API int bfb_set_agents(bfb_env env, int n, const double *pos, const double *volume,
                            const double *secretion, const double *uptake,
                            const double *saturation, const uint8_t *active, double dt);
+/* Agents from the state a Basic_Agent caches: current_voxel_index (n), and
+ * cell_source_sink_solver_temp1/temp2 (n*S) of set_internal_uptake_constants
+ * (BioFVM_basic_agent.cpp:155-176), in list order; active n flags or NULL.
+ * Used by callers that keep the reference's agent objects and their lazily
+ * refreshed constants (the C++ facade does). Voxels of active agents must lie
+ * in [0, V). */
+BFB_API int bfb_set_agent_constants(bfb_env env, int n, const int *voxel, const double *temp1,
+                                    const double *temp2, const uint8_t *active);
 /* current_voxel_index of each agent (list order). */
 BFB_API int bfb_agent_voxels(bfb_env env, int *out);
 BFB_API int bfb_cells_step(bfb_env env, double dt);
