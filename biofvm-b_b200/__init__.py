@@ -31,6 +31,7 @@ STEP_DIFFUSION = 2
 STEP_CELLS = 4
 OPT_FREEZE_FACTORS = 1
 OPT_USE_GRAPHS = 2
+OPT_USE_TMA = 3
 
 ERRORS = {
     -1: "BFB_ERR_INVALID_ARG",

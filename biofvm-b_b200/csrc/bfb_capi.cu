@@ -94,7 +94,7 @@ static int tail_start(const std::vector<std::vector<double>> &tabs, int n, int S
 }
 
 // The device tables for one axis from the reference's factors (den, c).
-//   FP64: den and c as they are.
+//   FP64: den and c as they are, and RN(1/den) for the division (div_rcp).
 //   FP32: 1/den as a hi+lo pair of floats, c1/den and c rounded once; the
 //         deviation form of the FP32 kernels (bfb_sweeps.cuh) needs no c1.
 static int upload_factors(bfb_env_s *env, int axis, int n, const std::vector<double> &den,
@@ -103,7 +103,9 @@ static int upload_factors(bfb_env_s *env, int axis, int n, const std::vector<dou
     const size_t nS = (size_t)n * S;
     std::vector<std::vector<double>> tabs;
     if (env->precision == BFB_FP64) {
-        tabs = {den, c};
+        std::vector<double> rcp(nS);
+        for (size_t q = 0; q < nS; ++q) rcp[q] = 1.0 / den[q];
+        tabs = {den, c, rcp};
     } else {
         std::vector<double> rh(nS), rl(nS), a(nS), cf(nS);
         for (int m = 0; m < n; ++m)
@@ -196,18 +198,25 @@ static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
     a.bulk.B = static_cast<const T *>(env->bulkB);
     a.bulk.dt = (T)dt;
     a.bulk.on = bulk && env->bulk_on;
+    a.err = env->d_err;
     return a;
+}
+
+static const CUtensorMap *tma_map(bfb_env_s *env, int axis) {
+    return (env->use_tma && env->tma_ok[axis]) ? &env->tmap[axis] : nullptr;
 }
 
 // One LOD diffusion step; `bulk` fuses a preceding bulk source/sink update
 // into the x-sweep load.
 template <typename T>
 static int run_diffusion(bfb_env_s *env, double dt, bool bulk, cudaStream_t s) {
-    int st = launch_strided<T>(make_args<T>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, s);
+    int st = launch_strided<T>(make_args<T>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, tma_map(env, 0),
+                               env->tma_crow[0], s);
     if (st) return st;
-    st = launch_strided<T>(make_args<T>(env, 1, false, dt), 1, false, env->tuning.warps_y, s);
+    st = launch_strided<T>(make_args<T>(env, 1, false, dt), 1, false, env->tuning.warps_y, tma_map(env, 1),
+                           env->tma_crow[1], s);
     if (st) return st;
-    return launch_contig<T>(make_args<T>(env, 2, false, dt), env->tuning.warps_z, s);
+    return launch_contig<T>(make_args<T>(env, 2, false, dt), env->tuning.warps_z, env->use_tma != 0, s);
 }
 
 template <typename T>
@@ -320,6 +329,15 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
     alloc(&env->c1, env->elem * n_substrates);
     alloc(&env->g, env->elem * 2 * n_substrates);
     alloc((void **)&env->d_mask, n_substrates);
+    alloc((void **)&env->d_err, sizeof(int));
+    if (!st) {
+        cudaError_t e = cudaMemset(env->d_err, 0, sizeof(int));
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemset");
+    }
+    if (!st)
+        for (int a = 0; a < 2; ++a)
+            env->tma_ok[a] = make_sweep_tensor_map(&env->tmap[a], &env->tma_crow[a], env->field, (int)env->elem, a,
+                                                   nx, ny, nz, n_substrates);
     if (!st) {
         cudaError_t e = cudaStreamCreateWithFlags(&env->own_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaStreamCreateWithFlags");
@@ -377,6 +395,7 @@ BFB_API int bfb_destroy(bfb_env env) {
     cudaFree(env->bulkA);
     cudaFree(env->bulkB);
     cudaFree(env->partials);
+    cudaFree(env->d_err);
     if (env->own_stream) cudaStreamDestroy(env->own_stream);
     delete env;
     return BFB_OK;
@@ -412,16 +431,29 @@ BFB_API int bfb_set_option(bfb_env env, int option, int value) {
         env->use_graphs = value != 0;
         drop_graph(env);
         break;
+    case BFB_OPT_USE_TMA:
+        env->use_tma = value != 0;
+        drop_graph(env);
+        break;
     default: return fail(BFB_ERR_INVALID_ARG, "unknown option");
     }
+    return BFB_OK;
+}
+
+// The device error flag is sticky: once a kernel's bounded wait ran out, the
+// env's field is not trustworthy and every later synchronize reports it.
+static int check_device_error(bfb_env_s *env) {
+    int flag = 0;
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    BFB_CUDA(cudaMemcpy(&flag, env->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) return fail(BFB_ERR_WATCHDOG, "a device-side wait ran out of its iteration limit (data movement stalled)");
     return BFB_OK;
 }
 
 BFB_API int bfb_synchronize(bfb_env env) {
     int st = check_env(env);
     if (st) return st;
-    BFB_CUDA(cudaStreamSynchronize(env->stream));
-    return BFB_OK;
+    return check_device_error(env);
 }
 
 BFB_API int bfb_set_coefficients(bfb_env env, const double *D, const double *lambda) {
@@ -466,8 +498,7 @@ BFB_API int bfb_get_field(bfb_env env, double *host) {
         if ((st = launch_convert_f2d((const float *)env->field, (double *)env->staging, env->N, env->stream))) return st;
         BFB_CUDA(cudaMemcpyAsync(host, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, env->stream));
     }
-    BFB_CUDA(cudaStreamSynchronize(env->stream));
-    return BFB_OK;
+    return check_device_error(env);
 }
 
 BFB_API int bfb_set_field_raw(bfb_env env, const void *host) {
@@ -752,18 +783,24 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
         if (flags & BFB_STEP_DIFFUSION) {
             const bool bulk = (flags & BFB_STEP_BULK) != 0;
             st = phase_ms(0, [&] {
-                return fp64 ? launch_strided<double>(make_args<double>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, s)
-                            : launch_strided<float>(make_args<float>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, s);
+                return fp64 ? launch_strided<double>(make_args<double>(env, 0, bulk, dt), 0, true, env->tuning.warps_x,
+                                                     tma_map(env, 0), env->tma_crow[0], s)
+                            : launch_strided<float>(make_args<float>(env, 0, bulk, dt), 0, true, env->tuning.warps_x,
+                                                    tma_map(env, 0), env->tma_crow[0], s);
             });
             if (!st)
                 st = phase_ms(1, [&] {
-                    return fp64 ? launch_strided<double>(make_args<double>(env, 1, false, dt), 1, false, env->tuning.warps_y, s)
-                                : launch_strided<float>(make_args<float>(env, 1, false, dt), 1, false, env->tuning.warps_y, s);
+                    return fp64 ? launch_strided<double>(make_args<double>(env, 1, false, dt), 1, false,
+                                                         env->tuning.warps_y, tma_map(env, 1), env->tma_crow[1], s)
+                                : launch_strided<float>(make_args<float>(env, 1, false, dt), 1, false,
+                                                        env->tuning.warps_y, tma_map(env, 1), env->tma_crow[1], s);
                 });
             if (!st)
                 st = phase_ms(2, [&] {
-                    return fp64 ? launch_contig<double>(make_args<double>(env, 2, false, dt), env->tuning.warps_z, s)
-                                : launch_contig<float>(make_args<float>(env, 2, false, dt), env->tuning.warps_z, s);
+                    return fp64 ? launch_contig<double>(make_args<double>(env, 2, false, dt), env->tuning.warps_z,
+                                                        env->use_tma != 0, s)
+                                : launch_contig<float>(make_args<float>(env, 2, false, dt), env->tuning.warps_z,
+                                                       env->use_tma != 0, s);
                 });
         } else if (flags & BFB_STEP_BULK) {
             st = phase_ms(3, [&] {

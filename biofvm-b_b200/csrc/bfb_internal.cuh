@@ -1,6 +1,7 @@
 // bfb_internal.cuh -- shared types of the B200 diffusion-decay library.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -123,4 +124,14 @@ struct bfb_env_s {
     uint64_t epoch = 1;
 
     bfb::SweepTuning tuning;
+
+    // TMA: tensor maps of the field for the x and y sweeps (made at creation
+    // when the grid meets TMA's alignment rules), and the switch
+    int use_tma = 1;
+    CUtensorMap tmap[2];
+    int tma_crow[2] = {0, 0};
+    int tma_ok[2] = {0, 0};
+
+    // sticky device error flag (a bounded wait in a kernel ran out)
+    int *d_err = nullptr;
 };

@@ -1,66 +1,12 @@
 // bfb_sweeps.cu -- Thomas sweep kernels (see bfb_sweeps.cuh for the design).
 #include "bfb_sweeps.cuh"
+#include "bfb_line.cuh"
 
 #include <algorithm>
 #include <mutex>
 
 namespace bfb {
 
-constexpr int kMaxSmem = 227 * 1024;  // opt-in dynamic shared memory per CTA on sm_100a
-constexpr int kChunks = 4;            // cp.async commit groups per strided tile
-
-// ---------------------------------------------------------------------------
-// cp.async helpers (LDGSTS: global -> shared without staging in registers)
-// ---------------------------------------------------------------------------
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
-    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    if constexpr (BYTES == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-__device__ __forceinline__ void cp_wait_dyn(int pending) {
-    switch (pending) {
-    case 0: cp_wait<0>(); break;
-    case 1: cp_wait<1>(); break;
-    case 2: cp_wait<2>(); break;
-    default: cp_wait<3>(); break;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Dirichlet lookups
-// ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ T dir_value(const DirFaces<T> &F, int i, int j, int k, int d) {
-    if (i == 0) return F.face[0][((size_t)j * F.nz + k) * F.S + d];
-    if (i == F.nx - 1) return F.face[1][((size_t)j * F.nz + k) * F.S + d];
-    if (j == 0) return F.face[2][((size_t)i * F.nz + k) * F.S + d];
-    if (j == F.ny - 1) return F.face[3][((size_t)i * F.nz + k) * F.S + d];
-    if (k == 0) return F.face[4][((size_t)i * F.ny + j) * F.S + d];
-    return F.face[5][((size_t)i * F.ny + j) * F.S + d];
-}
-
-__device__ __forceinline__ bool on_active_face(unsigned m, int i, int j, int k, int nx, int ny, int nz) {
-    return ((m & 1u) && i == 0) || ((m & 2u) && i == nx - 1) || ((m & 4u) && j == 0) ||
-           ((m & 8u) && j == ny - 1) || ((m & 16u) && k == 0) || ((m & 32u) && k == nz - 1);
-}
-
-// ---------------------------------------------------------------------------
-// Bulk source/sink update (BioFVM_microenvironment.cpp:1131-1148):
-//   rho = (rho + dt*A) / ((B*dt) + 1) with A = S*T, B = U + S; the first
-//   product is fused as in the reference build.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double bulk_update(double r, double A, double B, double dt) {
-    return __ddiv_rn(__fma_rn(dt, A, r), __dadd_rn(__dmul_rn(B, dt), 1.0));
-}
-__device__ __forceinline__ float bulk_update(float r, float A, float B, float dt) {
-    return __fdiv_rn(__fmaf_rn(dt, A, r), __fmaf_rn(B, dt, 1.0f));
-}
 
 // ---------------------------------------------------------------------------
 // One line, at line[m*ls] (m = 0..n-1), in shared or global memory.
@@ -72,8 +18,8 @@ __device__ __forceinline__ float bulk_update(float r, float A, float B, float dt
 // line pointer and stride are 64-bit so the global fallbacks can use it too.
 // ---------------------------------------------------------------------------
 struct LineFactors64 {
-    const double *den, *cb;
-    double den_t, cb_t, c1;
+    const double *den, *cb, *rcp;
+    double den_t, cb_t, rcp_t, c1;
     int S, m0;
 };
 
@@ -81,23 +27,25 @@ template <class Pre, class Out, class Ready>
 __device__ __forceinline__ void solve_line(double *line, long long ls, int n, const LineFactors64 &F, Pre pre,
                                            Out out, Ready ready) {
     ready(0);
-    double prev = __ddiv_rn(pre(0, line[0]), F.den[0]);
+    double prev = div_rcp(pre(0, line[0]), F.den[0], F.rcp[0]);
     line[0] = prev;
     const int hb = min(F.m0, n - 1);  // head rows [1, hb) read the tables
     for (int r = 1; r < hb; ++r) {
         ready(r);
-        prev = __ddiv_rn(__fma_rn(F.c1, prev, pre(r, line[r * ls])), F.den[(size_t)r * F.S]);
+        const size_t q = (size_t)r * F.S;
+        prev = div_rcp(__fma_rn(F.c1, prev, pre(r, line[r * ls])), F.den[q], F.rcp[q]);
         line[r * ls] = prev;
     }
 #pragma unroll 4
     for (int r = max(hb, 1); r < n - 1; ++r) {  // tail rows use register factors
         ready(r);
-        prev = __ddiv_rn(__fma_rn(F.c1, prev, pre(r, line[r * ls])), F.den_t);
+        prev = div_rcp(__fma_rn(F.c1, prev, pre(r, line[r * ls])), F.den_t, F.rcp_t);
         line[r * ls] = prev;
     }
     if (n > 1) {
         ready(n - 1);
-        prev = __ddiv_rn(__fma_rn(F.c1, prev, pre(n - 1, line[(n - 1) * ls])), F.den[(size_t)(n - 1) * F.S]);
+        const size_t q = (size_t)(n - 1) * F.S;
+        prev = div_rcp(__fma_rn(F.c1, prev, pre(n - 1, line[(n - 1) * ls])), F.den[q], F.rcp[q]);
     }
     double next = prev;
     out(n - 1, next);
@@ -167,11 +115,13 @@ __device__ __forceinline__ LineFactors64 line_factors(const SweepArgs<double> &a
     LineFactors64 F;
     F.den = a.fac.t0 + d;
     F.cb = a.fac.t1 + d;
+    F.rcp = a.fac.t2 + d;
     F.S = a.S;
     F.m0 = a.fac.m0;
     F.c1 = a.c1[d];
     F.den_t = a.fac.tail[d];
     F.cb_t = a.fac.tail[a.S + d];
+    F.rcp_t = a.fac.tail[2 * a.S + d];
     return F;
 }
 
@@ -191,96 +141,6 @@ __device__ __forceinline__ LineFactors32 line_factors(const SweepArgs<float> &a,
     F.gl = a.g[a.S + d];
     return F;
 }
-
-// ---------------------------------------------------------------------------
-// Lean per-lane recurrences for the shared-memory kernels. fwd<TAIL> /
-// bwd<TAIL> read the factor tables only when TAIL is false (rows < m0 and the
-// last row); TAIL rows use the register copies.
-// ---------------------------------------------------------------------------
-template <typename T>
-struct LineSolver;
-
-template <>
-struct LineSolver<double> {
-    const double *den, *cb;
-    double den_t, cb_t, c1;
-    int S;
-    double prev, next;
-    __device__ __forceinline__ LineSolver(const SweepArgs<double> &a, int d) {
-        den = a.fac.t0 + d;
-        cb = a.fac.t1 + d;
-        den_t = a.fac.tail[d];
-        cb_t = a.fac.tail[a.S + d];
-        c1 = a.c1[d];
-        S = a.S;
-    }
-    // returns the value stored for the backward pass
-    __device__ __forceinline__ double first(double x0) {
-        prev = __ddiv_rn(x0, den[0]);
-        return prev;
-    }
-    template <bool TAIL>
-    __device__ __forceinline__ double fwd(double x, int r) {
-        prev = __ddiv_rn(__fma_rn(c1, prev, x), TAIL ? den_t : den[(size_t)r * S]);
-        return prev;
-    }
-    __device__ __forceinline__ double out_last() {
-        next = prev;
-        return next;
-    }
-    template <bool TAIL>
-    __device__ __forceinline__ double bwd(double z, int r) {
-        next = __fma_rn(-(TAIL ? cb_t : cb[(size_t)r * S]), next, z);
-        return next;
-    }
-};
-
-template <>
-struct LineSolver<float> {
-    const float *rh, *rl, *a, *cb;
-    float rh_t, rl_t, a_t, cb_t, gh, gl;
-    int S;
-    float xb, p, next;
-    __device__ __forceinline__ LineSolver(const SweepArgs<float> &A, int d) {
-        rh = A.fac.t0 + d;
-        rl = A.fac.t1 + d;
-        a = A.fac.t2 + d;
-        cb = A.fac.t3 + d;
-        rh_t = A.fac.tail[d];
-        rl_t = A.fac.tail[A.S + d];
-        a_t = A.fac.tail[2 * A.S + d];
-        cb_t = A.fac.tail[3 * A.S + d];
-        gh = A.g[d];
-        gl = A.g[A.S + d];
-        S = A.S;
-    }
-    __device__ __forceinline__ float first(float x0) {
-        xb = x0;  // deviation reference; z_0 = (u_0 - xb)/den_0 = 0
-        p = 0.0f;
-        return 0.0f;
-    }
-    template <bool TAIL>
-    __device__ __forceinline__ float fwd(float x, int r) {
-        const float dlt = __fsub_rn(x, xb);
-        if (TAIL) {
-            p = __fmaf_rn(a_t, p, __fmaf_rn(dlt, rh_t, __fmul_rn(dlt, rl_t)));
-        } else {
-            const size_t q = (size_t)r * S;
-            p = __fmaf_rn(a[q], p, __fmaf_rn(dlt, rh[q], __fmul_rn(dlt, rl[q])));
-        }
-        return p;
-    }
-    __device__ __forceinline__ float y(float v) const { return __fmaf_rn(xb, gh, __fmaf_rn(xb, gl, v)); }
-    __device__ __forceinline__ float out_last() {
-        next = p;
-        return y(next);
-    }
-    template <bool TAIL>
-    __device__ __forceinline__ float bwd(float z, int r) {
-        next = __fmaf_rn(-(TAIL ? cb_t : cb[(size_t)r * S]), next, z);
-        return y(next);
-    }
-};
 
 // ---------------------------------------------------------------------------
 // Strided sweep (x: axis 0, y: axis 1). One warp = one 32-column tile.
@@ -678,7 +538,8 @@ static int go_strided(const SweepArgs<T> &a, const StridedGeom &g, int warps, si
 }
 
 template <typename T>
-int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, cudaStream_t s) {
+int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map, int crow,
+                   cudaStream_t s) {
     StridedGeom g;
     g.axis = axis;
     if (axis == 0) {
@@ -694,6 +555,10 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, cu
     }
     g.ncb = (int)((g.P + 31) / 32);
     warps = std::max(1, std::min(warps, 4));
+    if (map) {
+        const int st = launch_strided_tma<T>(a, g, map, crow, fuse_pre, warps, s);
+        if (st != kNotApplicable) return st;
+    }
     size_t smem = strided_smem(g.n, sizeof(T), warps);
     while (smem == 0 && warps > 1) smem = strided_smem(g.n, sizeof(T), --warps);
     if (smem == 0) {
@@ -726,7 +591,7 @@ static int go_contig(const SweepArgs<T> &a, const ContigGeom &g, int warps, size
 }
 
 template <typename T>
-int launch_contig(const SweepArgs<T> &a, int warps, cudaStream_t s) {
+int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s) {
     ContigGeom g;
     g.nz = a.nz;
     g.nrows = (long long)a.nx * a.ny;
@@ -742,6 +607,10 @@ int launch_contig(const SweepArgs<T> &a, int warps, cudaStream_t s) {
     const long long L = (long long)a.nz * a.S;
     const bool base16 = (reinterpret_cast<uintptr_t>(a.f) & 15) == 0;
     const int eb = (int)sizeof(T);
+    if (use_tma && base16 && (L * eb) % 16 == 0 && ((long long)g.RS * eb) % 16 == 0 && (L * eb) * g.R < (1 << 20)) {
+        const int st = launch_contig_tma<T>(a, g, warps, s);
+        if (st != kNotApplicable) return st;
+    }
     if (base16 && (L * eb) % 16 == 0 && ((long long)g.RS * eb) % 16 == 0) return go_contig<T, 16>(a, g, warps, smem, s);
     if (eb < 8 && (L * eb) % 8 == 0 && ((long long)g.RS * eb) % 8 == 0) return go_contig<T, 8>(a, g, warps, smem, s);
     return go_contig<T, (int)sizeof(T)>(a, g, warps, smem, s);
@@ -798,13 +667,14 @@ void sweeps_prepare_device() {
     opt_in(sweep_contig_kernel<float, 16>);
     opt_in(sweep_contig_kernel<float, 8>);
     opt_in(sweep_contig_kernel<float, 4>);
+    tma_prepare_device();
     done |= 1ull << (dev & 63);
 }
 
-template int launch_strided<double>(const SweepArgs<double> &, int, bool, int, cudaStream_t);
-template int launch_strided<float>(const SweepArgs<float> &, int, bool, int, cudaStream_t);
-template int launch_contig<double>(const SweepArgs<double> &, int, cudaStream_t);
-template int launch_contig<float>(const SweepArgs<float> &, int, cudaStream_t);
+template int launch_strided<double>(const SweepArgs<double> &, int, bool, int, const CUtensorMap *, int, cudaStream_t);
+template int launch_strided<float>(const SweepArgs<float> &, int, bool, int, const CUtensorMap *, int, cudaStream_t);
+template int launch_contig<double>(const SweepArgs<double> &, int, bool, cudaStream_t);
+template int launch_contig<float>(const SweepArgs<float> &, int, bool, cudaStream_t);
 template int launch_dirichlet<double>(const SweepArgs<double> &, cudaStream_t);
 template int launch_dirichlet<float>(const SweepArgs<float> &, cudaStream_t);
 template int launch_bulk<double>(const SweepArgs<double> &, long long, cudaStream_t);

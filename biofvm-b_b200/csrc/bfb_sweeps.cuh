@@ -34,8 +34,9 @@
 //
 // Arithmetic:
 //   FP64 -- the reference's operations in its order, bit for bit: the fused
-//     u += c1*u_prev and u -= c*u_next of its -ffp-contract=fast build and an
-//     IEEE division by den_m.
+//     u += c1*u_prev and u -= c*u_next of its -ffp-contract=fast build and a
+//     correctly rounded division by den_m (reciprocal + one residual
+//     correction, see div_rcp in bfb_sweeps.cu).
 //   FP32 -- FP32 storage and FP32 arithmetic, in "deviation" form. With
 //     xb = u_0 of the line and g = 1/(1 + c2), A*1 = (1 + c2)*1 exactly (every
 //     row of A sums to 1 + c2), so  A^{-1} u = g*xb + A^{-1}(u - xb).
@@ -50,7 +51,7 @@
 namespace bfb {
 
 // Per-axis factor tables on the device (see bfb_capi.cu: upload_factors).
-//   FP64: t0 = den, t1 = c (back-substitution coefficient)
+//   FP64: t0 = den, t1 = c (back-substitution coefficient), t2 = RN(1/den)
 //   FP32: t0 = 1/den (hi), t1 = 1/den (lo), t2 = c1/den, t3 = c
 // tail[q*S + d] = value of table q on rows [m0, n-2] (valid when m0 <= n-2).
 template <typename T>
@@ -69,6 +70,7 @@ struct SweepArgs {
     const T *g;    // FP32: [2*S] g = 1/(1 + c2) as hi, lo
     DirFaces<T> dir;
     BulkTerms<T> bulk;
+    int *err;      // device error flag: bounded waits that run out set bit 0
 };
 
 struct StridedGeom {
@@ -87,11 +89,25 @@ struct ContigGeom {
     int RS;                // shared-memory row stride (elements), RS = S (mod 32)
 };
 
-// launchers (bfb_sweeps.cu)
+// launchers (bfb_sweeps.cu). `map` (may be NULL) is the field's tensor map
+// for this axis; with it the TMA kernels run, otherwise cp.async ones.
 template <typename T>
-int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, cudaStream_t s);
+int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map, int crow,
+                   cudaStream_t s);
 template <typename T>
-int launch_contig(const SweepArgs<T> &a, int warps, cudaStream_t s);
+int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s);
+
+// TMA kernels (bfb_tma.cu); they return kNotApplicable when the tile does
+// not fit in shared memory, and the caller then takes another kernel.
+constexpr int kNotApplicable = 1;
+template <typename T>
+int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map, int crow, bool fuse_pre,
+                       int warps, cudaStream_t s);
+template <typename T>
+int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s);
+bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
+                           int S);
+void tma_prepare_device();
 template <typename T>
 int launch_dirichlet(const SweepArgs<T> &a, cudaStream_t s);
 template <typename T>

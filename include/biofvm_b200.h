@@ -62,6 +62,8 @@ typedef struct bfb_env_s *bfb_env;
                                     and kept, as BioFVM_parallel.cpp:714,913 does; 0: recomputed
                                     whenever dt differs from the cached one */
 #define BFB_OPT_USE_GRAPHS 2     /* 1 (default): bfb_simulate replays a captured CUDA graph */
+#define BFB_OPT_USE_TMA 3        /* 1 (default): sweeps move data with the TMA engine where the
+                                    grid's row pitch allows; 0: cp.async kernels everywhere */
 
 /* bfb_simulate flags: per step, in the order of examples/3D_tumor_example_X.cpp:346-348 */
 #define BFB_STEP_BULK 1

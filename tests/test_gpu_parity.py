@@ -29,9 +29,10 @@ def rel_linf(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-def make_env(bfb, rho, D, lam, prec, dx=20.0):
+def make_env(bfb, rho, D, lam, prec, dx=20.0, tma=1):
     nx, ny, nz, S = rho.shape
     env = bfb.Env((nx, ny, nz), S, dx=dx, precision=prec)
+    env.set_option(bfb.OPT_USE_TMA, tma)
     env.set_coefficients(D, lam)
     env.set_field(rho)
     return env
@@ -62,11 +63,12 @@ def test_multi_golden(bfb, name):
     assert np.array_equal(env.get_field(), g["out"])
 
 
-def test_bulk_golden_standalone_and_fused(bfb):
+@pytest.mark.parametrize("tma", [1, 0], ids=["tma", "cpasync"])
+def test_bulk_golden_standalone_and_fused(bfb, tma):
     g = golden("bulk_9x8x7_S3")
     dt = float(g["dt"])
     for fused in (False, True):
-        env = make_env(bfb, g["rho0"], g["D"], g["lam"], bfb.FP64, float(g["dx"]))
+        env = make_env(bfb, g["rho0"], g["D"], g["lam"], bfb.FP64, float(g["dx"]), tma=tma)
         env.set_bulk(g["S_rate"], g["T_target"], g["U_rate"])
         if fused:
             env.simulate(dt, 3, bfb.STEP_BULK | bfb.STEP_DIFFUSION)
@@ -75,6 +77,26 @@ def test_bulk_golden_standalone_and_fused(bfb):
                 env.bulk_step(dt)
                 env.diffusion_step(dt, 1)
         assert np.array_equal(env.get_field(), g["out"]), f"fused={fused}"
+
+
+@pytest.mark.parametrize("tma", [1, 0], ids=["tma", "cpasync"])
+def test_bulk_fused_aligned_grid(bfb, oracle, rng, tma):
+    """Bulk fused into the x-sweep load on a grid whose rows suit TMA."""
+    shape, S = (16, 12, 8), 4
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    rho0 = rng.random((*shape, S))
+    Sr, Tt, Ur = rng.random((3, *shape, S)) * 4.0
+    vals = rng.random((*shape, S)) * 5
+    act = np.array([1, 0, 1, 1], np.uint8)
+    env = make_env(bfb, rho0, D, lam, bfb.FP64, tma=tma)
+    env.set_dirichlet(act, values=vals)
+    env.set_bulk(Sr, Tt, Ur)
+    env.simulate(0.01, 3, bfb.STEP_BULK | bfb.STEP_DIFFUSION)
+    want = rho0
+    for _ in range(3):
+        want = oracle.bulk_step(want, 0.01, Sr, Tt, Ur)
+        want = oracle.lod_steps(want, 0.01, 20.0, D, lam, 1, vals, face_mask_all(act))
+    assert np.array_equal(env.get_field(), want)
 
 
 def test_agents_golden(bfb):
@@ -115,27 +137,29 @@ SHAPES = [((1, 1, 1), 1), ((1, 4, 6), 2), ((2, 3, 1), 3), ((3, 2, 2), 1), ((5, 1
           ((40, 3, 64), 7)]
 
 
+@pytest.mark.parametrize("tma", [1, 0], ids=["tma", "cpasync"])
 @pytest.mark.parametrize("shape,S", SHAPES)
-def test_random_shapes_fp64_bitexact(bfb, oracle, rng, shape, S):
+def test_random_shapes_fp64_bitexact(bfb, oracle, rng, shape, S, tma):
     D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
     rho0 = rng.random((*shape, S))
     vals = rng.random((*shape, S)) * 30
     act = (rng.random(S) < 0.7).astype(np.uint8)
     fm = (rng.random((6, S)) < 0.6).astype(np.uint8)  # per-face mask (extension)
-    env = make_env(bfb, rho0, D, lam, bfb.FP64)
+    env = make_env(bfb, rho0, D, lam, bfb.FP64, tma=tma)
     env.set_dirichlet(act, values=vals, face_mask=fm)
     env.diffusion_step(0.01, 3)
     want = oracle.lod_steps(rho0, 0.01, 20.0, D, lam, 3, vals, fm * act[None, :])
     assert np.array_equal(env.get_field(), want)
 
 
+@pytest.mark.parametrize("tma", [1, 0], ids=["tma", "cpasync"])
 @pytest.mark.parametrize("shape,S", SHAPES)
-def test_random_shapes_fp32(bfb, oracle, rng, shape, S):
+def test_random_shapes_fp32(bfb, oracle, rng, shape, S, tma):
     D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
     rho0 = rng.random((*shape, S))
     vals = rng.random((*shape, S)) * 30
     act = (rng.random(S) < 0.7).astype(np.uint8)
-    env = make_env(bfb, rho0, D, lam, bfb.FP32)
+    env = make_env(bfb, rho0, D, lam, bfb.FP32, tma=tma)
     env.set_dirichlet(act, values=vals)
     env.diffusion_step(0.01, 5)
     want = oracle.lod_steps(rho0, 0.01, 20.0, D, lam, 5, vals, face_mask_all(act))
