@@ -53,9 +53,9 @@ struct BulkTerms {
 
 // Launch configuration chosen by the autotuner (or defaults).
 struct SweepTuning {
-    int warps_x = 2;   // warps per CTA of the strided kernels (x and y)
-    int warps_y = 2;
-    int warps_z = 2;   // warps per CTA of the contiguous kernel (z)
+    int warps_x = 1;   // warps per CTA of the strided kernels (x and y); one warp
+    int warps_y = 1;   // per CTA packs shared memory tightest
+    int warps_z = 1;   // warps per CTA of the contiguous kernel (z)
 };
 
 }  // namespace bfb

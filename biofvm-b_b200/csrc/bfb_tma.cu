@@ -317,6 +317,121 @@ __global__ void __launch_bounds__(128) sweep_contig_tma_kernel(SweepArgs<T> a, C
 }
 
 // ---------------------------------------------------------------------------
+// Contiguous z sweep, pipelined: the tile's k range is cut into row groups of
+// kc rows; group c of every row is one bulk copy on mbarrier c, so the
+// forward elimination starts on group 0 while the later groups land, and the
+// back substitution stores each finished group while the lower ones are
+// still being computed. SC is the substrate count when it is a compile-time
+// constant (1, 2, 4, 8), 0 otherwise; every lane owns at most one line
+// (S <= 32 gives R = 32/S rows per warp).
+// ---------------------------------------------------------------------------
+template <typename T, int SC>
+__global__ void __launch_bounds__(128) sweep_contig_pipe_kernel(SweepArgs<T> a, ContigGeom g, int kc) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    const long long row0 = tile * g.R;
+    if (row0 >= g.nrows) return;
+    const int nr = (int)min((long long)g.R, g.nrows - row0);
+    const int S = SC > 0 ? SC : a.S;
+    const int nz = g.nz;
+    const int L = nz * S;
+    const int nch = (nz + kc - 1) / kc;
+    const size_t wbytes = (128 + (size_t)g.R * g.RS * sizeof(T) + 127) / 128 * 128;
+    unsigned char *wbase = smem_raw + (size_t)warp * wbytes;
+    const unsigned bar0 = smem_u32(wbase);
+    T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
+    T *__restrict__ base = a.f + (size_t)row0 * L;
+    auto seg_bytes = [&](int c) -> unsigned { return (unsigned)((min(nz, (c + 1) * kc) - c * kc) * S * (int)sizeof(T)); };
+
+    if (lane == 0) {
+        for (int c = 0; c < nch; ++c) mbar_init(bar0 + 8 * c, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    if (lane == 0) {
+        for (int c = 0; c < nch; ++c) {
+            const unsigned b = seg_bytes(c);
+            mbar_expect_tx(bar0 + 8 * c, b * (unsigned)nr);
+            for (int r = 0; r < nr; ++r)
+                bulk_load(smem_u32(sm + (size_t)r * g.RS + (size_t)c * kc * S), base + (size_t)r * L + (size_t)c * kc * S,
+                          b, bar0 + 8 * c);
+        }
+    }
+    auto wait_c = [&](int c) -> bool {
+        if (mbar_wait(bar0 + 8 * c, 0)) return true;
+        if (lane == 0) atomicOr(a.err, 1);
+        return false;
+    };
+
+    const bool active = lane < nr * S;
+    const int r = active ? lane / S : 0;
+    const int d = active ? lane - r * S : 0;
+    const long long row = row0 + r;
+    const int i = (int)(row / a.ny), j = (int)(row % a.ny);
+    const unsigned m = (a.dir.any && active) ? a.dir.mask[d] : 0u;
+    const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
+                          ((m & 8u) && j == a.ny - 1);
+    const bool lo_dir = m & 16u, hi_dir = m & 32u;
+    T *line = sm + (size_t)r * g.RS + d;
+    LineSolver<T> Ls(a, d);
+    const int m0 = a.fac.m0;
+
+    // ---- forward
+    if (!wait_c(0)) return;
+    if (active) line[0] = Ls.first(line[0]);
+    int k = 1;
+    for (int c = 0; c < nch; ++c) {
+        if (c > 0 && !wait_c(c)) return;
+        const int kend = min(nz - 1, (c + 1) * kc);
+        if (active) {
+            const int hend = min(kend, m0);
+            for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(line[k * S], k);
+#pragma unroll 8
+            for (; k < kend; ++k) line[k * S] = Ls.template fwd<true>(line[k * S], k);
+        }
+        k = max(k, kend);
+    }
+    if (active && nz > 1) Ls.template fwd<false>(line[(nz - 1) * S], nz - 1);
+
+    // ---- backward; each finished row group is stored for all rows of the tile
+    if (active) {
+        const T y = Ls.out_last();  // also seeds the back substitution
+        line[(nz - 1) * S] = (hi_dir || (lo_dir && nz == 1)) ? dir_value(a.dir, i, j, nz - 1, d) : y;
+    }
+    const int tl = max(m0, 1);
+    k = nz - 2;
+    for (int c = nch - 1; c >= 0; --c) {
+        const int klo = c * kc;
+        if (active) {
+            const int tstop = max(klo, tl);
+#pragma unroll 8
+            for (; k >= tstop; --k) line[k * S] = Ls.template bwd<true>(line[k * S], k);
+            const int hstop = max(klo, 1);
+            for (; k >= hstop; --k) line[k * S] = Ls.template bwd<false>(line[k * S], k);
+            if (klo == 0 && nz > 1) {
+                const T y = Ls.template bwd<false>(line[0], 0);
+                line[0] = lo_dir ? dir_value(a.dir, i, j, 0, d) : y;
+            }
+            if (line_dir)
+                for (int q = klo; q < min(nz, klo + kc); ++q) line[q * S] = dir_value(a.dir, i, j, q, d);
+        }
+        k = min(k, klo - 1);
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+            const unsigned b = seg_bytes(c);
+            for (int q = 0; q < nr; ++q)
+                bulk_store(base + (size_t)q * L + (size_t)klo * S, smem_u32(sm + (size_t)q * g.RS + (size_t)klo * S), b);
+            bulk_commit();
+        }
+    }
+    if (lane == 0) bulk_wait_read_all();
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -345,7 +460,24 @@ int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cud
     if (wb * warps > (size_t)kMaxSmem) return kNotApplicable;
     const long long tiles = (g.nrows + g.R - 1) / g.R;
     const unsigned blocks = (unsigned)((tiles + warps - 1) / warps);
-    sweep_contig_tma_kernel<T><<<blocks, warps * 32, wb * warps, s>>>(a, g);
+    const size_t smem = wb * warps;
+    if (a.S <= 32) {
+        // row groups of kc k-rows whose byte length keeps every copy 16-byte aligned
+        const int eb = (int)sizeof(T);
+        int q = 16;
+        for (int v = a.S * eb; v % 2 == 0 && q > 1; v /= 2) q /= 2;  // q = 16 / gcd(16, S*elem)
+        int kc = (g.nz + kChunks - 1) / kChunks;
+        kc = (kc + q - 1) / q * q;
+        switch (a.S) {
+        case 1: sweep_contig_pipe_kernel<T, 1><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        case 2: sweep_contig_pipe_kernel<T, 2><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        case 4: sweep_contig_pipe_kernel<T, 4><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        case 8: sweep_contig_pipe_kernel<T, 8><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        default: sweep_contig_pipe_kernel<T, 0><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        }
+    } else {
+        sweep_contig_tma_kernel<T><<<blocks, warps * 32, smem, s>>>(a, g);
+    }
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
 }
@@ -371,6 +503,16 @@ void tma_prepare_device() {
     opt_in_tma(sweep_strided_tma_kernel<float, true, true>);
     opt_in_tma(sweep_strided_tma_kernel<float, true, false>);
     opt_in_tma(sweep_strided_tma_kernel<float, false, false>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 1>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 2>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 4>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 8>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 0>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 1>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 2>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 4>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 8>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 0>);
     opt_in_tma(sweep_contig_tma_kernel<double>);
     opt_in_tma(sweep_contig_tma_kernel<float>);
 }
