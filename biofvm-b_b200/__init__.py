@@ -50,7 +50,7 @@ EXPORTS = [
     "bfb_get_field", "bfb_set_field_raw", "bfb_get_field_raw", "bfb_field_device_ptr", "bfb_set_dirichlet",
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
-    "bfb_checksum",
+    "bfb_checksum", "bfb_checksum_noalloc",
 ]
 
 
@@ -105,6 +105,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_step_host": [_vp, _vp, ctypes.c_double, ctypes.c_int],
         "bfb_profile_steps": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp],
         "bfb_checksum": [_vp, _dp],
+        "bfb_checksum_noalloc": [_vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, _vp, _vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

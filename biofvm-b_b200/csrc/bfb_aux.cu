@@ -341,4 +341,17 @@ int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s) {
     return BFB_OK;
 }
 
+// Checksum kernels on caller-provided scratch: `partials` holds at least
+// nblocks*S doubles; out_dev receives S doubles. Launches only, no allocation.
+int launch_checksum_raw(const void *field, int precision, long long V, int S, double *partials, int nblocks,
+                        double *out_dev, cudaStream_t s) {
+    if (precision == BFB_FP64)
+        checksum_partial_kernel<double><<<nblocks, kSumThreads, 0, s>>>((const double *)field, V, S, partials);
+    else
+        checksum_partial_kernel<float><<<nblocks, kSumThreads, 0, s>>>((const float *)field, V, S, partials);
+    checksum_final_kernel<<<1, kMaxSumS, 0, s>>>(partials, nblocks, S, out_dev);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+
 }  // namespace bfb

@@ -180,6 +180,24 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
 /* Per-substrate FP64 sum of the field over all voxels (mass checksum). */
 BFB_API int bfb_checksum(bfb_env env, double *out);
 
+/* No counterpart in the reference. The per-substrate FP64 sums of
+ * bfb_checksum for callers that must not allocate device memory -- for
+ * example code that owns its device buffers in its own pool, or a host loop
+ * with other streams in flight, which cudaMalloc/cudaFree would stall by
+ * synchronizing the device. The field is given directly: field_dev is a device
+ * array of n_voxels*n_substrates elements in the reference layout, of
+ * `precision` (BFB_FP64 / BFB_FP32); out_dev receives n_substrates doubles in
+ * device memory. Work is queued on `stream` (NULL: the legacy default stream)
+ * and the call returns without waiting. Its scratch is a fixed array inside
+ * the library, so at most BFB_NOALLOC_MAX_SUBSTRATES substrates (larger counts
+ * return BFB_ERR_SIZE), and calls that overlap on the GPU share that array and
+ * race: order them on one stream. The first call on each device looks the
+ * array's device address up (cudaGetSymbolAddress); make that first call
+ * before capturing a stream. The call allocates nothing. */
+#define BFB_NOALLOC_MAX_SUBSTRATES 64
+BFB_API int bfb_checksum_noalloc(const void *field_dev, int precision, long long n_voxels, int n_substrates,
+                                 double *out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
