@@ -34,13 +34,16 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parent
-NX = NY = NZ = 256
+NX = NY = NZ = 256  # the benchmark grid; --grid / --substrates resize it for profiling small cases
 S = 8
 DT = 0.01
 DX = 20.0
 SEED = 2026
-METRIC = "voxel*substrate updates/s per LOD step (256^3 voxels x 8 substrates)"
 UNIT = "voxel*substrate updates/s"
+
+
+def metric_name():
+    return f"voxel*substrate updates/s per LOD step ({NX}^3 voxels x {S} substrates)"
 
 
 def load_bfb():
@@ -224,12 +227,12 @@ def run_reference_arm(args):
         return 0
     rate, n, threads, name, el = r
     line = {
-        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "impl": "reference", "metric": metric_name(), "value": rate, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": warm, "ms_per_step": el / n * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded U[0,1) field, log-uniform D/lambda)",
         "config": config({"solver": name, "threads": threads, "ranks": "1 rank x N threads (MPI unavailable)"}),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{n} of the {args.steps} requested full 256^3x8 FP64 steps (capped at "
+                         "sample": f"{n} of the {args.steps} requested full {NX}^3x{S} FP64 steps (capped at "
                                    f"{args.ref_seconds:.0f} s) after 1 factor-setup step, best of LOD_3D / AVX256D"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -330,14 +333,14 @@ def run_our_arm(args):
         if r is not None:
             rate, n, threads, sname, el = r
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"{n} full 256^3x8 FP64 steps ({el:.1f} s) of the reference {sname} "
+                   "sample": f"{n} full {NX}^3x{S} FP64 steps ({el:.1f} s) of the reference {sname} "
                              "(faster of LOD_3D / AVX256D), after one factor-setup step"}
         else:
             rate, n = cpu_port_run(args.cpu_seconds)
             cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"{n} steps of a 64^3x8 sample with the oracle port (reference not built)"}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warm,
+        "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warm,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded U[0,1) field, log-uniform D/lambda)",
         "config": config(),
@@ -372,7 +375,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=60.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=256, help="edge of the cubic grid (profiling small cases)")
+    ap.add_argument("--substrates", type=int, default=8)
     args = ap.parse_args()
+    global NX, NY, NZ, S
+    NX = NY = NZ = args.grid
+    S = args.substrates
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_our_arm(args)
