@@ -292,8 +292,11 @@ def run_our_arm(args):
         prof = env.profile_steps(DT, min(K, 50), bfb.STEP_DIFFUSION)
         nprof = min(K, 50)
         results[name] = dict(ms=ms, clocks=clk, prof=prof, nprof=nprof, env=env, elem=4 if prec == bfb.FP32 else 8)
-        if name == "fp64":
-            env.close()
+
+    # both envs ran the same steps from the same field: FP32's error against FP64
+    n_steps_run = warm + K + min(K, 50)
+    err_linf, err_l2 = results["fp32"]["env"].compare(results["fp64"]["env"])
+    results["fp64"]["env"].close()
 
     # end to end through the C ABI with reference-facing host buffers
     env = results["fp32"]["env"]
@@ -355,6 +358,7 @@ def run_our_arm(args):
                  "step_roofline_frac": 6.0 * V * S * 8 / (r64["ms"] / K / 1e3) / 1e9 / peak,
                  "kernel_ms_per_launch": {p: float(x) for p, x in zip(phases, r64["prof"][:3] / r64["nprof"])}},
         "fp32_over_fp64": value / value64,
+        "fp32_error_vs_fp64": {"rel_linf": err_linf, "rel_l2": err_l2, "after_steps": n_steps_run},
         "clocks": r32["clocks"],
         "e2e": {"value": world * V * S * K_e2e / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": V * S * 8,
                 "d2h_bytes_per_step": V * S * 8, "steps": K_e2e,

@@ -47,10 +47,12 @@ ERRORS = {
 EXPORTS = [
     "bfb_last_error", "bfb_version", "bfb_create", "bfb_create_domain", "bfb_destroy", "bfb_get_shape",
     "bfb_set_stream", "bfb_set_option", "bfb_synchronize", "bfb_set_coefficients", "bfb_set_field",
-    "bfb_get_field", "bfb_set_field_raw", "bfb_get_field_raw", "bfb_field_device_ptr", "bfb_set_dirichlet",
+    "bfb_get_field", "bfb_set_field_raw", "bfb_get_field_raw", "bfb_set_field_device", "bfb_get_field_device",
+    "bfb_compare_fields", "bfb_field_device_ptr", "bfb_set_dirichlet",
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
-    "bfb_checksum", "bfb_checksum_noalloc",
+    "bfb_checksum", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
+    "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_checksum_noalloc",
 ]
 
 
@@ -90,6 +92,9 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_get_field": [_vp, _vp],
         "bfb_set_field_raw": [_vp, _vp],
         "bfb_get_field_raw": [_vp, _vp],
+        "bfb_set_field_device": [_vp, _vp, ctypes.c_int],
+        "bfb_get_field_device": [_vp, _vp, ctypes.c_int],
+        "bfb_compare_fields": [_vp, _vp, _dp],
         "bfb_field_device_ptr": [_vp, ctypes.POINTER(_vp)],
         "bfb_set_dirichlet": [_vp, _vp, _vp, _vp],
         "bfb_set_dirichlet_uniform": [_vp, _vp, _vp, _vp],
@@ -106,6 +111,12 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_profile_steps": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp],
         "bfb_checksum": [_vp, _dp],
         "bfb_checksum_noalloc": [_vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, _vp, _vp],
+        "bfb_batch_create": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)],
+        "bfb_batch_destroy": [_vp],
+        "bfb_batch_set_option": [_vp, ctypes.c_int, ctypes.c_int],
+        "bfb_batch_simulate": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
+        "bfb_batch_simulate_loop": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
+        "bfb_batch_synchronize": [_vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -248,6 +259,18 @@ class Env:
         _check(self.L.bfb_get_field_raw(self.h, _ptr(out)))
         return out
 
+    def set_field_device(self, ptr: int, precision: int):
+        _check(self.L.bfb_set_field_device(self.h, ctypes.c_void_p(ptr), precision))
+
+    def get_field_device(self, ptr: int, precision: int):
+        _check(self.L.bfb_get_field_device(self.h, ctypes.c_void_p(ptr), precision))
+
+    def compare(self, ref: "Env"):
+        """Relative L-inf and L2 of this field against ref's, computed on the device."""
+        out = np.zeros(4)
+        _check(self.L.bfb_compare_fields(self.h, ref.h, out.ctypes.data_as(_dp)))
+        return out[0] / max(out[1], 1e-300), float(np.sqrt(out[2] / max(out[3], 1e-300)))
+
     def field_device_ptr(self) -> int:
         p = _vp()
         _check(self.L.bfb_field_device_ptr(self.h, ctypes.byref(p)))
@@ -282,3 +305,38 @@ class Env:
         out = np.zeros(self.S)
         _check(self.L.bfb_checksum(self.h, out.ctypes.data_as(_dp)))
         return out
+
+
+class Batch:
+    """Many envs stepped by one persistent launch per step (a ``bfb_batch``)."""
+
+    def __init__(self, envs):
+        self.L = load_library()
+        self.envs = list(envs)  # kept alive: the batch references them
+        arr = (_vp * len(self.envs))(*[e.h for e in self.envs])
+        h = _vp()
+        _check(self.L.bfb_batch_create(ctypes.byref(h), len(self.envs), arr))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bfb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_warps(self, w):
+        _check(self.L.bfb_batch_set_option(self.h, 1, w))
+
+    def simulate(self, dt, n, flags=STEP_DIFFUSION):
+        _check(self.L.bfb_batch_simulate(self.h, dt, n, flags))
+
+    def simulate_loop(self, dt, n, flags=STEP_DIFFUSION):
+        _check(self.L.bfb_batch_simulate_loop(self.h, dt, n, flags))
+
+    def synchronize(self):
+        _check(self.L.bfb_batch_synchronize(self.h))

@@ -341,6 +341,71 @@ int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s) {
     return BFB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Field comparison: max|a-b|, max|b|, sum (a-b)^2, sum b^2 (FP64 partials per
+// block, summed in block order on the host).
+// ---------------------------------------------------------------------------
+template <typename TA, typename TB>
+__global__ void compare_kernel(const TA *__restrict__ a, const TB *__restrict__ b, long long N, double *__restrict__ part) {
+    __shared__ double s0[256], s1[256], s2[256], s3[256];
+    double mx = 0, mb = 0, sd = 0, sb = 0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (long long)gridDim.x * blockDim.x) {
+        const double x = (double)a[e], y = (double)b[e], df = x - y;
+        mx = fmax(mx, fabs(df));
+        mb = fmax(mb, fabs(y));
+        sd += df * df;
+        sb += y * y;
+    }
+    s0[threadIdx.x] = mx;
+    s1[threadIdx.x] = mb;
+    s2[threadIdx.x] = sd;
+    s3[threadIdx.x] = sb;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s0[threadIdx.x] = fmax(s0[threadIdx.x], s0[threadIdx.x + w]);
+            s1[threadIdx.x] = fmax(s1[threadIdx.x], s1[threadIdx.x + w]);
+            s2[threadIdx.x] += s2[threadIdx.x + w];
+            s3[threadIdx.x] += s3[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[4 * blockIdx.x + 0] = s0[0];
+        part[4 * blockIdx.x + 1] = s1[0];
+        part[4 * blockIdx.x + 2] = s2[0];
+        part[4 * blockIdx.x + 3] = s3[0];
+    }
+}
+
+int compare_fields(const void *a, int pa, const void *b, int pb, long long N, double *out4, cudaStream_t s) {
+    const int blocks = 592;
+    double *part = nullptr;
+    BFB_CUDA(cudaMalloc(&part, sizeof(double) * 4 * blocks));
+    if (pa == BFB_FP64 && pb == BFB_FP64)
+        compare_kernel<<<blocks, 256, 0, s>>>((const double *)a, (const double *)b, N, part);
+    else if (pa == BFB_FP32 && pb == BFB_FP64)
+        compare_kernel<<<blocks, 256, 0, s>>>((const float *)a, (const double *)b, N, part);
+    else if (pa == BFB_FP64 && pb == BFB_FP32)
+        compare_kernel<<<blocks, 256, 0, s>>>((const double *)a, (const float *)b, N, part);
+    else
+        compare_kernel<<<blocks, 256, 0, s>>>((const float *)a, (const float *)b, N, part);
+    std::vector<double> h(4 * blocks);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), part, sizeof(double) * 4 * blocks, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(part);
+    if (e != cudaSuccess) return cuda_fail(e, "compare_fields");
+    out4[0] = out4[1] = out4[2] = out4[3] = 0;
+    for (int q = 0; q < blocks; ++q) {
+        out4[0] = std::max(out4[0], h[4 * q]);
+        out4[1] = std::max(out4[1], h[4 * q + 1]);
+        out4[2] += h[4 * q + 2];
+        out4[3] += h[4 * q + 3];
+    }
+    return BFB_OK;
+}
+
 // Checksum kernels on caller-provided scratch: `partials` holds at least
 // nblocks*S doubles; out_dev receives S doubles. Launches only, no allocation.
 int launch_checksum_raw(const void *field, int precision, long long V, int S, double *partials, int nblocks,

@@ -24,6 +24,8 @@ int launch_cells(bfb_env_s *env, cudaStream_t s);
 // env->partials (allocated on demand, outside any stream capture).
 int checksum_prepare(bfb_env_s *env);
 int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s);
+// max|a-b|, max|b|, sum (a-b)^2, sum b^2 of two device fields of N elements.
+int compare_fields(const void *a, int pa, const void *b, int pb, long long N, double *out4, cudaStream_t s);
 // The same kernels on caller-provided scratch (partials: nblocks*S doubles).
 int launch_checksum_raw(const void *field, int precision, long long V, int S, double *partials, int nblocks,
                         double *out_dev, cudaStream_t s);

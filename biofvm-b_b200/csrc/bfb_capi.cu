@@ -172,6 +172,7 @@ template <typename T>
 static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
     SweepArgs<T> a;
     a.f = static_cast<T *>(env->field);
+    a.fo = a.f;
     a.nx = env->nx;
     a.ny = env->ny;
     a.nz = env->nz;
@@ -211,10 +212,10 @@ static const CUtensorMap *tma_map(bfb_env_s *env, int axis) {
 template <typename T>
 static int run_diffusion(bfb_env_s *env, double dt, bool bulk, cudaStream_t s) {
     int st = launch_strided<T>(make_args<T>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, tma_map(env, 0),
-                               env->tma_crow[0], s);
+                               tma_map(env, 0), env->tma_crow[0], s);
     if (st) return st;
     st = launch_strided<T>(make_args<T>(env, 1, false, dt), 1, false, env->tuning.warps_y, tma_map(env, 1),
-                           env->tma_crow[1], s);
+                           tma_map(env, 1), env->tma_crow[1], s);
     if (st) return st;
     return launch_contig<T>(make_args<T>(env, 2, false, dt), env->tuning.warps_z, env->use_tma != 0, s);
 }
@@ -239,6 +240,47 @@ static int run_steps(bfb_env_s *env, double dt, int n, int flags, cudaStream_t s
 
 static int run_steps_any(bfb_env_s *env, double dt, int n, int flags, cudaStream_t s) {
     return env->precision == BFB_FP64 ? run_steps<double>(env, dt, n, flags, s) : run_steps<float>(env, dt, n, flags, s);
+}
+
+// Hooks for the batched ensemble (bfb_batch.cu): the per-env state a step
+// needs, and the per-axis kernel arguments and tile geometry.
+int env_prepare_step(bfb_env_s *env, double dt, int flags) {
+    BFB_CUDA(cudaSetDevice(env->device));
+    if (flags & BFB_STEP_DIFFUSION) return ensure_factors(env, dt);
+    return BFB_OK;
+}
+
+template <typename T>
+SweepArgs<T> env_sweep_args(bfb_env_s *env, int axis, double dt) {
+    return make_args<T>(env, axis, false, dt);
+}
+template SweepArgs<double> env_sweep_args<double>(bfb_env_s *, int, double);
+template SweepArgs<float> env_sweep_args<float>(bfb_env_s *, int, double);
+
+int env_tile_plan(bfb_env_s *env, int elem, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]) {
+    const bool base16 = (reinterpret_cast<uintptr_t>(env->field) & 15) == 0;
+    gx->axis = 0;
+    gx->n = env->nx;
+    gx->P = (long long)env->ny * env->nz * env->S;
+    gx->slab_stride = 0;
+    gx->n_slabs = 1;
+    gx->ncb = (int)((gx->P + 31) / 32);
+    gy->axis = 1;
+    gy->n = env->ny;
+    gy->P = (long long)env->nz * env->S;
+    gy->slab_stride = (long long)env->ny * env->nz * env->S;
+    gy->n_slabs = env->nx;
+    gy->ncb = (int)((gy->P + 31) / 32);
+    vb16[0] = base16 && (gx->P * elem) % 16 == 0;
+    vb16[1] = base16 && (gy->P * elem) % 16 == 0 && (gy->slab_stride * elem) % 16 == 0;
+    gz->nz = env->nz;
+    gz->nrows = (long long)env->nx * env->ny;
+    if (!strided_smem(env->nx, elem, 1) || !strided_smem(env->ny, elem, 1) ||
+        !contig_smem(env->nz, env->S, elem, 1, &gz->R, &gz->RS))
+        return fail(BFB_ERR_UNSUPPORTED, "batch: an env's lines are too long for a shared-memory tile");
+    const long long L = (long long)env->nz * env->S;
+    vb16[2] = base16 && (L * elem) % 16 == 0 && ((long long)gz->RS * elem) % 16 == 0;
+    return BFB_OK;
 }
 
 static void drop_graph(bfb_env_s *env) {
@@ -273,6 +315,17 @@ static int bulk_tabulate(bfb_env_s *env, const double *Sr, const double *T, cons
 }  // namespace bfb
 
 using namespace bfb;
+
+// The device error flag is sticky: once a kernel's bounded wait ran out, the
+// env's field is not trustworthy and every later synchronize reports it.
+static int check_device_error(bfb_env_s *env) {
+    int flag = 0;
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    BFB_CUDA(cudaMemcpy(&flag, env->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) return fail(BFB_ERR_WATCHDOG, "a device-side wait ran out of its iteration limit (data movement stalled)");
+    return BFB_OK;
+}
+
 
 // ===========================================================================
 extern "C" {
@@ -440,16 +493,6 @@ BFB_API int bfb_set_option(bfb_env env, int option, int value) {
     return BFB_OK;
 }
 
-// The device error flag is sticky: once a kernel's bounded wait ran out, the
-// env's field is not trustworthy and every later synchronize reports it.
-static int check_device_error(bfb_env_s *env) {
-    int flag = 0;
-    BFB_CUDA(cudaStreamSynchronize(env->stream));
-    BFB_CUDA(cudaMemcpy(&flag, env->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) return fail(BFB_ERR_WATCHDOG, "a device-side wait ran out of its iteration limit (data movement stalled)");
-    return BFB_OK;
-}
-
 BFB_API int bfb_synchronize(bfb_env env) {
     int st = check_env(env);
     if (st) return st;
@@ -517,6 +560,48 @@ BFB_API int bfb_get_field_raw(bfb_env env, void *host) {
     BFB_CUDA(cudaMemcpyAsync(host, env->field, env->elem * env->N, cudaMemcpyDeviceToHost, env->stream));
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     return BFB_OK;
+}
+
+// Device-to-device field transfer with precision conversion.
+BFB_API int bfb_set_field_device(bfb_env env, const void *src, int src_precision) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!src) return fail(BFB_ERR_INVALID_ARG, "src is NULL");
+    if (src_precision != BFB_FP64 && src_precision != BFB_FP32) return fail(BFB_ERR_INVALID_ARG, "bad precision");
+    if (src_precision == env->precision) {
+        BFB_CUDA(cudaMemcpyAsync(env->field, src, env->elem * env->N, cudaMemcpyDeviceToDevice, env->stream));
+    } else if (src_precision == BFB_FP64) {
+        if ((st = launch_convert_d2f((const double *)src, (float *)env->field, env->N, env->stream))) return st;
+    } else {
+        if ((st = launch_convert_f2d((const float *)src, (double *)env->field, env->N, env->stream))) return st;
+    }
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_get_field_device(bfb_env env, void *dst, int dst_precision) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!dst) return fail(BFB_ERR_INVALID_ARG, "dst is NULL");
+    if (dst_precision != BFB_FP64 && dst_precision != BFB_FP32) return fail(BFB_ERR_INVALID_ARG, "bad precision");
+    if (dst_precision == env->precision) {
+        BFB_CUDA(cudaMemcpyAsync(dst, env->field, env->elem * env->N, cudaMemcpyDeviceToDevice, env->stream));
+    } else if (dst_precision == BFB_FP64) {
+        if ((st = launch_convert_f2d((const float *)env->field, (double *)dst, env->N, env->stream))) return st;
+    } else {
+        if ((st = launch_convert_d2f((const double *)env->field, (float *)dst, env->N, env->stream))) return st;
+    }
+    return check_device_error(env);
+}
+
+BFB_API int bfb_compare_fields(bfb_env test, bfb_env ref, double *out4) {
+    int st = check_env(test);
+    if (st) return st;
+    if (!ref || !out4) return fail(BFB_ERR_INVALID_ARG, "null argument");
+    if (test->N != ref->N || test->S != ref->S || test->device != ref->device)
+        return fail(BFB_ERR_SIZE, "fields differ in shape or device");
+    BFB_CUDA(cudaStreamSynchronize(ref->stream));
+    return compare_fields(test->field, test->precision, ref->field, ref->precision, test->N, out4, test->stream);
 }
 
 BFB_API int bfb_field_device_ptr(bfb_env env, void **dptr) {
@@ -784,16 +869,18 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
             const bool bulk = (flags & BFB_STEP_BULK) != 0;
             st = phase_ms(0, [&] {
                 return fp64 ? launch_strided<double>(make_args<double>(env, 0, bulk, dt), 0, true, env->tuning.warps_x,
-                                                     tma_map(env, 0), env->tma_crow[0], s)
+                                                     tma_map(env, 0), tma_map(env, 0), env->tma_crow[0], s)
                             : launch_strided<float>(make_args<float>(env, 0, bulk, dt), 0, true, env->tuning.warps_x,
-                                                    tma_map(env, 0), env->tma_crow[0], s);
+                                                    tma_map(env, 0), tma_map(env, 0), env->tma_crow[0], s);
             });
             if (!st)
                 st = phase_ms(1, [&] {
                     return fp64 ? launch_strided<double>(make_args<double>(env, 1, false, dt), 1, false,
-                                                         env->tuning.warps_y, tma_map(env, 1), env->tma_crow[1], s)
+                                                         env->tuning.warps_y, tma_map(env, 1), tma_map(env, 1),
+                                                         env->tma_crow[1], s)
                                 : launch_strided<float>(make_args<float>(env, 1, false, dt), 1, false,
-                                                        env->tuning.warps_y, tma_map(env, 1), env->tma_crow[1], s);
+                                                        env->tuning.warps_y, tma_map(env, 1), tma_map(env, 1),
+                                                        env->tma_crow[1], s);
                 });
             if (!st)
                 st = phase_ms(2, [&] {

@@ -103,8 +103,8 @@ struct LineSolver<double> {
         c1 = a.c1[d];
         S = a.S;
     }
-    // returns the value stored for the backward pass
-    __device__ __forceinline__ double first(double x0) {
+    // returns the value stored for the backward pass (xref: FP32 only)
+    __device__ __forceinline__ double first(double x0, double) {
         prev = div_rcp(x0, den[0], rcp[0]);
         return prev;
     }
@@ -149,10 +149,14 @@ struct LineSolver<float> {
         gl = A.g[A.S + d];
         S = A.S;
     }
-    __device__ __forceinline__ float first(float x0) {
-        xb = x0;  // deviation reference; z_0 = (u_0 - xb)/den_0 = 0
-        p = 0.0f;
-        return 0.0f;
+    // xref is the deviation reference: the line's row 1 (row 0 when n == 1).
+    // Not row 0, which on a Dirichlet line is the boundary value and can be
+    // far from the interior.
+    __device__ __forceinline__ float first(float x0, float xref) {
+        xb = xref;
+        const float dlt = __fsub_rn(x0, xb);
+        p = __fmaf_rn(dlt, rh[0], __fmul_rn(dlt, rl[0]));
+        return p;
     }
     template <bool TAIL>
     __device__ __forceinline__ float fwd(float x, int r) {

@@ -1,6 +1,6 @@
 // bfb_sweeps.cu -- Thomas sweep kernels (see bfb_sweeps.cuh for the design).
 #include "bfb_sweeps.cuh"
-#include "bfb_line.cuh"
+#include "bfb_tiles.cuh"
 
 #include <algorithm>
 #include <mutex>
@@ -72,9 +72,14 @@ template <class Pre, class Out, class Ready>
 __device__ __forceinline__ void solve_line(float *line, long long ls, int n, const LineFactors32 &F, Pre pre, Out out,
                                            Ready ready) {
     ready(0);
-    const float xb = pre(0, line[0]);  // deviation reference: the line's first value
-    float p = 0.0f;                     // z_0 = (u_0 - xb)/den_0 = 0
-    line[0] = 0.0f;
+    ready(min(1, n - 1));
+    const float xb = pre(min(1, n - 1), line[min(1, n - 1) * ls]);  // deviation reference: row 1
+    float p;
+    {
+        const float dlt = __fsub_rn(pre(0, line[0]), xb);
+        p = __fmaf_rn(dlt, F.rh[0], __fmul_rn(dlt, F.rl[0]));
+    }
+    line[0] = p;
     const int hb = min(F.m0, n - 1);
     for (int r = 1; r < hb; ++r) {
         ready(r);
@@ -152,143 +157,10 @@ __device__ __forceinline__ LineFactors32 line_factors(const SweepArgs<float> &a,
 template <typename T, int VB, bool FUSE_PRE, bool BULK>
 __global__ void __launch_bounds__(128) sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
     if (tile >= (long long)g.n_slabs * g.ncb) return;
-    const int slab = (int)(tile / g.ncb);
-    const long long col0 = (tile % g.ncb) * 32;
-    const int ncols = (int)min((long long)32, g.P - col0);
-    const int n = g.n;
-    const long long P = g.P;
-    T *__restrict__ sm = reinterpret_cast<T *>(smem_raw) + (size_t)warp * n * 32;
-    T *__restrict__ base = a.f + (size_t)slab * g.slab_stride + col0;
-
-    // ---- stage the tile: kChunks commit groups of rows
-    const int crow = (n + kChunks - 1) / kChunks;
-    const int nch = (n + crow - 1) / crow;  // non-empty groups
-    constexpr int EPV = VB / (int)sizeof(T);  // elements per copy
-    const bool vec = (VB > (int)sizeof(T)) && ncols == 32;
-#pragma unroll 1
-    for (int ch = 0; ch < kChunks; ++ch) {
-        const int r0 = min(n, ch * crow), r1 = min(n, r0 + crow);
-        if (vec) {
-            constexpr int VPR = 32 / EPV;  // copies per row
-            const int total = (r1 - r0) * VPR;
-            for (int v = lane; v < total; v += 32) {
-                const int r = r0 + v / VPR, q = (v % VPR) * EPV;
-                cp_async<VB>(sm + r * 32 + q, base + (size_t)r * P + q);
-            }
-        } else if (lane < ncols) {
-            for (int r = r0; r < r1; ++r) cp_async<sizeof(T)>(sm + r * 32 + lane, base + (size_t)r * P + lane);
-        }
-        cp_commit();
-    }
-    // Group ch has landed for the whole warp after wait(ch). Every lane takes
-    // the same nch waits: one lane's 16-byte copies fill rows other lanes read.
-    auto wait = [&](int ch) {
-        cp_wait_dyn(kChunks - 1 - ch);
-        __syncwarp();
-    };
-    const bool valid = lane < ncols;
-    if (!valid) {
-        for (int ch = 0; ch < nch; ++ch) wait(ch);
-        return;
-    }
-
-    // ---- line coordinates of this lane
-    const long long col = col0 + lane;
-    const int S = a.S;
-    const int d = (int)(col % S);
-    int ci, cj, ck;  // voxel coordinates with the line coordinate left at 0
-    if (g.axis == 0) {
-        const long long t = col / S;
-        ck = (int)(t % a.nz);
-        cj = (int)(t / a.nz);
-        ci = 0;
-    } else {
-        ck = (int)(col / S);
-        ci = slab;
-        cj = 0;
-    }
-    const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
-    bool col_dir, lo_dir, hi_dir;
-    if (g.axis == 0) {
-        col_dir = ((m & 4u) && cj == 0) || ((m & 8u) && cj == a.ny - 1) || ((m & 16u) && ck == 0) ||
-                  ((m & 32u) && ck == a.nz - 1);
-        lo_dir = m & 1u;
-        hi_dir = m & 2u;
-    } else {
-        col_dir = ((m & 1u) && ci == 0) || ((m & 2u) && ci == a.nx - 1) || ((m & 16u) && ck == 0) ||
-                  ((m & 32u) && ck == a.nz - 1);
-        lo_dir = m & 4u;
-        hi_dir = m & 8u;
-    }
-    auto vox_dir = [&](int mm) -> T {
-        return g.axis == 0 ? dir_value(a.dir, mm, cj, ck, d) : dir_value(a.dir, ci, mm, ck, d);
-    };
-    const T *bA = nullptr, *bB = nullptr;
-    if constexpr (BULK) {
-        bA = a.bulk.A + (size_t)slab * g.slab_stride + col;
-        bB = a.bulk.B + (size_t)slab * g.slab_stride + col;
-    }
-    auto load = [&](int r) -> T {
-        T x = sm[r * 32 + lane];
-        if constexpr (BULK) x = bulk_update(x, bA[(size_t)r * P], bB[(size_t)r * P], a.bulk.dt);
-        return x;
-    };
-
-    LineSolver<T> L(a, d);
-    const int m0 = a.fac.m0;
-
-    // ---- forward elimination in shared memory, group by group as copies land
-    wait(0);
-    {
-        T x0 = load(0);
-        if (FUSE_PRE && (lo_dir || (hi_dir && n == 1))) x0 = vox_dir(0);
-        sm[lane] = L.first(x0);
-    }
-    int r = 1;
-    for (int ch = 0; ch < nch; ++ch) {
-        if (ch > 0) wait(ch);
-        const int rend = min(n - 1, (ch + 1) * crow);
-        const int hend = min(rend, m0);
-        for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(load(r), r);
-#pragma unroll 8
-        for (; r < rend; ++r) sm[r * 32 + lane] = L.template fwd<true>(load(r), r);
-    }
-    if (n > 1) {
-        T x = load(n - 1);
-        if (FUSE_PRE && hi_dir) x = vox_dir(n - 1);
-        L.template fwd<false>(x, n - 1);
-    }
-
-    // ---- back substitution straight to global memory
-    T *gp = base + lane + (size_t)(n - 1) * P;
-    {
-        T y = L.out_last();
-        if (hi_dir || (lo_dir && n == 1)) y = vox_dir(n - 1);
-        *gp = y;
-    }
-    const int tl = max(m0, 1);
-    r = n - 2;
-#pragma unroll 8
-    for (; r >= tl; --r) {
-        gp -= P;
-        *gp = L.template bwd<true>(sm[r * 32 + lane], r);
-    }
-    for (; r >= 1; --r) {
-        gp -= P;
-        *gp = L.template bwd<false>(sm[r * 32 + lane], r);
-    }
-    if (n > 1) {
-        T y = L.template bwd<false>(sm[lane], 0);
-        if (lo_dir) y = vox_dir(0);
-        gp -= P;
-        *gp = y;
-    }
-    if (col_dir)  // the whole column is on an active face of another axis
-        for (int q = 0; q < n; ++q) base[lane + (size_t)q * P] = vox_dir(q);
+    strided_tile<T, VB, FUSE_PRE, BULK>(a, g, tile, reinterpret_cast<T *>(smem_raw) + (size_t)warp * g.n * 32);
 }
 
 // ---------------------------------------------------------------------------
@@ -297,85 +169,10 @@ __global__ void __launch_bounds__(128) sweep_strided_kernel(SweepArgs<T> a, Stri
 template <typename T, int VB>
 __global__ void __launch_bounds__(128) sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
-    const long long row0 = tile * g.R;
-    if (row0 >= g.nrows) return;
-    const int nr = (int)min((long long)g.R, g.nrows - row0);
-    const int S = a.S, nz = g.nz;
-    const int L = nz * S;
-    T *__restrict__ sm = reinterpret_cast<T *>(smem_raw) + (size_t)warp * g.R * g.RS;
-    T *__restrict__ base = a.f + (size_t)row0 * L;
-    constexpr int EPV = VB / (int)sizeof(T);
-
-    // ---- stage nr rows (one contiguous block of global memory) into padded rows
-    {
-        const int vpr = L / EPV;
-        const int total = nr * vpr;
-        for (int v = lane; v < total; v += 32) {
-            const int r = v / vpr, q = (v - r * vpr) * EPV;
-            cp_async<VB>(sm + (size_t)r * g.RS + q, base + (size_t)r * L + q);
-        }
-        cp_commit();
-        cp_wait<0>();
-        __syncwarp();
-    }
-
-    // ---- lane (r, d) solves line (row0 + r, d) in place
-    const int m0 = a.fac.m0;
-    for (int t = lane; t < nr * S; t += 32) {
-        const int r = t / S, d = t - r * S;
-        const long long row = row0 + r;
-        const int i = (int)(row / a.ny), j = (int)(row % a.ny);
-        const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
-        const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
-                              ((m & 8u) && j == a.ny - 1);
-        const bool lo_dir = m & 16u, hi_dir = m & 32u;
-        T *line = sm + (size_t)r * g.RS + d;
-        LineSolver<T> Ls(a, d);
-        line[0] = Ls.first(line[0]);
-        const int hend = min(nz - 1, m0);
-        int k = 1;
-        for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(line[k * S], k);
-#pragma unroll 8
-        for (; k < nz - 1; ++k) line[k * S] = Ls.template fwd<true>(line[k * S], k);
-        if (nz > 1) Ls.template fwd<false>(line[(nz - 1) * S], nz - 1);
-        {
-            const T y = Ls.out_last();  // also seeds the back substitution
-            line[(nz - 1) * S] = (hi_dir || (lo_dir && nz == 1)) ? dir_value(a.dir, i, j, nz - 1, d) : y;
-        }
-        const int tl = max(m0, 1);
-        k = nz - 2;
-#pragma unroll 8
-        for (; k >= tl; --k) line[k * S] = Ls.template bwd<true>(line[k * S], k);
-        for (; k >= 1; --k) line[k * S] = Ls.template bwd<false>(line[k * S], k);
-        if (nz > 1) {
-            const T y = Ls.template bwd<false>(line[0], 0);
-            line[0] = lo_dir ? dir_value(a.dir, i, j, 0, d) : y;
-        }
-        if (line_dir)
-            for (int q = 0; q < nz; ++q) line[q * S] = dir_value(a.dir, i, j, q, d);
-    }
-    __syncwarp();
-
-    // ---- copy the rows back out
-    {
-        const int vpr = L / EPV;
-        const int total = nr * vpr;
-        for (int v = lane; v < total; v += 32) {
-            const int r = v / vpr, q = (v - r * vpr) * EPV;
-            const T *src = sm + (size_t)r * g.RS + q;
-            T *dst = base + (size_t)r * L + q;
-            if constexpr (VB == 16) {
-                *reinterpret_cast<int4 *>(dst) = *reinterpret_cast<const int4 *>(src);
-            } else if constexpr (VB == 8) {
-                *reinterpret_cast<int2 *>(dst) = *reinterpret_cast<const int2 *>(src);
-            } else {
-                *dst = *src;
-            }
-        }
-    }
+    if (tile * g.R >= g.nrows) return;
+    contig_tile<T, VB>(a, g, tile, reinterpret_cast<T *>(smem_raw) + (size_t)warp * g.R * g.RS);
 }
 
 // ---------------------------------------------------------------------------
@@ -418,8 +215,12 @@ __global__ void sweep_strided_global_kernel(SweepArgs<T> a, StridedGeom g) {
     auto vox_dir = [&](int mm) -> T {
         return g.axis == 0 ? dir_value(a.dir, mm, cj, ck, d) : dir_value(a.dir, ci, mm, ck, d);
     };
-    T *line = a.f + (size_t)slab * g.slab_stride + col;
     const long long P = g.P;
+    T *line = a.fo + (size_t)slab * g.slab_stride + col;  // solved in place in the output
+    if (a.fo != a.f) {
+        const T *src = a.f + (size_t)slab * g.slab_stride + col;
+        for (int r = 0; r < n; ++r) line[(size_t)r * P] = src[(size_t)r * P];
+    }
     auto pre = [&](int r, T x) -> T {
         if constexpr (FUSE_PRE) {
             if (a.bulk.on) {
@@ -450,7 +251,11 @@ __global__ void sweep_contig_global_kernel(SweepArgs<T> a, long long nrows) {
     const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
                           ((m & 8u) && j == a.ny - 1);
     const bool lo_dir = m & 16u, hi_dir = m & 32u;
-    T *line = a.f + (size_t)row * nz * S + d;
+    T *line = a.fo + (size_t)row * nz * S + d;  // solved in place in the output
+    if (a.fo != a.f) {
+        const T *src = a.f + (size_t)row * nz * S + d;
+        for (int k = 0; k < nz; ++k) line[(size_t)k * S] = src[(size_t)k * S];
+    }
     auto pre = [](int, T x) -> T { return x; };
     auto out = [&](int k, T y) {
         if (line_dir || (k == 0 && lo_dir) || (k == nz - 1 && hi_dir)) y = dir_value(a.dir, i, j, k, d);
@@ -538,8 +343,8 @@ static int go_strided(const SweepArgs<T> &a, const StridedGeom &g, int warps, si
 }
 
 template <typename T>
-int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map, int crow,
-                   cudaStream_t s) {
+int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map,
+                   const CUtensorMap *map_out, int crow, cudaStream_t s) {
     StridedGeom g;
     g.axis = axis;
     if (axis == 0) {
@@ -555,8 +360,8 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, co
     }
     g.ncb = (int)((g.P + 31) / 32);
     warps = std::max(1, std::min(warps, 4));
-    if (map) {
-        const int st = launch_strided_tma<T>(a, g, map, crow, fuse_pre, warps, s);
+    if (map && map_out) {
+        const int st = launch_strided_tma<T>(a, g, map, map_out, crow, fuse_pre, warps, s);
         if (st != kNotApplicable) return st;
     }
     size_t smem = strided_smem(g.n, sizeof(T), warps);
@@ -671,8 +476,10 @@ void sweeps_prepare_device() {
     done |= 1ull << (dev & 63);
 }
 
-template int launch_strided<double>(const SweepArgs<double> &, int, bool, int, const CUtensorMap *, int, cudaStream_t);
-template int launch_strided<float>(const SweepArgs<float> &, int, bool, int, const CUtensorMap *, int, cudaStream_t);
+template int launch_strided<double>(const SweepArgs<double> &, int, bool, int, const CUtensorMap *,
+                                    const CUtensorMap *, int, cudaStream_t);
+template int launch_strided<float>(const SweepArgs<float> &, int, bool, int, const CUtensorMap *, const CUtensorMap *,
+                                   int, cudaStream_t);
 template int launch_contig<double>(const SweepArgs<double> &, int, bool, cudaStream_t);
 template int launch_contig<float>(const SweepArgs<float> &, int, bool, cudaStream_t);
 template int launch_dirichlet<double>(const SweepArgs<double> &, cudaStream_t);

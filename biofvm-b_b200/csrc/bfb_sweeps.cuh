@@ -38,7 +38,8 @@
 //     correctly rounded division by den_m (reciprocal + one residual
 //     correction, see div_rcp in bfb_sweeps.cu).
 //   FP32 -- FP32 storage and FP32 arithmetic, in "deviation" form. With
-//     xb = u_0 of the line and g = 1/(1 + c2), A*1 = (1 + c2)*1 exactly (every
+//     xb = u_1 of the line (u_0 when n == 1; row 0 of a Dirichlet line holds
+//     the boundary value) and g = 1/(1 + c2), A*1 = (1 + c2)*1 exactly (every
 //     row of A sums to 1 + c2), so  A^{-1} u = g*xb + A^{-1}(u - xb).
 //     The recurrence runs on u - xb with the reciprocal form
 //     z_m = (u_m - xb)*r_m + a_m*z_(m-1)  (r = 1/den, a = c1/den), r and g
@@ -63,7 +64,8 @@ struct Factors {
 
 template <typename T>
 struct SweepArgs {
-    T *f;
+    T *f;          // input field
+    T *fo;         // output field (== f for the in-place sweeps of a step)
     int nx, ny, nz, S;
     Factors<T> fac;
     const T *c1;   // FP64: [S] c1 = dt*D/dx^2
@@ -92,8 +94,8 @@ struct ContigGeom {
 // launchers (bfb_sweeps.cu). `map` (may be NULL) is the field's tensor map
 // for this axis; with it the TMA kernels run, otherwise cp.async ones.
 template <typename T>
-int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map, int crow,
-                   cudaStream_t s);
+int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map,
+                   const CUtensorMap *map_out, int crow, cudaStream_t s);
 template <typename T>
 int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s);
 
@@ -101,8 +103,8 @@ int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s
 // not fit in shared memory, and the caller then takes another kernel.
 constexpr int kNotApplicable = 1;
 template <typename T>
-int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map, int crow, bool fuse_pre,
-                       int warps, cudaStream_t s);
+int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map,
+                       const CUtensorMap *map_out, int crow, bool fuse_pre, int warps, cudaStream_t s);
 template <typename T>
 int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s);
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,

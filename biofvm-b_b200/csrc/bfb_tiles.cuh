@@ -1,0 +1,237 @@
+// bfb_tiles.cuh -- one warp's tile of a strided (x, y) or contiguous (z)
+// sweep, staged with cp.async. The single-env kernels (bfb_sweeps.cu) and the
+// batched ensemble kernel (bfb_batch.cu) both run these.
+#pragma once
+#include "bfb_line.cuh"
+
+namespace bfb {
+
+// One strided tile (32 lines of one slab) by the calling warp; sm is the
+// warp's shared-memory region of n*32 elements. Used by the single-env kernel
+// below and by the batched ensemble kernel (bfb_batch.cu).
+template <typename T, int VB, bool FUSE_PRE, bool BULK>
+__device__ __forceinline__ void strided_tile(const SweepArgs<T> &a, const StridedGeom &g, long long tile, T *sm) {
+    const int lane = threadIdx.x & 31;
+    const int slab = (int)(tile / g.ncb);
+    const long long col0 = (tile % g.ncb) * 32;
+    const int ncols = (int)min((long long)32, g.P - col0);
+    const int n = g.n;
+    const long long P = g.P;
+    T *__restrict__ base = a.f + (size_t)slab * g.slab_stride + col0;   // input
+    T *__restrict__ obase = a.fo + (size_t)slab * g.slab_stride + col0; // output (== base in place)
+
+    // ---- stage the tile: kChunks commit groups of rows
+    const int crow = (n + kChunks - 1) / kChunks;
+    const int nch = (n + crow - 1) / crow;  // non-empty groups
+    constexpr int EPV = VB / (int)sizeof(T);  // elements per copy
+    const bool vec = (VB > (int)sizeof(T)) && ncols == 32;
+#pragma unroll 1
+    for (int ch = 0; ch < kChunks; ++ch) {
+        const int r0 = min(n, ch * crow), r1 = min(n, r0 + crow);
+        if (vec) {
+            constexpr int VPR = 32 / EPV;  // copies per row
+            const int total = (r1 - r0) * VPR;
+            for (int v = lane; v < total; v += 32) {
+                const int r = r0 + v / VPR, q = (v % VPR) * EPV;
+                cp_async<VB>(sm + r * 32 + q, base + (size_t)r * P + q);
+            }
+        } else if (lane < ncols) {
+            for (int r = r0; r < r1; ++r) cp_async<sizeof(T)>(sm + r * 32 + lane, base + (size_t)r * P + lane);
+        }
+        cp_commit();
+    }
+    // Group ch has landed for the whole warp after wait(ch). Every lane takes
+    // the same nch waits: one lane's 16-byte copies fill rows other lanes read.
+    auto wait = [&](int ch) {
+        cp_wait_dyn(kChunks - 1 - ch);
+        __syncwarp();
+    };
+    const bool valid = lane < ncols;
+    if (!valid) {
+        for (int ch = 0; ch < nch; ++ch) wait(ch);
+        return;
+    }
+
+    // ---- line coordinates of this lane
+    const long long col = col0 + lane;
+    const int S = a.S;
+    const int d = (int)(col % S);
+    int ci, cj, ck;  // voxel coordinates with the line coordinate left at 0
+    if (g.axis == 0) {
+        const long long t = col / S;
+        ck = (int)(t % a.nz);
+        cj = (int)(t / a.nz);
+        ci = 0;
+    } else {
+        ck = (int)(col / S);
+        ci = slab;
+        cj = 0;
+    }
+    const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
+    bool col_dir, lo_dir, hi_dir;
+    if (g.axis == 0) {
+        col_dir = ((m & 4u) && cj == 0) || ((m & 8u) && cj == a.ny - 1) || ((m & 16u) && ck == 0) ||
+                  ((m & 32u) && ck == a.nz - 1);
+        lo_dir = m & 1u;
+        hi_dir = m & 2u;
+    } else {
+        col_dir = ((m & 1u) && ci == 0) || ((m & 2u) && ci == a.nx - 1) || ((m & 16u) && ck == 0) ||
+                  ((m & 32u) && ck == a.nz - 1);
+        lo_dir = m & 4u;
+        hi_dir = m & 8u;
+    }
+    auto vox_dir = [&](int mm) -> T {
+        return g.axis == 0 ? dir_value(a.dir, mm, cj, ck, d) : dir_value(a.dir, ci, mm, ck, d);
+    };
+    const T *bA = nullptr, *bB = nullptr;
+    if constexpr (BULK) {
+        bA = a.bulk.A + (size_t)slab * g.slab_stride + col;
+        bB = a.bulk.B + (size_t)slab * g.slab_stride + col;
+    }
+    auto load = [&](int r) -> T {
+        T x = sm[r * 32 + lane];
+        if constexpr (BULK) x = bulk_update(x, bA[(size_t)r * P], bB[(size_t)r * P], a.bulk.dt);
+        return x;
+    };
+
+    LineSolver<T> L(a, d);
+    const int m0 = a.fac.m0;
+
+    // a line's input row after the step's leading Dirichlet
+    auto xin = [&](int q) -> T {
+        T x = load(q);
+        if (FUSE_PRE && ((q == 0 && lo_dir) || (q == n - 1 && hi_dir))) x = vox_dir(q);
+        return x;
+    };
+
+    // ---- forward elimination in shared memory, group by group as copies land
+    const int rref = min(1, n - 1);  // row of the deviation reference
+    const int ref_ch = rref / crow;
+    for (int ch = 0; ch <= ref_ch; ++ch) wait(ch);
+    sm[lane] = L.first(xin(0), xin(rref));
+    int r = 1;
+    for (int ch = 0; ch < nch; ++ch) {
+        if (ch > ref_ch) wait(ch);
+        const int rend = min(n - 1, (ch + 1) * crow);
+        const int hend = min(rend, m0);
+        for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(load(r), r);
+#pragma unroll 8
+        for (; r < rend; ++r) sm[r * 32 + lane] = L.template fwd<true>(load(r), r);
+    }
+    if (n > 1) {
+        T x = load(n - 1);
+        if (FUSE_PRE && hi_dir) x = vox_dir(n - 1);
+        L.template fwd<false>(x, n - 1);
+    }
+
+    // ---- back substitution straight to global memory
+    T *gp = obase + lane + (size_t)(n - 1) * P;
+    {
+        T y = L.out_last();
+        if (hi_dir || (lo_dir && n == 1)) y = vox_dir(n - 1);
+        *gp = y;
+    }
+    const int tl = max(m0, 1);
+    r = n - 2;
+#pragma unroll 8
+    for (; r >= tl; --r) {
+        gp -= P;
+        *gp = L.template bwd<true>(sm[r * 32 + lane], r);
+    }
+    for (; r >= 1; --r) {
+        gp -= P;
+        *gp = L.template bwd<false>(sm[r * 32 + lane], r);
+    }
+    if (n > 1) {
+        T y = L.template bwd<false>(sm[lane], 0);
+        if (lo_dir) y = vox_dir(0);
+        gp -= P;
+        *gp = y;
+    }
+    if (col_dir)  // the whole column is on an active face of another axis
+        for (int q = 0; q < n; ++q) obase[lane + (size_t)q * P] = vox_dir(q);
+}
+
+// One contiguous tile (R rows) by the calling warp; sm is the warp's region
+// of R*RS elements. Used by the single-env kernel below and by bfb_batch.cu.
+template <typename T, int VB>
+__device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigGeom &g, long long tile, T *sm) {
+    const int lane = threadIdx.x & 31;
+    const long long row0 = tile * g.R;
+    const int nr = (int)min((long long)g.R, g.nrows - row0);
+    const int S = a.S, nz = g.nz;
+    const int L = nz * S;
+    T *__restrict__ base = a.f + (size_t)row0 * L;
+    T *__restrict__ obase = a.fo + (size_t)row0 * L;
+    constexpr int EPV = VB / (int)sizeof(T);
+
+    // ---- stage nr rows (one contiguous block of global memory) into padded rows
+    {
+        const int vpr = L / EPV;
+        const int total = nr * vpr;
+        for (int v = lane; v < total; v += 32) {
+            const int r = v / vpr, q = (v - r * vpr) * EPV;
+            cp_async<VB>(sm + (size_t)r * g.RS + q, base + (size_t)r * L + q);
+        }
+        cp_commit();
+        cp_wait<0>();
+        __syncwarp();
+    }
+
+    // ---- lane (r, d) solves line (row0 + r, d) in place
+    const int m0 = a.fac.m0;
+    for (int t = lane; t < nr * S; t += 32) {
+        const int r = t / S, d = t - r * S;
+        const long long row = row0 + r;
+        const int i = (int)(row / a.ny), j = (int)(row % a.ny);
+        const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
+        const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
+                              ((m & 8u) && j == a.ny - 1);
+        const bool lo_dir = m & 16u, hi_dir = m & 32u;
+        T *line = sm + (size_t)r * g.RS + d;
+        LineSolver<T> Ls(a, d);
+        line[0] = Ls.first(line[0], line[min(1, nz - 1) * S]);
+        const int hend = min(nz - 1, m0);
+        int k = 1;
+        for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(line[k * S], k);
+#pragma unroll 8
+        for (; k < nz - 1; ++k) line[k * S] = Ls.template fwd<true>(line[k * S], k);
+        if (nz > 1) Ls.template fwd<false>(line[(nz - 1) * S], nz - 1);
+        {
+            const T y = Ls.out_last();  // also seeds the back substitution
+            line[(nz - 1) * S] = (hi_dir || (lo_dir && nz == 1)) ? dir_value(a.dir, i, j, nz - 1, d) : y;
+        }
+        const int tl = max(m0, 1);
+        k = nz - 2;
+#pragma unroll 8
+        for (; k >= tl; --k) line[k * S] = Ls.template bwd<true>(line[k * S], k);
+        for (; k >= 1; --k) line[k * S] = Ls.template bwd<false>(line[k * S], k);
+        if (nz > 1) {
+            const T y = Ls.template bwd<false>(line[0], 0);
+            line[0] = lo_dir ? dir_value(a.dir, i, j, 0, d) : y;
+        }
+        if (line_dir)
+            for (int q = 0; q < nz; ++q) line[q * S] = dir_value(a.dir, i, j, q, d);
+    }
+    __syncwarp();
+
+    // ---- copy the rows back out
+    {
+        const int vpr = L / EPV;
+        const int total = nr * vpr;
+        for (int v = lane; v < total; v += 32) {
+            const int r = v / vpr, q = (v - r * vpr) * EPV;
+            const T *src = sm + (size_t)r * g.RS + q;
+            T *dst = obase + (size_t)r * L + q;
+            if constexpr (VB == 16) {
+                *reinterpret_cast<int4 *>(dst) = *reinterpret_cast<const int4 *>(src);
+            } else if constexpr (VB == 8) {
+                *reinterpret_cast<int2 *>(dst) = *reinterpret_cast<const int2 *>(src);
+            } else {
+                *dst = *src;
+            }
+        }
+    }
+}
+
+}  // namespace bfb

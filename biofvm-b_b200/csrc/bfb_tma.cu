@@ -99,7 +99,8 @@ __host__ __device__ inline size_t strided_tma_warp_bytes(int n, int crow, int el
 // ---------------------------------------------------------------------------
 template <typename T, bool FUSE_PRE, bool BULK>
 __global__ void __launch_bounds__(128)
-    sweep_strided_tma_kernel(const __grid_constant__ CUtensorMap map, SweepArgs<T> a, StridedGeom g, int crow) {
+    sweep_strided_tma_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap map_out,
+                             SweepArgs<T> a, StridedGeom g, int crow) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -182,16 +183,22 @@ __global__ void __launch_bounds__(128)
     LineSolver<T> L(a, d);
     const int m0 = a.fac.m0;
 
+    // a line's input row after the step's leading Dirichlet
+    auto xin = [&](int q) -> T {
+        T x = load(q);
+        if (FUSE_PRE && ((q == 0 && lo_dir) || (q == n - 1 && hi_dir))) x = vox_dir(q);
+        return x;
+    };
+
     // ---- forward elimination, row group by row group as the copies land
-    if (!wait_group(0)) return;
-    {
-        T x0 = load(0);
-        if (FUSE_PRE && (lo_dir || (hi_dir && n == 1))) x0 = vox_dir(0);
-        sm[lane] = L.first(x0);
-    }
+    const int rref = min(1, n - 1);  // row of the deviation reference
+    const int ref_ch = rref / crow;
+    for (int ch = 0; ch <= ref_ch; ++ch)
+        if (!wait_group(ch)) return;
+    sm[lane] = L.first(xin(0), xin(rref));
     int r = 1;
     for (int ch = 0; ch < nch; ++ch) {
-        if (ch > 0 && !wait_group(ch)) return;
+        if (ch > ref_ch && !wait_group(ch)) return;
         const int rend = min(n - 1, (ch + 1) * crow);
         const int hend = min(rend, m0);
         for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(load(r), r);
@@ -229,7 +236,7 @@ __global__ void __launch_bounds__(128)
         fence_async_smem();
         __syncwarp();
         if (lane == 0) {
-            tma_store(&map, col0, rlo, slab, rank, sm_u32 + ch * chunk_bytes);
+            tma_store(&map_out, col0, rlo, slab, rank, sm_u32 + ch * chunk_bytes);
             bulk_commit();
         }
     }
@@ -256,6 +263,7 @@ __global__ void __launch_bounds__(128) sweep_contig_tma_kernel(SweepArgs<T> a, C
     const unsigned bar = smem_u32(wbase);
     T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
     T *__restrict__ base = a.f + (size_t)row0 * L;
+    T *__restrict__ obase = a.fo + (size_t)row0 * L;
     const unsigned row_bytes = (unsigned)L * (unsigned)sizeof(T);
 
     if (lane == 0) {
@@ -283,7 +291,7 @@ __global__ void __launch_bounds__(128) sweep_contig_tma_kernel(SweepArgs<T> a, C
         const bool lo_dir = m & 16u, hi_dir = m & 32u;
         T *line = sm + (size_t)r * g.RS + d;
         LineSolver<T> Ls(a, d);
-        line[0] = Ls.first(line[0]);
+        line[0] = Ls.first(line[0], line[min(1, nz - 1) * S]);
         const int hend = min(nz - 1, m0);
         int k = 1;
         for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(line[k * S], k);
@@ -309,7 +317,7 @@ __global__ void __launch_bounds__(128) sweep_contig_tma_kernel(SweepArgs<T> a, C
     fence_async_smem();
     __syncwarp();
     if (lane == 0) {
-        for (int r = 0; r < nr; ++r) bulk_store(base + (size_t)r * L, smem_u32(sm + (size_t)r * g.RS), row_bytes);
+        for (int r = 0; r < nr; ++r) bulk_store(obase + (size_t)r * L, smem_u32(sm + (size_t)r * g.RS), row_bytes);
         bulk_commit();
         bulk_wait_read_all();
     }
@@ -343,6 +351,7 @@ __global__ void __launch_bounds__(128) sweep_contig_pipe_kernel(SweepArgs<T> a, 
     const unsigned bar0 = smem_u32(wbase);
     T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
     T *__restrict__ base = a.f + (size_t)row0 * L;
+    T *__restrict__ obase = a.fo + (size_t)row0 * L;
     auto seg_bytes = [&](int c) -> unsigned { return (unsigned)((min(nz, (c + 1) * kc) - c * kc) * S * (int)sizeof(T)); };
 
     if (lane == 0) {
@@ -379,11 +388,14 @@ __global__ void __launch_bounds__(128) sweep_contig_pipe_kernel(SweepArgs<T> a, 
     const int m0 = a.fac.m0;
 
     // ---- forward
-    if (!wait_c(0)) return;
-    if (active) line[0] = Ls.first(line[0]);
+    const int kref = min(1, nz - 1);  // row of the deviation reference
+    const int ref_c = kref / kc;
+    for (int c = 0; c <= ref_c; ++c)
+        if (!wait_c(c)) return;
+    if (active) line[0] = Ls.first(line[0], line[kref * S]);
     int k = 1;
     for (int c = 0; c < nch; ++c) {
-        if (c > 0 && !wait_c(c)) return;
+        if (c > ref_c && !wait_c(c)) return;
         const int kend = min(nz - 1, (c + 1) * kc);
         if (active) {
             const int hend = min(kend, m0);
@@ -423,7 +435,7 @@ __global__ void __launch_bounds__(128) sweep_contig_pipe_kernel(SweepArgs<T> a, 
         if (lane == 0) {
             const unsigned b = seg_bytes(c);
             for (int q = 0; q < nr; ++q)
-                bulk_store(base + (size_t)q * L + (size_t)klo * S, smem_u32(sm + (size_t)q * g.RS + (size_t)klo * S), b);
+                bulk_store(obase + (size_t)q * L + (size_t)klo * S, smem_u32(sm + (size_t)q * g.RS + (size_t)klo * S), b);
             bulk_commit();
         }
     }
@@ -435,8 +447,8 @@ __global__ void __launch_bounds__(128) sweep_contig_pipe_kernel(SweepArgs<T> a, 
 // Host side
 // ---------------------------------------------------------------------------
 template <typename T>
-int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map, int crow, bool fuse_pre,
-                       int warps, cudaStream_t s) {
+int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map,
+                       const CUtensorMap *map_out, int crow, bool fuse_pre, int warps, cudaStream_t s) {
     const size_t wb = strided_tma_warp_bytes(g.n, crow, sizeof(T));
     while (warps > 1 && wb * warps > (size_t)kMaxSmem) --warps;
     if (wb * warps > (size_t)kMaxSmem) return kNotApplicable;  // the caller takes another kernel
@@ -444,11 +456,11 @@ int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtens
     const unsigned blocks = (unsigned)((tiles + warps - 1) / warps);
     const size_t smem = wb * warps;
     if (fuse_pre && a.bulk.on)
-        sweep_strided_tma_kernel<T, true, true><<<blocks, warps * 32, smem, s>>>(*map, a, g, crow);
+        sweep_strided_tma_kernel<T, true, true><<<blocks, warps * 32, smem, s>>>(*map, *map_out, a, g, crow);
     else if (fuse_pre)
-        sweep_strided_tma_kernel<T, true, false><<<blocks, warps * 32, smem, s>>>(*map, a, g, crow);
+        sweep_strided_tma_kernel<T, true, false><<<blocks, warps * 32, smem, s>>>(*map, *map_out, a, g, crow);
     else
-        sweep_strided_tma_kernel<T, false, false><<<blocks, warps * 32, smem, s>>>(*map, a, g, crow);
+        sweep_strided_tma_kernel<T, false, false><<<blocks, warps * 32, smem, s>>>(*map, *map_out, a, g, crow);
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
 }
@@ -482,10 +494,10 @@ int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cud
     return BFB_OK;
 }
 
-template int launch_strided_tma<double>(const SweepArgs<double> &, const StridedGeom &, const CUtensorMap *, int, bool,
-                                        int, cudaStream_t);
-template int launch_strided_tma<float>(const SweepArgs<float> &, const StridedGeom &, const CUtensorMap *, int, bool,
-                                       int, cudaStream_t);
+template int launch_strided_tma<double>(const SweepArgs<double> &, const StridedGeom &, const CUtensorMap *,
+                                        const CUtensorMap *, int, bool, int, cudaStream_t);
+template int launch_strided_tma<float>(const SweepArgs<float> &, const StridedGeom &, const CUtensorMap *,
+                                       const CUtensorMap *, int, bool, int, cudaStream_t);
 template int launch_contig_tma<double>(const SweepArgs<double> &, const ContigGeom &, int, cudaStream_t);
 template int launch_contig_tma<float>(const SweepArgs<float> &, const ContigGeom &, int, cudaStream_t);
 

@@ -109,6 +109,18 @@ BFB_API int bfb_set_field(bfb_env env, const double *host);
 BFB_API int bfb_get_field(bfb_env env, double *host);
 BFB_API int bfb_set_field_raw(bfb_env env, const void *host);
 BFB_API int bfb_get_field_raw(bfb_env env, void *host);
+/* Device-to-device transfer of the field, converting from/to src/dst
+ * precision (BFB_FP64 / BFB_FP32); src/dst hold V*S elements on the env's
+ * device. The copy is ordered on the env's stream only: work that produces
+ * src on another stream must be complete (or that stream given to
+ * bfb_set_stream) before the call. Both calls return after the copy. */
+BFB_API int bfb_set_field_device(bfb_env env, const void *src, int src_precision);
+BFB_API int bfb_get_field_device(bfb_env env, void *dst, int dst_precision);
+/* Error of one env's field against another's of the same shape (any
+ * precisions): out4 = {max|a-b|, max|b|, sum (a-b)^2, sum b^2}, accumulated
+ * in FP64 on the device. Relative L-inf = out4[0]/out4[1], relative
+ * L2 = sqrt(out4[2]/out4[3]). */
+BFB_API int bfb_compare_fields(bfb_env test, bfb_env ref, double *out4);
 /* Device pointer of the field (env precision); valid until bfb_destroy. */
 BFB_API int bfb_field_device_ptr(bfb_env env, void **dptr);
 
@@ -179,6 +191,25 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
 
 /* Per-substrate FP64 sum of the field over all voxels (mass checksum). */
 BFB_API int bfb_checksum(bfb_env env, double *out);
+
+/* ---- Batched ensembles ---------------------------------------------------
+ * Many independent envs (uneven shapes and substrate counts; one device and
+ * one precision) stepped together: bfb_batch_simulate runs one LOD step of
+ * every env -- and, with BFB_STEP_CELLS, its agents -- as ONE persistent
+ * kernel launch whose warps pull (env, stage, tile) work items from a device
+ * queue, replayed from a CUDA graph. The batch references the envs; they must
+ * outlive it, and their own settings (coefficients, Dirichlet, agents) are
+ * the ones used. bfb_batch_simulate_loop runs the same steps as one
+ * bfb_simulate call per env (the per-instance launch loop). Not in the
+ * reference, which runs one Microenvironment per MPI job. */
+typedef struct bfb_batch_s *bfb_batch;
+#define BFB_BATCH_OPT_WARPS_PER_CTA 1 /* 1..4, default 1 */
+BFB_API int bfb_batch_create(bfb_batch *out, int n_envs, const bfb_env *envs);
+BFB_API int bfb_batch_destroy(bfb_batch batch);
+BFB_API int bfb_batch_set_option(bfb_batch batch, int option, int value);
+BFB_API int bfb_batch_simulate(bfb_batch batch, double dt, int n_steps, int flags);
+BFB_API int bfb_batch_simulate_loop(bfb_batch batch, double dt, int n_steps, int flags);
+BFB_API int bfb_batch_synchronize(bfb_batch batch);
 
 /* No counterpart in the reference. The per-substrate FP64 sums of
  * bfb_checksum for callers that must not allocate device memory -- for
