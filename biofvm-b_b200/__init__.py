@@ -52,7 +52,7 @@ EXPORTS = [
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
     "bfb_checksum", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
-    "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_checksum_noalloc",
+    "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_adjoint_run", "bfb_checksum_noalloc",
 ]
 
 
@@ -117,6 +117,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_batch_simulate": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_simulate_loop": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_synchronize": [_vp],
+        "bfb_adjoint_run": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _dp, _dp,
+                            _dp, _dp, _dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -304,6 +306,27 @@ class Env:
     def checksum(self):
         out = np.zeros(self.S)
         _check(self.L.bfb_checksum(self.h, out.ctypes.data_as(_dp)))
+        return out
+
+    def adjoint_run(self, dt, n_steps, dL_dfinal_ptr: int, flags=STEP_DIFFUSION, checkpoint_every=None,
+                    dL_dinitial_ptr: int = None, final_ptr: int = None, agent_grads=False):
+        """Reverse mode of n_steps steps from the current field (bfb_adjoint_run).
+
+        The pointers are device arrays of the env precision in the field layout.
+        Returns a dict of host gradients: D, lambda and, with agent_grads,
+        secretion / uptake / saturation as [n_agents, S] arrays."""
+        K = checkpoint_every or max(1, int(round(n_steps ** 0.5)))
+        gD, gL = np.zeros(self.S), np.zeros(self.S)
+        na = getattr(self, "n_agents", 0)
+        ga = [np.zeros((na, self.S)) for _ in range(3)] if agent_grads else [None] * 3
+        ap = [None if g is None else g.ctypes.data_as(_dp) for g in ga]
+        _check(self.L.bfb_adjoint_run(self.h, dt, n_steps, flags, K, ctypes.c_void_p(dL_dfinal_ptr),
+                                      None if dL_dinitial_ptr is None else ctypes.c_void_p(dL_dinitial_ptr),
+                                      None if final_ptr is None else ctypes.c_void_p(final_ptr),
+                                      gD.ctypes.data_as(_dp), gL.ctypes.data_as(_dp), *ap))
+        out = {"D": gD, "lambda": gL}
+        if agent_grads:
+            out.update(secretion=ga[0], uptake=ga[1], saturation=ga[2])
         return out
 
 

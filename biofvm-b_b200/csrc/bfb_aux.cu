@@ -129,6 +129,8 @@ void agents_free(bfb_env_s *env) {
     cudaFree(env->seg_voxel);
     cudaFree(env->ag_t1);
     cudaFree(env->ag_t2);
+    cudaFree(env->ag_order);
+    env->ag_order = nullptr;
     env->agent_voxel = env->seg_start = env->seg_voxel = nullptr;
     env->ag_t1 = env->ag_t2 = nullptr;
     env->n_agents = env->n_occ = env->n_active = 0;
@@ -203,6 +205,8 @@ static int index_agents(bfb_env_s *env, int n, const int *d_vox, const double *d
     BFB_CUDA(cudaMemcpyAsync(env->seg_voxel, d_unique.p, sizeof(int) * n_occ, cudaMemcpyDeviceToDevice, s));
     env->n_occ = n_occ;
 
+    BFB_CUDA(cudaMalloc(&env->ag_order, sizeof(int) * na));
+    BFB_CUDA(cudaMemcpyAsync(env->ag_order, d_idx_sorted.p, sizeof(int) * na, cudaMemcpyDeviceToDevice, s));
     BFB_CUDA(cudaMalloc(&env->ag_t1, env->elem * (size_t)na * S));
     BFB_CUDA(cudaMalloc(&env->ag_t2, env->elem * (size_t)na * S));
     const long long tot = (long long)na * S;

@@ -449,6 +449,7 @@ BFB_API int bfb_destroy(bfb_env env) {
     cudaFree(env->bulkB);
     cudaFree(env->partials);
     cudaFree(env->d_err);
+    cudaFree(env->adj_ws);
     if (env->own_stream) cudaStreamDestroy(env->own_stream);
     delete env;
     return BFB_OK;
@@ -747,6 +748,14 @@ BFB_API int bfb_set_agents(bfb_env env, int n, const double *pos, const double *
         return fail(BFB_ERR_INVALID_ARG, "agent arrays must not be NULL");
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     st = agents_build(env, n, pos, volume, secretion, uptake, saturation, active, dt);
+    if (!st) {
+        const size_t nS = (size_t)n * env->S;
+        env->h_vol.assign(volume, volume + n);
+        env->h_sec.assign(secretion, secretion + nS);
+        env->h_upt.assign(uptake, uptake + nS);
+        env->h_sat.assign(saturation, saturation + nS);
+        env->agent_dt = dt;
+    }
     env->epoch++;
     return st;
 }
@@ -759,6 +768,10 @@ BFB_API int bfb_set_agent_constants(bfb_env env, int n, const int *voxel, const 
     if (n > 0 && (!voxel || !temp1 || !temp2)) return fail(BFB_ERR_INVALID_ARG, "agent arrays must not be NULL");
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     st = agents_build_constants(env, n, voxel, temp1, temp2, active);
+    env->h_vol.clear();  // rates unknown: the adjoint gives no per-agent rate gradients
+    env->h_sec.clear();
+    env->h_upt.clear();
+    env->h_sat.clear();
     env->epoch++;
     return st;
 }

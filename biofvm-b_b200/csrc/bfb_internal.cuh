@@ -110,6 +110,10 @@ struct bfb_env_s {
     int *seg_voxel = nullptr;            // [n_occ]
     void *ag_t1 = nullptr, *ag_t2 = nullptr;  // [n_active][S] in voxel-sorted, list-stable order
     int n_active = 0;
+    int *ag_order = nullptr;             // [n_active]: list index of each sorted agent
+    // rates as given to bfb_set_agents (list order), for the adjoint's chain rule
+    std::vector<double> h_vol, h_sec, h_upt, h_sat;
+    double agent_dt = 0;
 
     // scratch for reductions
     double *partials = nullptr;
@@ -134,4 +138,9 @@ struct bfb_env_s {
 
     // sticky device error flag (a bounded wait in a kernel ran out)
     int *d_err = nullptr;
+
+    // reverse-mode workspace (bfb_adjoint.cu): one device block, kept between
+    // calls and grown on demand, freed by bfb_destroy
+    void *adj_ws = nullptr;
+    size_t adj_ws_bytes = 0;
 };

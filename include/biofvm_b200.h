@@ -211,6 +211,33 @@ BFB_API int bfb_batch_simulate(bfb_batch batch, double dt, int n_steps, int flag
 BFB_API int bfb_batch_simulate_loop(bfb_batch batch, double dt, int n_steps, int flags);
 BFB_API int bfb_batch_synchronize(bfb_batch batch);
 
+/* ---- Reverse mode ---------------------------------------------------------
+ * No counterpart in the reference. Runs n_steps steps of `flags`
+ * (BFB_STEP_DIFFUSION, optionally | BFB_STEP_CELLS) from the env's current
+ * field, keeping a checkpoint every checkpoint_every steps, and returns the
+ * gradients of a scalar loss L(final field) given dL/d(final field):
+ *   dL_dfinal     device, N elements of the env precision (required)
+ *   dL_dinitial   device, N elements: dL/d(initial field)         (or NULL)
+ *   final_field   device, N elements: the field after n_steps     (or NULL)
+ *   dL_dD, dL_dlambda              host, [S] doubles              (or NULL)
+ *   dL_dsecretion, dL_duptake, dL_dsaturation
+ *                 host, [n_agents][S] doubles in bfb_set_agents' list order
+ *                 (or NULL); inactive agents get 0. They need the rates of
+ *                 bfb_set_agents (BFB_ERR_STATE after bfb_set_agent_constants).
+ * The derivative is that of the step as computed: the LOD splitting, the
+ * active Dirichlet faces (their values are constants) and the agents'
+ * implicit update, with the factors held at this dt. dL/dD and dL/dlambda are
+ * summed in a fixed order (run-to-run identical). The env's field holds the
+ * final field afterwards. The reverse pass recomputes each segment from its
+ * checkpoint and keeps that segment's stage fields: device memory is about
+ * (n_steps/checkpoint_every + 3*checkpoint_every + 3) fields. BFB_STEP_BULK is
+ * not supported (BFB_ERR_UNSUPPORTED), nor lines whose two shared-memory tiles
+ * exceed 227 KB (n*32*2 elements on x and y). Synchronous: returns when the
+ * host gradients are written. */
+BFB_API int bfb_adjoint_run(bfb_env env, double dt, int n_steps, int flags, int checkpoint_every,
+                            const void *dL_dfinal, void *dL_dinitial, void *final_field, double *dL_dD,
+                            double *dL_dlambda, double *dL_dsecretion, double *dL_duptake, double *dL_dsaturation);
+
 /* No counterpart in the reference. The per-substrate FP64 sums of
  * bfb_checksum for callers that must not allocate device memory -- for
  * example code that owns its device buffers in its own pool, or a host loop

@@ -149,3 +149,63 @@ def test_adjoint_oracle_matches_finite_differences(oracle, rng):
         e[idx] = 1.0
         fd = (loss(rho + e, D, lam) - loss(rho - e, D, lam)) / 2
         assert abs(fd - g_rho[idx]) <= 1e-10
+
+
+def test_oracle_multistep_adjoint_with_agents_matches_finite_differences(oracle, rng):
+    """The composed reverse mode the GPU tests compare against (tests/adjoint_ref.py):
+    3 steps of (LOD step, agents) with Dirichlet faces, checked by central
+    differences of the oracle's own forward."""
+    from adjoint_ref import oracle_adjoint
+    shape, S, n = (5, 4, 6), 2, 3
+    dx, dt = 20.0, 0.01
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-2, 1.0, S)
+    rho = rng.random((*shape, S))
+    vals = rng.random((*shape, S))
+    fm = np.zeros((6, S), np.uint8)
+    fm[0, 0] = fm[3, 1] = fm[4, 0] = 1
+    na = 12
+    pos = rng.uniform(0, 1, (na, 3)) * np.array(shape) * dx
+    pos[:4] = pos[0]
+    ag = dict(pos=pos, vol=rng.uniform(500, 3000, na), active=(np.arange(na) % 5 != 3).astype(np.uint8))
+    ag["sec"], ag["upt"], ag["sat"] = log_uniform(rng, 1e-2, 10.0, (3, na, S))
+    w = rng.standard_normal((*shape, S))
+    g = oracle_adjoint(oracle, rho, w, n, dt, dx, D, lam, (vals, fm), ag)
+
+    def loss(r=rho, Dv=D, lv=lam, a=ag):
+        return float((oracle_adjoint(oracle, r, w, n, dt, dx, Dv, lv, (vals, fm), a)["final"] * w).sum())
+
+    def central(f, h):
+        return (f(h) - f(-h)) / (2 * h)
+
+    for q in range(S):
+        def fD(e, q=q):
+            Dp = D.copy()
+            Dp[q] += e
+            return loss(Dv=Dp)
+        assert abs(central(fD, 1e-4 * D[q]) - g["D"][q]) <= 1e-6 * max(1e-3, abs(g["D"][q]))
+
+        def fL(e, q=q):
+            Lp = lam.copy()
+            Lp[q] += e
+            return loss(lv=Lp)
+        assert abs(central(fL, 1e-4 * lam[q]) - g["lambda"][q]) <= 1e-6 * max(1e-3, abs(g["lambda"][q]))
+    key = {"secretion": "sec", "uptake": "upt", "saturation": "sat"}
+    for a in range(na):
+        for name, k in key.items():
+            d = a % S
+
+            def fA(e, a=a, d=d, k=k):
+                b = dict(ag)
+                b[k] = ag[k].copy()
+                b[k][a, d] += e
+                return loss(a=b)
+            fd = central(fA, 1e-3 * ag[k][a, d])
+            if not ag["active"][a]:
+                assert g[name][a, d] == 0.0 and fd == 0.0
+            else:
+                assert abs(fd - g[name][a, d]) <= 1e-6 * max(1e-6, abs(g[name][a, d])), (name, a)
+    for idx in [(0, 0, 0, 0), (2, 1, 3, 1), (4, 3, 5, 0)]:
+        e = np.zeros_like(rho)
+        e[idx] = 1e-3
+        fd = (loss(r=rho + e) - loss(r=rho - e)) / 2e-3
+        assert abs(fd - g["initial"][idx]) <= 1e-9
