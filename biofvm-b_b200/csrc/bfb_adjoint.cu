@@ -11,95 +11,285 @@
 //     mu_y = A_y^-1 (1 - M) mu_z,  mu_x = A_x^-1 (1 - M) mu_y,  dL/du = (1 - M) mu_x
 //     dL/dc1 -= sum_a mu_a^T Lap y_a,  dL/dc2 -= sum_a mu_a^T y_a
 // where Lap = dA/dc1 is tridiag(-1, 2, -1) with end diagonals 1 (0 when n = 1),
-// c1 = dt D/dx^2 and c2 = dt lambda/3. The oracle holds the same derivation
-// (oracle/lod_oracle.c: orc_lod_step_adjoint) for the tests.
+// c1 = dt D/dx^2 and c2 = dt lambda/3 (A = (1 + c2) I + c1 Lap). The oracle
+// holds the same derivation (oracle/lod_oracle.c: orc_lod_step_adjoint).
 //
-// Each adjoint sweep is one kernel: a warp stages the stage input (s0, s1 or
-// s2) and the incoming adjoint for 32 lines into shared memory, solves both
-// systems with the forward factors (y_a and mu_a), adds mu.Lap y and mu.y per
-// line into a slot of a partial-sum buffer, and writes mu_a. The per-substrate
-// sums are reduced in a fixed order, so the gradients are deterministic.
+// Kernels. One adjoint sweep is two launches:
+//   * the solve mu_a = A_a^-1 (1 - M) lam: the forward sweep's kernels with
+//     the mask on the load (x / y: TMA tiles of 32 lines in row groups on
+//     per-group mbarriers, z: 1-D bulk copies of whole rows), one read and
+//     one write of the field;
+//   * the sums mu.Lap y and mu.y over the new mu and the forward sweep's
+//     stored output s_(a+1) = Dir(y_a): one thread per line, two reads.
+// Staging y beside the adjoint in the solve's shared memory instead halves
+// the lines in flight per SM and left that kernel latency-bound at ~12% of
+// HBM bandwidth (one warp per SM sub-partition); the split costs one extra
+// read of mu and keeps both launches bandwidth-bound. Grids the TMA path
+// cannot describe use cp.async kernels that do both steps in one launch.
+// y_a differs from the stored s_(a+1) only on active faces. On lines that lie
+// inside a face of another axis the masked adjoint is zero, so mu is zero and
+// y does not matter; at the two ends of a line on the sweep's own faces, y is
+// rebuilt from the end row of A y = s, whose right side is the face value:
+//   y_0 = (g_0 + c1 y_1) / (1 + c1 + c2)  (and the mirror at n-1; a 2x2 solve
+//   when n = 2 and both ends are faces; g/(1 + c2) when n = 1).
+// dL/du = (1 - M) mu_x is not formed: its two readers mask on their own
+// loads (the agents' adjoint of the step before, and the z solve), and
+// adjoint_mask_kernel masks the returned dL/d(initial field).
+// Per-substrate sums: each warp reduces its lanes per substrate and adds the
+// result to its own slot of a partial buffer, across all steps; one kernel at
+// the end adds the slots in a fixed order. Gradients are run-to-run identical.
 //
-// Checkpointing: the forward run keeps the field every K steps. The reverse
-// pass walks the segments backwards; for each it recomputes the K steps from
-// the checkpoint with out-of-place sweeps, keeping u, s1, s2 of every step and
-// the pre-agent values at agent voxels, then reverses them.
+// Checkpointing: the forward pass keeps the field at the start of every
+// K-step segment except the last, whose stage fields it writes directly. The
+// reverse pass walks the segments backwards; each earlier segment is
+// recomputed from its checkpoint with out-of-place sweeps that keep, per step,
+// s1, s2 and the step's output (and the pre-agent values at occupied voxels).
 #include <algorithm>
 #include <vector>
 
 #include "bfb_aux.cuh"
 #include "bfb_tiles.cuh"
+#include "bfb_tma.cuh"
 
 namespace bfb {
 
-// One line solved in place with the forward factors (any right-hand side).
-template <typename T>
-__device__ __forceinline__ void thomas_inplace(LineSolver<T> &L, T *line, int ls, int n, int m0) {
-    line[0] = L.first(line[0], line[min(1, n - 1) * ls]);
-    const int hend = min(n - 1, m0);
-    int k = 1;
-    for (; k < hend; ++k) line[k * ls] = L.template fwd<false>(line[k * ls], k);
-#pragma unroll 4
-    for (; k < n - 1; ++k) line[k * ls] = L.template fwd<true>(line[k * ls], k);
-    if (n > 1) L.template fwd<false>(line[(n - 1) * ls], n - 1);
-    line[(n - 1) * ls] = L.out_last();
-    const int tl = max(m0, 1);
-    k = n - 2;
-#pragma unroll 4
-    for (; k >= tl; --k) line[k * ls] = L.template bwd<true>(line[k * ls], k);
-    for (; k >= 0; --k) line[k * ls] = L.template bwd<false>(line[k * ls], k);
-}
+// Terms of the adjoint sweeps besides the forward's SweepArgs.
+struct AdjTerms {
+    const double *c1;  // [S] dt*D/dx^2
+    const double *c2;  // [S] dt*lambda/3
+    double *part;      // [tiles of this sweep][S][2] running sums (mu.Lap y, mu.y)
+};
 
-// mu.Lap y and mu.y along one line (FP64 accumulation)
-template <typename T>
-__device__ __forceinline__ void line_dots(const T *y, const T *mu, int ls, int n, double &dl, double &dy) {
-    for (int m = 0; m < n; ++m) {
-        const double ym = (double)y[m * ls], mm = (double)mu[m * ls];
-        double lap = 0.0;
-        if (n > 1) {
-            if (m == 0) lap = ym - (double)y[ls];
-            else if (m == n - 1) lap = ym - (double)y[(m - 1) * ls];
-            else lap = 2.0 * ym - (double)y[(m - 1) * ls] - (double)y[(m + 1) * ls];
+__device__ __forceinline__ double shfl_xor_d(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+
+// Adds this warp's per-substrate sums of (dl, dy) to slot[d][2]. Lanes
+// without a line pass dl = dy = 0. `d` is the lane's substrate.
+__device__ __forceinline__ void tile_partials(double dl, double dy, int d, int S, double *__restrict__ slot) {
+    const int lane = threadIdx.x & 31;
+    if (32 % S == 0) {  // lanes of one substrate are lane = d (mod S)
+        for (int o = 16; o >= S; o >>= 1) {
+            dl += shfl_xor_d(dl, o);
+            dy += shfl_xor_d(dy, o);
         }
-        dl += mm * lap;
-        dy += mm * ym;
+        if (lane < S) {
+            slot[2 * lane] += dl;
+            slot[2 * lane + 1] += dy;
+        }
+    } else {
+        for (int q = 0; q < S; ++q) {
+            double u = d == q ? dl : 0.0, w = d == q ? dy : 0.0;
+            for (int o = 16; o > 0; o >>= 1) {
+                u += shfl_xor_d(u, o);
+                w += shfl_xor_d(w, o);
+            }
+            if (lane == 0) {
+                slot[2 * q] += u;
+                slot[2 * q + 1] += w;
+            }
+        }
     }
 }
 
-// Adjoint of one strided sweep (x: axis 0 with PRE_DIR, y: axis 1).
-//   a.f  = stage input (u for x, with the step's leading Dirichlet applied here)
-//   lam  = incoming adjoint; a.fo = mu out; part = [tiles*32][2] slot sums
-template <typename T, bool PRE_DIR>
-__global__ void __launch_bounds__(32) adjoint_strided_kernel(SweepArgs<T> a, const T *__restrict__ lam, StridedGeom g,
-                                                             double *__restrict__ part) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// The forward sweep's y at a line's two ends when they lie on the sweep's own
+// active faces (see the file comment); FP64.
+struct EndFix {
+    bool lo = false, hi = false;
+    double y0 = 0.0, yn = 0.0;
+    __device__ __forceinline__ void make(bool lo_dir, bool hi_dir, int n, double c1, double c2, double g0, double gn,
+                                         double y1_stored, double yn2_stored) {
+        lo = lo_dir;
+        hi = hi_dir;
+        if (!lo && !hi) return;
+        const double a1 = 1.0 + c1 + c2;
+        if (n == 1) {
+            y0 = yn = g0 / (1.0 + c2);
+        } else if (n == 2 && lo && hi) {
+            const double det = a1 * a1 - c1 * c1;
+            y0 = (a1 * g0 + c1 * gn) / det;
+            yn = (c1 * g0 + a1 * gn) / det;
+        } else {
+            // with n == 2 and one face end, the other end's stored value is y itself
+            if (lo) y0 = (g0 + c1 * y1_stored) / a1;
+            if (hi) yn = (gn + c1 * yn2_stored) / a1;
+        }
+    }
+};
+
+// mu.Lap y and mu.y at row m of a line; yv(q) returns y at row q (FP64).
+template <typename YV>
+__device__ __forceinline__ void dots_at(int m, int n, double mu, YV yv, double &dl, double &dy) {
+    const double yc = yv(m);
+    double lap = 0.0;
+    if (n > 1) {
+        if (m == 0)
+            lap = yc - yv(1);
+        else if (m == n - 1)
+            lap = yc - yv(n - 2);
+        else
+            lap = 2.0 * yc - yv(m - 1) - yv(m + 1);
+    }
+    dl += mu * lap;
+    dy += mu * yc;
+}
+
+// ---------------------------------------------------------------------------
+// Strided adjoint solve with TMA (rank 2: x, rank 3: y): mu = A^-1 (1 - M) lam
+// for the 32 lines of a warp, with the forward sweep's pipeline (one tile,
+// row groups on their own mbarriers, finished groups stored while the lower
+// ones are computed). The sums over mu and y are left to adjoint_dots_kernel.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128)
+    adjoint_solve_strided_tma_kernel(const __grid_constant__ CUtensorMap map_l,
+                                     const __grid_constant__ CUtensorMap map_mu, SweepArgs<T> a, StridedGeom g,
+                                     int crow) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (tile >= (long long)g.n_slabs * g.ncb) return;
+    const int slab = (int)(tile / g.ncb);
+    const int col0 = (int)((tile % g.ncb) * 32);
+    const int n = g.n;
+    const long long P = g.P;
+    const int nch = (n + crow - 1) / crow;
+    const int rank = g.axis == 0 ? 2 : 3;
+    unsigned char *wbase = smem_raw + (size_t)warp * strided_tma_warp_bytes(n, crow, sizeof(T));
+    const unsigned bar0 = smem_u32(wbase);
+    T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
+    const unsigned sm_u32 = smem_u32(sm);
+    const unsigned chunk_bytes = (unsigned)crow * 32u * (unsigned)sizeof(T);
+
+    if (lane == 0) {
+        for (int ch = 0; ch < nch; ++ch) mbar_init(bar0 + 8 * ch, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    if (lane == 0) {
+        for (int ch = 0; ch < nch; ++ch) {
+            mbar_expect_tx(bar0 + 8 * ch, chunk_bytes);
+            tma_load(sm_u32 + ch * chunk_bytes, &map_l, col0, ch * crow, slab, rank, bar0 + 8 * ch);
+        }
+    }
+
+    const long long col = (long long)col0 + lane;
+    const bool valid = col < P;
+    const int S = a.S;
+    const int d = (int)(col % S);
+    int ci, cj, ck;
+    if (g.axis == 0) {
+        const long long q = col / S;
+        ck = (int)(q % a.nz);
+        cj = (int)(q / a.nz);
+        ci = 0;
+    } else {
+        ck = (int)(col / S);
+        ci = slab;
+        cj = 0;
+    }
+    const unsigned m = (a.dir.any && valid) ? a.dir.mask[d] : 0u;
+    bool col_dir, lo_dir, hi_dir;
+    if (g.axis == 0) {
+        col_dir = ((m & 4u) && cj == 0) || ((m & 8u) && cj == a.ny - 1) || ((m & 16u) && ck == 0) ||
+                  ((m & 32u) && ck == a.nz - 1);
+        lo_dir = m & 1u;
+        hi_dir = m & 2u;
+    } else {
+        col_dir = ((m & 1u) && ci == 0) || ((m & 2u) && ci == a.nx - 1) || ((m & 16u) && ck == 0) ||
+                  ((m & 32u) && ck == a.nz - 1);
+        lo_dir = m & 4u;
+        hi_dir = m & 8u;
+    }
+    auto wait_group = [&](int ch) -> bool {
+        if (mbar_wait(bar0 + 8 * ch, 0)) return true;
+        if (lane == 0) atomicOr(a.err, 1);
+        return false;
+    };
+    // masked adjoint: interior rows lose only whole lines on other faces,
+    // the end rows also their own faces
+    auto xin = [&](int q) -> T { return col_dir ? T(0) : sm[q * 32 + lane]; };
+    auto xend = [&](int q) -> T {
+        return (col_dir || (q == 0 && lo_dir) || (q == n - 1 && hi_dir)) ? T(0) : sm[q * 32 + lane];
+    };
+    LineSolver<T> L(a, d);
+    const int m0 = a.fac.m0;
+
+    // ---- forward elimination, row group by row group as the copies land
+    const int rref = min(1, n - 1);
+    const int ref_ch = rref / crow;
+    for (int ch = 0; ch <= ref_ch; ++ch)
+        if (!wait_group(ch)) return;
+    sm[lane] = L.first(xend(0), xend(rref));
+    int r = 1;
+    for (int ch = 0; ch < nch; ++ch) {
+        if (ch > ref_ch && !wait_group(ch)) return;
+        const int rend = min(n - 1, (ch + 1) * crow);
+        const int hend = min(rend, m0);
+        for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(xin(r), r);
+#pragma unroll 8
+        for (; r < rend; ++r) sm[r * 32 + lane] = L.template fwd<true>(xin(r), r);
+    }
+    if (n > 1) L.template fwd<false>(xend(n - 1), n - 1);
+
+    // ---- back substitution into the tile; each finished row group is stored
+    sm[(n - 1) * 32 + lane] = L.out_last();
+    const int tl = max(m0, 1);
+    r = n - 2;
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        const int rlo = ch * crow;
+        const int tstop = max(rlo, tl);
+#pragma unroll 8
+        for (; r >= tstop; --r) sm[r * 32 + lane] = L.template bwd<true>(sm[r * 32 + lane], r);
+        const int hstop = max(rlo, 1);
+        for (; r >= hstop; --r) sm[r * 32 + lane] = L.template bwd<false>(sm[r * 32 + lane], r);
+        if (rlo == 0 && n > 1) sm[lane] = L.template bwd<false>(sm[lane], 0);
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+            tma_store(&map_mu, col0, rlo, slab, rank, sm_u32 + ch * chunk_bytes);
+            bulk_commit();
+        }
+    }
+    if (lane == 0) bulk_wait_read_all();
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Strided adjoint sweep with cp.async (grids TMA cannot describe).
+//   a.f: incoming adjoint, yin: stored s_(a+1), a.fo: output mu
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(32) adjoint_strided_kernel(SweepArgs<T> a, const T *__restrict__ yin, StridedGeom g,
+                                                             AdjTerms t) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x;
     const long long tile = blockIdx.x;
     const int n = g.n;
     const long long P = g.P;
-    T *smX = reinterpret_cast<T *>(smem_raw);
-    T *smL = smX + (size_t)n * 32;
+    T *sl = reinterpret_cast<T *>(smem_raw);
+    T *sy = sl + (size_t)n * 32;
     const int slab = (int)(tile / g.ncb);
     const long long col0 = (tile % g.ncb) * 32;
     const int ncols = (int)min((long long)32, P - col0);
     const size_t off = (size_t)slab * g.slab_stride + col0;
     if (lane < ncols)
         for (int r = 0; r < n; ++r) {
-            cp_async<sizeof(T)>(smX + r * 32 + lane, a.f + off + (size_t)r * P + lane);
-            cp_async<sizeof(T)>(smL + r * 32 + lane, lam + off + (size_t)r * P + lane);
+            cp_async<sizeof(T)>(sl + r * 32 + lane, a.f + off + (size_t)r * P + lane);
+            cp_async<sizeof(T)>(sy + r * 32 + lane, yin + off + (size_t)r * P + lane);
         }
     cp_commit();
     cp_wait<0>();
     __syncwarp();
+    const bool valid = lane < ncols;
+    const long long col = col0 + lane;
+    const int S = a.S, d = (int)(col % S);
     double dl = 0.0, dy = 0.0;
-    if (lane < ncols) {
-        const long long col = col0 + lane;
-        const int S = a.S, d = (int)(col % S);
+    if (valid) {
         int ci, cj, ck;
         if (g.axis == 0) {
-            const long long t = col / S;
-            ck = (int)(t % a.nz);
-            cj = (int)(t / a.nz);
+            const long long q = col / S;
+            ck = (int)(q % a.nz);
+            cj = (int)(q / a.nz);
             ci = 0;
         } else {
             ck = (int)(col / S);
@@ -119,117 +309,357 @@ __global__ void __launch_bounds__(32) adjoint_strided_kernel(SweepArgs<T> a, con
             lo_dir = m & 4u;
             hi_dir = m & 8u;
         }
-        T *xl = smX + lane, *ll = smL + lane;
-        if (PRE_DIR) {
-            if (lo_dir) xl[0] = g.axis == 0 ? dir_value(a.dir, 0, cj, ck, d) : dir_value(a.dir, ci, 0, ck, d);
-            if (hi_dir)
-                xl[(n - 1) * 32] =
-                    g.axis == 0 ? dir_value(a.dir, n - 1, cj, ck, d) : dir_value(a.dir, ci, n - 1, ck, d);
-        }
+        T *ll = sl + lane;
+        const T *yl = sy + lane;
         if (col_dir) {
-            for (int r = 0; r < n; ++r) ll[r * 32] = T(0);
+            for (int q = 0; q < n; ++q) ll[q * 32] = T(0);
         } else {
             if (lo_dir) ll[0] = T(0);
             if (hi_dir) ll[(n - 1) * 32] = T(0);
         }
-        LineSolver<T> L1(a, d), L2(a, d);
-        thomas_inplace(L1, xl, 32, n, a.fac.m0);
-        thomas_inplace(L2, ll, 32, n, a.fac.m0);
-        line_dots(xl, ll, 32, n, dl, dy);
+        EndFix fx;
+        if (!col_dir && (lo_dir || hi_dir)) {
+            auto gv = [&](int q) -> double {
+                return (double)(g.axis == 0 ? dir_value(a.dir, q, cj, ck, d) : dir_value(a.dir, ci, q, ck, d));
+            };
+            fx.make(lo_dir, hi_dir, n, t.c1[d], t.c2[d], gv(0), gv(n - 1), n > 1 ? (double)yl[32] : 0.0,
+                    n > 1 ? (double)yl[(n - 2) * 32] : 0.0);
+        }
+        auto yv = [&](int q) -> double {
+            if (q == 0 && fx.lo) return fx.y0;
+            if (q == n - 1 && fx.hi) return fx.yn;
+            return (double)yl[q * 32];
+        };
+        LineSolver<T> Ls(a, d);
+        const int m0 = a.fac.m0;
+        ll[0] = Ls.first(ll[0], ll[min(1, n - 1) * 32]);
+        const int hend = min(n - 1, m0);
+        int k = 1;
+        for (; k < hend; ++k) ll[k * 32] = Ls.template fwd<false>(ll[k * 32], k);
+        for (; k < n - 1; ++k) ll[k * 32] = Ls.template fwd<true>(ll[k * 32], k);
+        if (n > 1) Ls.template fwd<false>(ll[(n - 1) * 32], n - 1);
         T *out = a.fo + off + lane;
-        for (int r = 0; r < n; ++r) out[(size_t)r * P] = ll[r * 32];
+        T mu = Ls.out_last();
+        dots_at(n - 1, n, (double)mu, yv, dl, dy);
+        out[(size_t)(n - 1) * P] = mu;
+        const int tl = max(m0, 1);
+        for (k = n - 2; k >= tl; --k) {
+            mu = Ls.template bwd<true>(ll[k * 32], k);
+            dots_at(k, n, (double)mu, yv, dl, dy);
+            out[(size_t)k * P] = mu;
+        }
+        for (; k >= 0; --k) {
+            mu = Ls.template bwd<false>(ll[k * 32], k);
+            dots_at(k, n, (double)mu, yv, dl, dy);
+            out[(size_t)k * P] = mu;
+        }
     }
-    part[2 * ((size_t)tile * 32 + lane)] = dl;
-    part[2 * ((size_t)tile * 32 + lane) + 1] = dy;
+    tile_partials(dl, dy, d, S, t.part + (size_t)tile * S * 2);
 }
 
-// Adjoint of the contiguous z sweep; line t = (r, d) of the tile is row
-// row0 + r, substrate d, and lanes take lines t = lane, lane + 32, ...
-// Slot t of the tile (LPT slots, a multiple of 32 >= R*S) gets that line's sums.
+// ---------------------------------------------------------------------------
+// Contiguous (z) adjoint solve, the forward pipe kernel's pipeline; S <= 32,
+// lane (r, d) owns line (row0 + r, d). SC: substrate count when a
+// compile-time constant.
+// ---------------------------------------------------------------------------
+template <typename T, int SC>
+__global__ void __launch_bounds__(128) adjoint_solve_contig_pipe_kernel(SweepArgs<T> a, ContigGeom g, int kc) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    const long long row0 = tile * g.R;
+    if (row0 >= g.nrows) return;
+    const int nr = (int)min((long long)g.R, g.nrows - row0);
+    const int S = SC > 0 ? SC : a.S;
+    const int nz = g.nz;
+    const int L = nz * S;
+    const int nch = (nz + kc - 1) / kc;
+    const size_t wbytes = (128 + (size_t)g.R * g.RS * sizeof(T) + 127) / 128 * 128;
+    unsigned char *wbase = smem_raw + (size_t)warp * wbytes;
+    const unsigned bar0 = smem_u32(wbase);
+    T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
+    const T *__restrict__ base = a.f + (size_t)row0 * L;
+    T *__restrict__ obase = a.fo + (size_t)row0 * L;
+    auto seg_bytes = [&](int c) -> unsigned { return (unsigned)((min(nz, (c + 1) * kc) - c * kc) * S * (int)sizeof(T)); };
+
+    if (lane == 0) {
+        for (int c = 0; c < nch; ++c) mbar_init(bar0 + 8 * c, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    if (lane == 0) {
+        for (int c = 0; c < nch; ++c) {
+            const unsigned b = seg_bytes(c);
+            mbar_expect_tx(bar0 + 8 * c, b * (unsigned)nr);
+            for (int r = 0; r < nr; ++r)
+                bulk_load(smem_u32(sm + (size_t)r * g.RS + (size_t)c * kc * S), base + (size_t)r * L + (size_t)c * kc * S,
+                          b, bar0 + 8 * c);
+        }
+    }
+    auto wait_c = [&](int c) -> bool {
+        if (mbar_wait(bar0 + 8 * c, 0)) return true;
+        if (lane == 0) atomicOr(a.err, 1);
+        return false;
+    };
+
+    const bool active = lane < nr * S;
+    const int r = active ? lane / S : 0;
+    const int d = active ? lane - r * S : 0;
+    const long long row = row0 + r;
+    const int i = (int)(row / a.ny), j = (int)(row % a.ny);
+    const unsigned m = (a.dir.any && active) ? a.dir.mask[d] : 0u;
+    const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
+                          ((m & 8u) && j == a.ny - 1);
+    const bool lo_dir = m & 16u, hi_dir = m & 32u;
+    T *line = sm + (size_t)r * g.RS + d;
+    auto xin = [&](int q) -> T { return line_dir ? T(0) : line[q * S]; };
+    auto xend = [&](int q) -> T {
+        return (line_dir || (q == 0 && lo_dir) || (q == nz - 1 && hi_dir)) ? T(0) : line[q * S];
+    };
+    LineSolver<T> Ls(a, d);
+    const int m0 = a.fac.m0;
+
+    const int kref = min(1, nz - 1);
+    const int ref_c = kref / kc;
+    for (int c = 0; c <= ref_c; ++c)
+        if (!wait_c(c)) return;
+    if (active) line[0] = Ls.first(xend(0), xend(kref));
+    int k = 1;
+    for (int c = 0; c < nch; ++c) {
+        if (c > ref_c && !wait_c(c)) return;
+        const int kend = min(nz - 1, (c + 1) * kc);
+        if (active) {
+            const int hend = min(kend, m0);
+            for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(xin(k), k);
+#pragma unroll 8
+            for (; k < kend; ++k) line[k * S] = Ls.template fwd<true>(xin(k), k);
+        }
+        k = max(k, kend);
+    }
+    if (active && nz > 1) Ls.template fwd<false>(xend(nz - 1), nz - 1);
+
+    if (active) line[(nz - 1) * S] = Ls.out_last();
+    const int tl = max(m0, 1);
+    k = nz - 2;
+    for (int c = nch - 1; c >= 0; --c) {
+        const int klo = c * kc;
+        if (active) {
+            const int tstop = max(klo, tl);
+#pragma unroll 8
+            for (; k >= tstop; --k) line[k * S] = Ls.template bwd<true>(line[k * S], k);
+            const int hstop = max(klo, 1);
+            for (; k >= hstop; --k) line[k * S] = Ls.template bwd<false>(line[k * S], k);
+            if (klo == 0 && nz > 1) line[0] = Ls.template bwd<false>(line[0], 0);
+        }
+        k = min(k, klo - 1);
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+            const unsigned b = seg_bytes(c);
+            for (int q = 0; q < nr; ++q)
+                bulk_store(obase + (size_t)q * L + (size_t)klo * S, smem_u32(sm + (size_t)q * g.RS + (size_t)klo * S), b);
+            bulk_commit();
+        }
+    }
+    if (lane == 0) bulk_wait_read_all();
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// The sums of one adjoint sweep: sum_m mu_m y_m and the edge form of
+// mu.Lap y, sum_(m < n-1) (mu_m - mu_(m+1)) (y_m - y_(m+1)), with y's face
+// ends rebuilt (EndFix). Each line is cut into segments of `seg` rows and one
+// thread walks one segment (rows [s*seg, s*seg + seg) and the edge out of its
+// last row). Element m of line l is at (l / inner) * n * inner + (l % inner)
+// + m * inner; thread g takes line g % nlines, segment g / nlines, so
+// consecutive threads read consecutive addresses on the x and y axes and
+// consecutive substrates on z. blockDim = S * 2^p, so a thread's substrate is
+// threadIdx.x % S and the per-substrate block sums are a fixed-order tree.
+// ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(32) adjoint_contig_kernel(SweepArgs<T> a, const T *__restrict__ lam, ContigGeom g,
-                                                            int LPT, double *__restrict__ part) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(256) adjoint_dots_kernel(const T *__restrict__ mu, const T *__restrict__ y,
+                                                           DirFaces<T> dir, int axis, int n, long long inner,
+                                                           long long nlines, int seg, AdjTerms t) {
+    __shared__ double s0[256], s1[256];
+    const int S = dir.S;
+    const int tid = threadIdx.x;
+    const int d = tid % S;
+    const long long gidx = (long long)blockIdx.x * blockDim.x + tid;
+    const long long nsegs = (long long)((n + seg - 1) / seg);
+    double dl = 0.0, dyy = 0.0;
+    if (gidx < nlines * nsegs) {
+        const long long l = gidx % nlines;
+        const int q0 = (int)(gidx / nlines) * seg;
+        const int q1 = min(n, q0 + seg);  // rows [q0, q1); edges (m, m+1) for m in [q0, q1), m + 1 < n
+        const long long outer = l / inner;
+        const size_t base = (size_t)outer * n * inner + (size_t)(l - outer * inner);
+        const T *__restrict__ mp = mu + base;
+        const T *__restrict__ yp = y + base;
+        const unsigned msk = dir.any ? dir.mask[d] : 0u;
+        const bool lo = msk & (1u << (2 * axis)), hi = msk & (2u << (2 * axis));
+        EndFix fx;
+        // rebuilt ends are read by the segments holding rows 0, n-2 and n-1
+        if ((lo || hi) && (q0 == 0 || q1 >= n - 1)) {
+            const long long v0 = (long long)(base / S);  // voxel of element 0
+            const long long yz = (long long)dir.ny * dir.nz;
+            const int vi = (int)(v0 / yz), vj = (int)((v0 / dir.nz) % dir.ny), vk = (int)(v0 % dir.nz);
+            auto gv = [&](int q) -> double {
+                int ii = vi, jj = vj, kk = vk;
+                if (axis == 0) ii = q; else if (axis == 1) jj = q; else kk = q;
+                return (double)dir_value(dir, ii, jj, kk, d);
+            };
+            fx.make(lo, hi, n, t.c1[d], t.c2[d], gv(0), gv(n - 1), n > 1 ? (double)yp[inner] : 0.0,
+                    n > 1 ? (double)yp[(size_t)(n - 2) * inner] : 0.0);
+        }
+        auto yat = [&](int q) -> double {
+            if (q == 0 && fx.lo) return fx.y0;
+            if (q == n - 1 && fx.hi) return fx.yn;
+            return (double)yp[(size_t)q * inner];
+        };
+        double mprev = (double)mp[(size_t)q0 * inner];
+        double yprev = yat(q0);
+        dyy = mprev * yprev;
+        double dl1 = 0.0, dy1 = 0.0;  // second accumulators: two independent chains
+        const int qe = min(q1 + 1, n);  // last row read (edge partner of row q1 - 1)
+        int q = q0 + 1;
+        // interior rows (not 0, not n-1): plain loads
+        const int qi = min(qe, n - 1);
+#pragma unroll 2
+        for (; q + 1 < qi; q += 2) {
+            const double ma = (double)mp[(size_t)q * inner], ya = (double)yp[(size_t)q * inner];
+            const double mb = (double)mp[(size_t)(q + 1) * inner], yb = (double)yp[(size_t)(q + 1) * inner];
+            dl += (mprev - ma) * (yprev - ya);
+            dl1 += (ma - mb) * (ya - yb);
+            if (q < q1) dyy += ma * ya;
+            if (q + 1 < q1) dy1 += mb * yb;
+            mprev = mb;
+            yprev = yb;
+        }
+        for (; q < qe; ++q) {
+            const double ma = (double)mp[(size_t)q * inner], ya = yat(q);
+            dl += (mprev - ma) * (yprev - ya);
+            if (q < q1) dyy += ma * ya;
+            mprev = ma;
+            yprev = ya;
+        }
+        dl += dl1;
+        dyy += dy1;
+    }
+    s0[tid] = dl;
+    s1[tid] = dyy;
+    __syncthreads();
+    for (int h = blockDim.x / S / 2; h >= 1; h >>= 1) {
+        if (tid < h * S) {
+            s0[tid] += s0[tid + h * S];
+            s1[tid] += s1[tid + h * S];
+        }
+        __syncthreads();
+    }
+    if (tid < S) {
+        double *slot = t.part + ((size_t)blockIdx.x * S + tid) * 2;
+        slot[0] += s0[tid];
+        slot[1] += s1[tid];
+    }
+}
+
+// Contiguous adjoint sweep with cp.async (any S; lines t = lane, lane + 32, ...).
+template <typename T>
+__global__ void __launch_bounds__(32) adjoint_contig_kernel(SweepArgs<T> a, const T *__restrict__ yin, ContigGeom g,
+                                                            AdjTerms t) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x;
     const long long tile = blockIdx.x;
     const long long row0 = tile * g.R;
     const int nr = (int)min((long long)g.R, g.nrows - row0);
     const int S = a.S, nz = g.nz, L = nz * S;
-    T *smX = reinterpret_cast<T *>(smem_raw);
-    T *smL = smX + (size_t)g.R * g.RS;
-    const T *X = a.f + (size_t)row0 * L;
-    const T *Lm = lam + (size_t)row0 * L;
+    T *sl = reinterpret_cast<T *>(smem_raw);
+    T *sy = sl + (size_t)g.R * g.RS;
+    const T *Lm = a.f + (size_t)row0 * L;
+    const T *Y = yin + (size_t)row0 * L;
     for (int e = lane; e < nr * L; e += 32) {
         const int r = e / L, q = e - r * L;
-        cp_async<sizeof(T)>(smX + (size_t)r * g.RS + q, X + e);
-        cp_async<sizeof(T)>(smL + (size_t)r * g.RS + q, Lm + e);
+        cp_async<sizeof(T)>(sl + (size_t)r * g.RS + q, Lm + e);
+        cp_async<sizeof(T)>(sy + (size_t)r * g.RS + q, Y + e);
     }
     cp_commit();
     cp_wait<0>();
     __syncwarp();
-    double *slot = part + 2 * (size_t)tile * LPT;
-    for (int t = lane; t < LPT; t += 32) {
+    double *slot = t.part + (size_t)tile * S * 2;
+    const int rounds = (g.R * S + 31) / 32;
+    for (int rd = 0; rd < rounds; ++rd) {
+        const int tt = rd * 32 + lane;
         double dl = 0.0, dy = 0.0;
-        if (t < nr * S) {
-            const int r = t / S, d = t - r * S;
+        int d = -1;
+        if (tt < nr * S) {
+            const int r = tt / S;
+            d = tt - r * S;
             const long long row = row0 + r;
             const int i = (int)(row / a.ny), j = (int)(row % a.ny);
             const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
             const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
                                   ((m & 8u) && j == a.ny - 1);
             const bool lo_dir = m & 16u, hi_dir = m & 32u;
-            T *xl = smX + (size_t)r * g.RS + d, *ll = smL + (size_t)r * g.RS + d;
+            T *ll = sl + (size_t)r * g.RS + d;
+            const T *yl = sy + (size_t)r * g.RS + d;
             if (line_dir) {
-                for (int k = 0; k < nz; ++k) ll[k * S] = T(0);
+                for (int q = 0; q < nz; ++q) ll[q * S] = T(0);
             } else {
                 if (lo_dir) ll[0] = T(0);
                 if (hi_dir) ll[(nz - 1) * S] = T(0);
             }
-            LineSolver<T> L1(a, d), L2(a, d);
-            thomas_inplace(L1, xl, S, nz, a.fac.m0);
-            thomas_inplace(L2, ll, S, nz, a.fac.m0);
-            line_dots(xl, ll, S, nz, dl, dy);
+            EndFix fx;
+            if (!line_dir && (lo_dir || hi_dir))
+                fx.make(lo_dir, hi_dir, nz, t.c1[d], t.c2[d], (double)dir_value(a.dir, i, j, 0, d),
+                        (double)dir_value(a.dir, i, j, nz - 1, d), nz > 1 ? (double)yl[S] : 0.0,
+                        nz > 1 ? (double)yl[(nz - 2) * S] : 0.0);
+            auto yv = [&](int q) -> double {
+                if (q == 0 && fx.lo) return fx.y0;
+                if (q == nz - 1 && fx.hi) return fx.yn;
+                return (double)yl[q * S];
+            };
+            LineSolver<T> Ls(a, d);
+            const int m0 = a.fac.m0;
+            ll[0] = Ls.first(ll[0], ll[min(1, nz - 1) * S]);
+            const int hend = min(nz - 1, m0);
+            int k = 1;
+            for (; k < hend; ++k) ll[k * S] = Ls.template fwd<false>(ll[k * S], k);
+            for (; k < nz - 1; ++k) ll[k * S] = Ls.template fwd<true>(ll[k * S], k);
+            if (nz > 1) Ls.template fwd<false>(ll[(nz - 1) * S], nz - 1);
+            T mu = Ls.out_last();
+            dots_at(nz - 1, nz, (double)mu, yv, dl, dy);
+            ll[(nz - 1) * S] = mu;
+            const int tl = max(m0, 1);
+            for (k = nz - 2; k >= tl; --k) {
+                mu = Ls.template bwd<true>(ll[k * S], k);
+                dots_at(k, nz, (double)mu, yv, dl, dy);
+                ll[k * S] = mu;
+            }
+            for (; k >= 0; --k) {
+                mu = Ls.template bwd<false>(ll[k * S], k);
+                dots_at(k, nz, (double)mu, yv, dl, dy);
+                ll[k * S] = mu;
+            }
         }
-        slot[2 * t] = dl;
-        slot[2 * t + 1] = dy;
+        tile_partials(dl, dy, d, S, slot);
     }
     __syncwarp();
     T *O = a.fo + (size_t)row0 * L;
     for (int e = lane; e < nr * L; e += 32) {
         const int r = e / L, q = e - r * L;
-        O[e] = smL[(size_t)r * g.RS + q];
+        O[e] = sl[(size_t)r * g.RS + q];
     }
 }
 
-// Per-substrate sums of the slot partials, in slot order: block d adds the
-// slots of substrate d into gacc[d] (mu.Lap y) and gacc[S + d] (mu.y).
-// Strided sweeps: 32 slots per tile, slot = column. Contiguous sweep: LPT
-// slots per tile, slot = line (r, d) of the tile.
-__global__ void adjoint_reduce_kernel(const double *__restrict__ part, long long ntiles, int strided, long long P,
-                                      int ncb, int S, int LPT, int R, long long nrows, double *__restrict__ gacc) {
+// gacc[d] = sum over slots of part[slot][d][0], gacc[S + d] likewise for [1];
+// block d adds its slots in a fixed order.
+__global__ void adjoint_reduce_kernel(const double *__restrict__ part, long long nslots, int S, double *__restrict__ gacc) {
     __shared__ double s0[256], s1[256];
     const int d = blockIdx.x;
-    const int per = strided ? 32 : LPT;
-    const long long nslots = ntiles * per;
     double a0 = 0.0, a1 = 0.0;
     for (long long q = threadIdx.x; q < nslots; q += blockDim.x) {
-        const long long tile = q / per;
-        const int t = (int)(q % per);
-        int dq;
-        bool valid;
-        if (strided) {
-            const long long col = (tile % ncb) * 32 + t;
-            valid = col < P;
-            dq = (int)(col % S);
-        } else {
-            const int nr = (int)min((long long)R, nrows - tile * R);
-            valid = t < nr * S;
-            dq = t % S;
-        }
-        if (valid && dq == d) {
-            a0 += part[2 * q];
-            a1 += part[2 * q + 1];
-        }
+        a0 += part[(q * S + d) * 2];
+        a1 += part[(q * S + d) * 2 + 1];
     }
     s0[threadIdx.x] = a0;
     s1[threadIdx.x] = a1;
@@ -242,8 +672,8 @@ __global__ void adjoint_reduce_kernel(const double *__restrict__ part, long long
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        gacc[d] += s0[0];
-        gacc[S + d] += s1[0];
+        gacc[d] = s0[0];
+        gacc[S + d] = s1[0];
     }
 }
 
@@ -272,31 +702,21 @@ __global__ void adjoint_mask_kernel(T *f, DirFaces<T> dir) {
         j = (int)(q % dir.ny);
     }
     const size_t vb = (((size_t)i * dir.ny + j) * dir.nz + k) * dir.S;
-    for (int d = 0; d < dir.S; ++d) {
-        const unsigned m = dir.mask[d];
-        if (((m & 1u) && i == 0) || ((m & 2u) && i == dir.nx - 1) || ((m & 4u) && j == 0) ||
-            ((m & 8u) && j == dir.ny - 1) || ((m & 16u) && k == 0) || ((m & 32u) && k == dir.nz - 1))
-            f[vb + d] = T(0);
-    }
+    for (int d = 0; d < dir.S; ++d)
+        if (on_active_face(dir.mask[d], i, j, k, dir.nx, dir.ny, dir.nz)) f[vb + d] = T(0);
 }
 
+// Agents' update of a recomputed step, keeping the pre-agent values v.
 template <typename T>
-__global__ void gather_occ_kernel(const T *__restrict__ f, const int *__restrict__ seg_voxel, int n_occ, int S,
-                                  T *__restrict__ out) {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (long long)n_occ * S) return;
-    out[e] = f[(size_t)seg_voxel[e / S] * S + (e % S)];
-}
-
-template <typename T>
-__global__ void cells_on_kernel(T *__restrict__ f, int S, int n_occ, const int *__restrict__ seg_start,
-                                const int *__restrict__ seg_voxel, const T *__restrict__ t1,
-                                const T *__restrict__ t2) {
+__global__ void cells_keep_kernel(T *__restrict__ f, int S, int n_occ, const int *__restrict__ seg_start,
+                                  const int *__restrict__ seg_voxel, const T *__restrict__ t1, const T *__restrict__ t2,
+                                  T *__restrict__ vkeep) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)n_occ * S) return;
     const int s = (int)(e / S), d = (int)(e % S);
     const size_t fe = (size_t)seg_voxel[s] * S + d;
     T x = f[fe];
+    vkeep[e] = x;
     for (int q = seg_start[s]; q < seg_start[s + 1]; ++q) {
         const size_t z = (size_t)q * S + d;
         if constexpr (sizeof(T) == 8)
@@ -310,20 +730,30 @@ __global__ void cells_on_kernel(T *__restrict__ f, int S, int n_occ, const int *
 // Cells^T at one (voxel, substrate): the agents of the voxel applied
 // x_k = (x_(k-1) + t1_k)/t2_k in list order; backwards,
 // dL/dt1_k += g/t2_k, dL/dt2_k -= g x_k/t2_k, g <- g/t2_k. The x_k are
-// replayed from the pre-agent value v (x_0).
+// replayed from the pre-agent value v = x_0, which is also written back into
+// the step's output w (turning it into Dir(y_z) for the z adjoint).
+// With `dir` active (every step but the run's last), lam is the next step's
+// mu_x, and its active-face entries are masked here: the next step's leading
+// Dirichlet overwrote those voxels.
 template <typename T>
-__global__ void cells_adjoint_kernel(T *__restrict__ lam, const T *__restrict__ vocc, int S, int n_occ,
-                                     const int *__restrict__ seg_start, const int *__restrict__ seg_voxel,
+__global__ void cells_adjoint_kernel(T *__restrict__ lam, T *__restrict__ w, const T *__restrict__ vkeep, int S,
+                                     int n_occ, const int *__restrict__ seg_start, const int *__restrict__ seg_voxel,
                                      const T *__restrict__ t1, const T *__restrict__ t2, double *__restrict__ gt1,
-                                     double *__restrict__ gt2) {
+                                     double *__restrict__ gt2, DirFaces<T> dir) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)n_occ * S) return;
     const int s = (int)(e / S), d = (int)(e % S);
-    const size_t fe = (size_t)seg_voxel[s] * S + d;
+    const int vox = seg_voxel[s];
+    const size_t fe = (size_t)vox * S + d;
     const int q0 = seg_start[s], q1 = seg_start[s + 1];
+    const T v = vkeep[e];
     double g = (double)lam[fe];
+    if (dir.any) {
+        const int k = vox % dir.nz, j = (vox / dir.nz) % dir.ny, i = vox / (dir.nz * dir.ny);
+        if (on_active_face(dir.mask[d], i, j, k, dir.nx, dir.ny, dir.nz)) g = 0.0;
+    }
     for (int k = q1 - 1; k >= q0; --k) {
-        double x = (double)vocc[e];  // replay x_k
+        double x = (double)v;  // replay x_k
         for (int q = q0; q <= k; ++q) x = (x + (double)t1[(size_t)q * S + d]) / (double)t2[(size_t)q * S + d];
         const double tt = (double)t2[(size_t)k * S + d];
         gt1[(size_t)k * S + d] += g / tt;
@@ -331,6 +761,7 @@ __global__ void cells_adjoint_kernel(T *__restrict__ lam, const T *__restrict__ 
         g /= tt;
     }
     lam[fe] = (T)g;
+    w[fe] = v;
 }
 
 }  // namespace bfb
@@ -361,6 +792,7 @@ struct Carve {
     }
 };
 
+// A field-sized buffer with its x (0) and y (1) tensor maps.
 struct Buf {
     void *p = nullptr;
     CUtensorMap map[2];
@@ -368,44 +800,190 @@ struct Buf {
     int crow[2] = {0, 0};
 };
 
+template <typename K>
+void opt_in(K k) {
+    cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+}
+
+template <typename T>
+void opt_in_all() {
+    static int done_dev = -1;  // per instantiation (precision)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (done_dev == dev) return;
+    opt_in(adjoint_solve_strided_tma_kernel<T>);
+    opt_in(adjoint_strided_kernel<T>);
+    opt_in(adjoint_solve_contig_pipe_kernel<T, 1>);
+    opt_in(adjoint_solve_contig_pipe_kernel<T, 2>);
+    opt_in(adjoint_solve_contig_pipe_kernel<T, 4>);
+    opt_in(adjoint_solve_contig_pipe_kernel<T, 8>);
+    opt_in(adjoint_solve_contig_pipe_kernel<T, 0>);
+    opt_in(adjoint_contig_kernel<T>);
+    done_dev = dev;
+}
+
+template <typename T>
+struct Adjoint {
+    bfb_env_s *env = nullptr;
+    double dt = 0;
+    cudaStream_t st = nullptr;
+    int S = 0;
+    StridedGeom gx, gy;
+    ContigGeom gz;
+    int kc = 0;  // z row-group length of the pipelined kernel (0: the cp.async kernel)
+    const double *coef = nullptr;  // [2S]: c1, c2
+    double *part_x = nullptr, *part_y = nullptr, *part_z = nullptr;
+    long long tiles_z = 0;
+
+    void map(Buf &b) {
+        for (int a = 0; a < 2; ++a)
+            b.ok[a] = env->use_tma && make_sweep_tensor_map(&b.map[a], &b.crow[a], b.p, sizeof(T), a, env->nx,
+                                                            env->ny, env->nz, S);
+    }
+
+    // one forward sweep, out of place
+    int fwd(int axis, Buf &in, Buf &out) {
+        SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
+        a.f = static_cast<T *>(in.p);
+        a.fo = static_cast<T *>(out.p);
+        if (axis < 2) {
+            const bool tma = in.ok[axis] && out.ok[axis];
+            return launch_strided<T>(a, axis, axis == 0, 1, tma ? &in.map[axis] : nullptr,
+                                     tma ? &out.map[axis] : nullptr, in.crow[axis], st);
+        }
+        return launch_contig<T>(a, 1, env->use_tma != 0, st);
+    }
+
+    // the sums of one sweep over the stored y and the new mu
+    static constexpr int kDotSeg = 64;  // rows per thread in the sums kernel
+    int dots_threads() const {
+        int threads = S;
+        while (threads * 2 <= 256) threads *= 2;
+        return threads;
+    }
+    long long dots_blocks(int axis) const {
+        const int n = axis == 0 ? env->nx : (axis == 1 ? env->ny : env->nz);
+        const long long work = (long long)env->N / n * ((n + kDotSeg - 1) / kDotSeg);
+        return (work + dots_threads() - 1) / dots_threads();
+    }
+    int dots(int axis, const SweepArgs<T> &a, const T *mu, const T *y, const AdjTerms &t) {
+        const int n = axis == 0 ? env->nx : (axis == 1 ? env->ny : env->nz);
+        const long long inner = axis == 0 ? (long long)env->ny * env->nz * S : (axis == 1 ? (long long)env->nz * S : S);
+        const long long nlines = (long long)env->N / n;
+        adjoint_dots_kernel<T><<<(unsigned)dots_blocks(axis), dots_threads(), 0, st>>>(mu, y, a.dir, axis, n, inner,
+                                                                                       nlines, kDotSeg, t);
+        BFB_CUDA(cudaGetLastError());
+        return BFB_OK;
+    }
+
+    // one adjoint sweep: lam (in) and y (stored forward output) -> mu (out)
+    int adj(int axis, Buf &lam, Buf &y, Buf &mu) {
+        SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
+        a.f = static_cast<T *>(lam.p);
+        a.fo = static_cast<T *>(mu.p);
+        const AdjTerms t{coef, coef + S, axis == 0 ? part_x : (axis == 1 ? part_y : part_z)};
+        const T *yp = static_cast<const T *>(y.p);
+        if (axis < 2) {
+            const StridedGeom &g = axis == 0 ? gx : gy;
+            const unsigned tiles = (unsigned)((long long)g.n_slabs * g.ncb);
+            if (lam.ok[axis] && mu.ok[axis]) {
+                const int crow = lam.crow[axis];
+                const size_t wb = strided_tma_warp_bytes(g.n, crow, sizeof(T));
+                if (wb <= (size_t)kMaxSmem) {
+                    adjoint_solve_strided_tma_kernel<T><<<tiles, 32, wb, st>>>(lam.map[axis], mu.map[axis], a, g, crow);
+                    BFB_CUDA(cudaGetLastError());
+                    return dots(axis, a, static_cast<const T *>(mu.p), yp, t);
+                }
+            }
+            const size_t smem = 2 * (size_t)g.n * 32 * sizeof(T);
+            if (smem > (size_t)kMaxSmem) return fail(BFB_ERR_UNSUPPORTED, "adjoint: lines too long for shared memory");
+            adjoint_strided_kernel<T><<<tiles, 32, smem, st>>>(a, yp, g, t);
+            BFB_CUDA(cudaGetLastError());
+            return BFB_OK;
+        }
+        const unsigned tiles = (unsigned)tiles_z;
+        if (kc > 0) {
+            const size_t wb = (128 + (size_t)gz.R * gz.RS * sizeof(T) + 127) / 128 * 128;
+            switch (S) {
+            case 1: adjoint_solve_contig_pipe_kernel<T, 1><<<tiles, 32, wb, st>>>(a, gz, kc); break;
+            case 2: adjoint_solve_contig_pipe_kernel<T, 2><<<tiles, 32, wb, st>>>(a, gz, kc); break;
+            case 4: adjoint_solve_contig_pipe_kernel<T, 4><<<tiles, 32, wb, st>>>(a, gz, kc); break;
+            case 8: adjoint_solve_contig_pipe_kernel<T, 8><<<tiles, 32, wb, st>>>(a, gz, kc); break;
+            default: adjoint_solve_contig_pipe_kernel<T, 0><<<tiles, 32, wb, st>>>(a, gz, kc); break;
+            }
+            BFB_CUDA(cudaGetLastError());
+            return dots(2, a, static_cast<const T *>(mu.p), yp, t);
+        }
+        const size_t smem = 2 * (size_t)gz.R * gz.RS * sizeof(T);
+        if (smem > (size_t)kMaxSmem) return fail(BFB_ERR_UNSUPPORTED, "adjoint: rows too long for shared memory");
+        adjoint_contig_kernel<T><<<tiles, 32, smem, st>>>(a, yp, gz, t);
+        BFB_CUDA(cudaGetLastError());
+        return BFB_OK;
+    }
+};
+
 template <typename T>
 int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const void *dL_dfinal, void *dL_dinitial,
                 void *final_field, double *gD, double *gL, double *gsec, double *gupt, double *gsat) {
     const int S = env->S;
-    const size_t N = (size_t)env->N;
-    const size_t fb = N * sizeof(T);
+    const size_t fb = (size_t)env->N * sizeof(T);
     cudaStream_t st = env->stream;
     const bool cells = (flags & BFB_STEP_CELLS) && env->n_occ > 0;
     int rc = env_prepare_step(env, dt, BFB_STEP_DIFFUSION);
     if (rc) return rc;
-    StridedGeom gx, gy;
-    ContigGeom gz;
+    Adjoint<T> A;
+    A.env = env;
+    A.dt = dt;
+    A.st = st;
+    A.S = S;
     int vb16[3];
-    if ((rc = env_tile_plan(env, sizeof(T), &gx, &gy, &gz, vb16))) return rc;
+    if ((rc = env_tile_plan(env, sizeof(T), &A.gx, &A.gy, &A.gz, vb16))) return rc;
+    opt_in_all<T>();
+    const long long tiles_x = (long long)A.gx.n_slabs * A.gx.ncb, tiles_y = (long long)A.gy.n_slabs * A.gy.ncb;
+    A.tiles_z = (A.gz.nrows + A.gz.R - 1) / A.gz.R;
+    {   // pipelined z solve: the forward pipe kernel's alignment rules
+        const long long L = (long long)env->nz * S;
+        const int eb = (int)sizeof(T);
+        const size_t wb = (128 + (size_t)A.gz.R * A.gz.RS * eb + 127) / 128 * 128;
+        if (env->use_tma && S <= 32 && (L * eb) % 16 == 0 && ((long long)A.gz.RS * eb) % 16 == 0 &&
+            wb <= (size_t)kMaxSmem) {
+            int q = 16;
+            for (int v = S * eb; v % 2 == 0 && q > 1; v /= 2) q /= 2;  // q = 16 / gcd(16, S*elem)
+            const int kc = (env->nz + kChunks - 1) / kChunks;
+            A.kc = (kc + q - 1) / q * q;
+        }
+    }
 
+    // ---- workspace
     const int nseg = (n_steps + K - 1) / K;
-    const int LPT = (gz.R * S + 31) / 32 * 32;  // partial slots per contiguous tile
-    const long long slots_x = (long long)gx.n_slabs * gx.ncb * 32, slots_y = (long long)gy.n_slabs * gy.ncb * 32,
-                    slots_z = (gz.nrows + gz.R - 1) / gz.R * LPT;
-    const long long slots = std::max(slots_x, std::max(slots_y, slots_z));
-    const size_t occ = (size_t)env->n_occ * S, nact = (size_t)env->n_active * S;
-    std::vector<T *> ckpt(nseg);
-    std::vector<Buf> U(K + 1), S1(K), S2(K);
-    T *lam = nullptr, *mu = nullptr, *vocc = nullptr;
-    double *part = nullptr, *gacc = nullptr, *gt1 = nullptr, *gt2 = nullptr;
+    const size_t occ = (size_t)env->n_occ * S;
+    const size_t nact = (size_t)env->n_active * S;
+    // partial-sum slots per axis: tiles of the fused fallback kernels or blocks of the sums kernel
+    const long long reg_x = std::max(tiles_x, A.dots_blocks(0)), reg_y = std::max(tiles_y, A.dots_blocks(1)),
+                    reg_z = std::max(A.tiles_z, A.dots_blocks(2));
+    const long long slots = reg_x + reg_y + reg_z;
+    std::vector<T *> ckpt(nseg - 1);
+    std::vector<Buf> S1(K), S2(K), W(K);
+    Buf lam, mu, ck;
+    T *vkeep = nullptr;
+    double *part = nullptr, *gacc = nullptr, *gt1 = nullptr, *gt2 = nullptr, *coef = nullptr;
     auto carve = [&](Carve &c) {
         for (auto &p : ckpt) c.take(&p, fb);
-        for (auto *v : {&U, &S1, &S2})
+        for (auto *v : {&S1, &S2, &W})
             for (auto &b : *v) {
                 T *p;
                 c.take(&p, fb);
                 b.p = p;
             }
-        c.take(&lam, fb);
-        c.take(&mu, fb);
-        c.take(&part, sizeof(double) * 2 * slots);
+        for (Buf *b : {&lam, &mu}) {
+            T *p;
+            c.take(&p, fb);
+            b->p = p;
+        }
+        c.take(&part, sizeof(double) * 2 * S * slots);
         c.take(&gacc, sizeof(double) * 2 * S);
-        c.take(&vocc, sizeof(T) * occ * K);
+        c.take(&coef, sizeof(double) * 2 * S);
+        c.take(&vkeep, sizeof(T) * occ * K);
         c.take(&gt1, sizeof(double) * nact);
         c.take(&gt2, sizeof(double) * nact);
     };
@@ -416,7 +994,7 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
         cudaFree(env->adj_ws);
         env->adj_ws = nullptr;
         env->adj_ws_bytes = 0;
-        cudaError_t e = cudaMalloc(&env->adj_ws, sizing.off);
+        const cudaError_t e = cudaMalloc(&env->adj_ws, sizing.off);
         if (e != cudaSuccess) {
             env->adj_ws = nullptr;
             return cuda_fail(e, "cudaMalloc (adjoint workspace)");
@@ -426,118 +1004,109 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
     Carve c;
     c.base = static_cast<char *>(env->adj_ws);
     carve(c);
-    for (auto *v : {&U, &S1, &S2})
-        for (auto &b : *v)
-            for (int a = 0; a < 2; ++a)
-                b.ok[a] = env->use_tma && make_sweep_tensor_map(&b.map[a], &b.crow[a], b.p, sizeof(T), a, env->nx,
-                                                                env->ny, env->nz, S);
-    BFB_CUDA(cudaMemsetAsync(gacc, 0, sizeof(double) * 2 * S, st));
+    for (auto *v : {&S1, &S2, &W})
+        for (auto &b : *v) A.map(b);
+    A.map(lam);
+    A.map(mu);
+    A.part_x = part;
+    A.part_y = part + 2 * S * reg_x;
+    A.part_z = part + 2 * S * (reg_x + reg_y);
+    // c1 and c2 as the factor precompute forms them, at the dt the factors hold
+    const double fdt = env->factor_dt;
+    std::vector<double> hcoef(2 * S);
+    for (int d = 0; d < S; ++d) {
+        double c1 = env->D[d] * fdt;
+        c1 /= env->dx;
+        c1 /= env->dx;
+        double c2 = env->lambda[d] * fdt;
+        c2 /= 3.0;
+        hcoef[d] = c1;
+        hcoef[S + d] = c2;
+    }
+    A.coef = coef;
+    BFB_CUDA(cudaMemcpyAsync(coef, hcoef.data(), sizeof(double) * 2 * S, cudaMemcpyHostToDevice, st));
+    BFB_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * 2 * S * slots, st));
     if (nact) {
         BFB_CUDA(cudaMemsetAsync(gt1, 0, sizeof(double) * nact, st));
         BFB_CUDA(cudaMemsetAsync(gt2, 0, sizeof(double) * nact, st));
     }
-
-    // ---- forward with checkpoints (the env's own fast path)
-    const int fwd_flags = BFB_STEP_DIFFUSION | (cells ? BFB_STEP_CELLS : 0);
-    for (int c = 0; c < nseg; ++c) {
-        BFB_CUDA(cudaMemcpyAsync(ckpt[c], env->field, fb, cudaMemcpyDeviceToDevice, st));
-        const int len = std::min(K, n_steps - c * K);
-        if ((rc = bfb_simulate(env, dt, len, fwd_flags))) return rc;
-    }
-    if (final_field) BFB_CUDA(cudaMemcpyAsync(final_field, env->field, fb, cudaMemcpyDeviceToDevice, st));
-    BFB_CUDA(cudaMemcpyAsync(lam, dL_dfinal, fb, cudaMemcpyDeviceToDevice, st));
-
-    // launch helpers
-    const int warps = 1;
-    auto fwd_sweep = [&](int axis, Buf &in, Buf &out) -> int {
-        SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
-        a.f = static_cast<T *>(in.p);
-        a.fo = static_cast<T *>(out.p);
-        if (axis < 2) {
-            const bool tma = in.ok[axis] && out.ok[axis];
-            return launch_strided<T>(a, axis, axis == 0, warps, tma ? &in.map[axis] : nullptr,
-                                     tma ? &out.map[axis] : nullptr, in.crow[axis], st);
-        }
-        return launch_contig<T>(a, warps, env->use_tma != 0, st);
-    };
-    auto dirfaces = [&]() {
-        SweepArgs<T> a = env_sweep_args<T>(env, 0, dt);
-        return a.dir;
-    };
-    auto adj_sweep = [&](int axis, const T *X, const T *lin, T *mout) -> int {
-        SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
-        a.f = const_cast<T *>(X);
-        a.fo = mout;
-        if (axis < 2) {
-            const StridedGeom &g = axis == 0 ? gx : gy;
-            const size_t smem = 2 * (size_t)g.n * 32 * sizeof(T);
-            if (smem > 227 * 1024) return fail(BFB_ERR_UNSUPPORTED, "adjoint: lines too long for shared memory");
-            const unsigned blocks = (unsigned)((long long)g.n_slabs * g.ncb);
-            if (axis == 0) {
-                cudaFuncSetAttribute(adjoint_strided_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024);
-                adjoint_strided_kernel<T, true><<<blocks, 32, smem, st>>>(a, lin, g, part);
-            } else {
-                cudaFuncSetAttribute(adjoint_strided_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024);
-                adjoint_strided_kernel<T, false><<<blocks, 32, smem, st>>>(a, lin, g, part);
-            }
-            BFB_CUDA(cudaGetLastError());
-            adjoint_reduce_kernel<<<S, 256, 0, st>>>(part, blocks, 1, g.P, g.ncb, S, 32, 0, 0, gacc);
-        } else {
-            const size_t smem = 2 * (size_t)gz.R * gz.RS * sizeof(T);
-            if (smem > 227 * 1024) return fail(BFB_ERR_UNSUPPORTED, "adjoint: rows too long for shared memory");
-            const unsigned blocks = (unsigned)((gz.nrows + gz.R - 1) / gz.R);
-            cudaFuncSetAttribute(adjoint_contig_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            adjoint_contig_kernel<T><<<blocks, 32, smem, st>>>(a, lin, gz, LPT, part);
-            BFB_CUDA(cudaGetLastError());
-            adjoint_reduce_kernel<<<S, 256, 0, st>>>(part, blocks, 0, 0, 0, S, LPT, gz.R, gz.nrows, gacc);
-        }
-        BFB_CUDA(cudaGetLastError());
-        return BFB_OK;
-    };
-    const DirFaces<T> dir = dirfaces();
-    const long long nface = 2 * ((long long)env->ny * env->nz + (long long)env->nx * env->nz +
-                                 (long long)env->nx * env->ny);
-    auto mask = [&](T *f) -> int {
-        if (!dir.any) return BFB_OK;
-        adjoint_mask_kernel<T><<<(unsigned)((nface + 255) / 256), 256, 0, st>>>(f, dir);
-        BFB_CUDA(cudaGetLastError());
-        return BFB_OK;
-    };
     const unsigned occ_blocks = (unsigned)((occ + 255) / 256);
     const T *t1 = static_cast<const T *>(env->ag_t1), *t2 = static_cast<const T *>(env->ag_t2);
 
-    // ---- reverse, segment by segment
-    for (int c = nseg - 1; c >= 0; --c) {
-        const int len = std::min(K, n_steps - c * K);
-        BFB_CUDA(cudaMemcpyAsync(U[0].p, ckpt[c], fb, cudaMemcpyDeviceToDevice, st));
-        for (int j = 0; j < len; ++j) {  // recompute, keeping every stage input
-            if ((rc = fwd_sweep(0, U[j], S1[j])) || (rc = fwd_sweep(1, S1[j], S2[j])) ||
-                (rc = fwd_sweep(2, S2[j], U[j + 1])))
-                return rc;
+    // len forward steps from `in`, keeping s1, s2 and every step's output
+    auto segment = [&](Buf &in, int len) -> int {
+        for (int j = 0; j < len; ++j) {
+            int r;
+            if ((r = A.fwd(0, j == 0 ? in : W[j - 1], S1[j])) || (r = A.fwd(1, S1[j], S2[j])) ||
+                (r = A.fwd(2, S2[j], W[j])))
+                return r;
             if (cells) {
-                gather_occ_kernel<T><<<occ_blocks, 256, 0, st>>>(static_cast<T *>(U[j + 1].p), env->seg_voxel,
-                                                                 env->n_occ, S, vocc + (size_t)j * occ);
-                cells_on_kernel<T><<<occ_blocks, 256, 0, st>>>(static_cast<T *>(U[j + 1].p), S, env->n_occ,
-                                                               env->seg_start, env->seg_voxel, t1, t2);
+                cells_keep_kernel<T><<<occ_blocks, 256, 0, st>>>(static_cast<T *>(W[j].p), S, env->n_occ,
+                                                                 env->seg_start, env->seg_voxel, t1, t2,
+                                                                 vkeep + (size_t)j * occ);
                 BFB_CUDA(cudaGetLastError());
             }
         }
-        for (int j = len - 1; j >= 0; --j) {  // reverse each step
+        return BFB_OK;
+    };
+
+    // ---- forward: checkpoints of the earlier segments, stage fields of the last
+    const int fwd_flags = BFB_STEP_DIFFUSION | (cells ? BFB_STEP_CELLS : 0);
+    for (int s = 0; s < nseg - 1; ++s) {
+        BFB_CUDA(cudaMemcpyAsync(ckpt[s], env->field, fb, cudaMemcpyDeviceToDevice, st));
+        if ((rc = bfb_simulate(env, dt, K, fwd_flags))) return rc;
+    }
+    const int last_len = n_steps - (nseg - 1) * K;
+    {
+        Buf f;
+        f.p = env->field;
+        for (int a = 0; a < 2; ++a) {
+            f.ok[a] = env->use_tma && env->tma_ok[a];
+            f.map[a] = env->tmap[a];
+            f.crow[a] = env->tma_crow[a];
+        }
+        if ((rc = segment(f, last_len))) return rc;
+    }
+    BFB_CUDA(cudaMemcpyAsync(env->field, W[last_len - 1].p, fb, cudaMemcpyDeviceToDevice, st));
+    if (final_field) BFB_CUDA(cudaMemcpyAsync(final_field, W[last_len - 1].p, fb, cudaMemcpyDeviceToDevice, st));
+    BFB_CUDA(cudaMemcpyAsync(lam.p, dL_dfinal, fb, cudaMemcpyDeviceToDevice, st));
+
+    // ---- reverse, segment by segment
+    const DirFaces<T> dirf = env_sweep_args<T>(env, 0, dt).dir;
+    Buf *pl = &lam, *pm = &mu;
+    for (int s = nseg - 1; s >= 0; --s) {
+        const int len = s == nseg - 1 ? last_len : K;
+        if (s < nseg - 1) {
+            ck.p = ckpt[s];
+            A.map(ck);
+            if ((rc = segment(ck, len))) return rc;
+        }
+        for (int j = len - 1; j >= 0; --j) {
             if (cells) {
-                cells_adjoint_kernel<T><<<occ_blocks, 256, 0, st>>>(lam, vocc + (size_t)j * occ, S, env->n_occ,
-                                                                    env->seg_start, env->seg_voxel, t1, t2, gt1, gt2);
+                DirFaces<T> dj = dirf;
+                if (s == nseg - 1 && j == len - 1) dj.any = 0;  // dL/d(final field) is not masked
+                cells_adjoint_kernel<T><<<occ_blocks, 256, 0, st>>>(
+                    static_cast<T *>(pl->p), static_cast<T *>(W[j].p), vkeep + (size_t)j * occ, S, env->n_occ,
+                    env->seg_start, env->seg_voxel, t1, t2, gt1, gt2, dj);
                 BFB_CUDA(cudaGetLastError());
             }
-            if ((rc = adj_sweep(2, static_cast<T *>(S2[j].p), lam, mu))) return rc;
-            if ((rc = adj_sweep(1, static_cast<T *>(S1[j].p), mu, lam))) return rc;
-            if ((rc = adj_sweep(0, static_cast<T *>(U[j].p), lam, mu))) return rc;
-            if ((rc = mask(mu))) return rc;
-            std::swap(lam, mu);  // lam = dL/du of this step's input
+            if ((rc = A.adj(2, *pl, W[j], *pm))) return rc;
+            if ((rc = A.adj(1, *pm, S2[j], *pl))) return rc;
+            if ((rc = A.adj(0, *pl, S1[j], *pm))) return rc;
+            std::swap(pl, pm);  // *pl = dL/du of this step's input
         }
     }
-    if (dL_dinitial) BFB_CUDA(cudaMemcpyAsync(dL_dinitial, lam, fb, cudaMemcpyDeviceToDevice, st));
+    if (dL_dinitial) {
+        if (dirf.any) {
+            const long long nface = 2 * ((long long)env->ny * env->nz + (long long)env->nx * env->nz +
+                                         (long long)env->nx * env->ny);
+            adjoint_mask_kernel<T><<<(unsigned)((nface + 255) / 256), 256, 0, st>>>(static_cast<T *>(pl->p), dirf);
+            BFB_CUDA(cudaGetLastError());
+        }
+        BFB_CUDA(cudaMemcpyAsync(dL_dinitial, pl->p, fb, cudaMemcpyDeviceToDevice, st));
+    }
+    adjoint_reduce_kernel<<<S, 256, 0, st>>>(part, slots, S, gacc);
+    BFB_CUDA(cudaGetLastError());
 
     // ---- gradients to the caller
     std::vector<double> acc(2 * S);
@@ -551,7 +1120,10 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
                                  st));
     }
     BFB_CUDA(cudaStreamSynchronize(st));
-    const double kD = -dt / (env->dx * env->dx), kL = -dt / 3.0;
+    int herr = 0;
+    BFB_CUDA(cudaMemcpy(&herr, env->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return fail(BFB_ERR_WATCHDOG, "adjoint: a device-side wait ran out of its iteration limit");
+    const double kD = -fdt / (env->dx * env->dx), kL = -fdt / 3.0;
     for (int d = 0; d < S; ++d) {
         if (gD) gD[d] = kD * acc[d];
         if (gL) gL[d] = kL * acc[S + d];
@@ -567,12 +1139,12 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
         const double dV = (env->dx * env->dx) * env->dx;
         for (int q = 0; q < env->n_active; ++q) {
             const int a = order[q];
-            const double c = env->agent_dt * env->h_vol[a] / dV;
+            const double cc = env->agent_dt * env->h_vol[a] / dV;
             for (int d = 0; d < S; ++d) {
                 const size_t qa = (size_t)q * S + d, la = (size_t)a * S + d;
-                if (gsec) gsec[la] = h1[qa] * c * env->h_sat[la] + h2[qa] * c;
-                if (gupt) gupt[la] = h2[qa] * c;
-                if (gsat) gsat[la] = h1[qa] * c * env->h_sec[la];
+                if (gsec) gsec[la] = h1[qa] * cc * env->h_sat[la] + h2[qa] * cc;
+                if (gupt) gupt[la] = h2[qa] * cc;
+                if (gsat) gsat[la] = h1[qa] * cc * env->h_sec[la];
             }
         }
     }

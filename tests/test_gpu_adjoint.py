@@ -92,6 +92,7 @@ def _rel(a, b):
     (7, 3, (12, 10, 17), 3, 0),
     (5, 2, (10, 12, 11), 2, 120),
     (4, 4, (33, 9, 40), 1, 60),
+    (3, 2, (24, 20, 32), 8, 150),
 ])
 def test_adjoint_fp64_matches_oracle(bfb, oracle, n_steps, K, shape, S, agents):
     rng = np.random.default_rng(500 + n_steps * 7 + S)
@@ -121,10 +122,10 @@ def test_adjoint_is_deterministic(bfb):
     env.close()
 
 
-def _loss_fd(bfb, env, rho0, w, n_steps, dt, flags):
+def _field_fd(bfb, env, rho0, n_steps, dt, flags):
     env.set_field(rho0)
     env.simulate(dt, n_steps, flags)
-    return float(np.sum(w * env.get_field()))
+    return env.get_field()
 
 
 def test_adjoint_fp64_matches_finite_differences(bfb):
@@ -138,12 +139,14 @@ def test_adjoint_fp64_matches_finite_differences(bfb):
     g = _gpu_adjoint(bfb, env, rho0, w, n, dt, 2, ag)
 
     def fd(apply, h):
+        # L = <w, u> is linear in u: difference the fields, then weight, so
+        # that the difference is not taken between two large sums
         apply(+h)
-        lp = _loss_fd(bfb, env, rho0p[0], w, n, dt, flags)
+        up = _field_fd(bfb, env, rho0p[0], n, dt, flags)
         apply(-h)
-        lm = _loss_fd(bfb, env, rho0p[0], w, n, dt, flags)
+        um = _field_fd(bfb, env, rho0p[0], n, dt, flags)
         apply(0.0)
-        return (lp - lm) / (2 * h)
+        return float(np.sum(w * (up - um))) / (2 * h)
 
     rho0p = [rho0]
     checks = []
@@ -310,33 +313,41 @@ def test_inverse_problem_128cube_10k_agents(bfb):
     kinds = ["secretion", "uptake", "saturation"]
     samples += [(kinds[q % 3], (int(a), int(rng.integers(S)))) for q, a in enumerate(agents)]
     key = {"secretion": "sec", "uptake": "upt", "saturation": "sat"}
+    def perturbed_field(kind, idx, e):
+        # every call sets all parameters, perturbing only (kind, idx)
+        Dv, Lv = P["D"].copy(), P["lam"].copy()
+        arrs = {k: P[k].copy() for k in ("sec", "upt", "sat")}
+        if kind == "D":
+            Dv[idx] += e
+        elif kind == "lambda":
+            Lv[idx] += e
+        else:
+            arrs[key[kind]][idx] += e
+        env.set_coefficients(Dv, Lv)
+        env.set_agents(P["pos"], P["vol"], arrs["sec"], arrs["upt"], arrs["sat"], dt)
+        env.set_field(P["rho0"])
+        env.simulate(dt, steps, flags)
+        return env.get_field()
+
+    def central(kind, idx, h):
+        # L(+h) - L(-h) = sum (u+ - u-) ((u+ + u-)/2 - target): formed from the
+        # field difference, not as the difference of two large sums
+        up, um = perturbed_field(kind, idx, h), perturbed_field(kind, idx, -h)
+        return float(np.sum((up - um) * (0.5 * (up + um) - target))) / (2 * h)
+
     for kind, idx in samples:
         if kind in ("D", "lambda"):
-            base = P["D"] if kind == "D" else P["lam"]
-            h = 1e-4 * base[idx]
-            vals = []
-            for e in (h, -h):
-                arr = base.copy()
-                arr[idx] += e
-                env.set_coefficients(arr if kind == "D" else P["D"], arr if kind == "lambda" else P["lam"])
-                vals.append(loss()[0])
-            env.set_coefficients(P["D"], P["lam"])
+            h = 1e-3 * (P["D"] if kind == "D" else P["lam"])[idx]
             adj = g64[kind][idx]
         else:
-            a, d = idx
-            h = 1e-3 * P[key[kind]][a, d]
-            vals = []
-            for e in (h, -h):
-                arrs = {k: P[k] for k in ("sec", "upt", "sat")}
-                arrs[key[kind]] = P[key[kind]].copy()
-                arrs[key[kind]][a, d] += e
-                env.set_agents(P["pos"], P["vol"], arrs["sec"], arrs["upt"], arrs["sat"], dt)
-                vals.append(loss()[0])
-            env.set_agents(P["pos"], P["vol"], P["sec"], P["upt"], P["sat"], dt)
-            adj = g64[kind][a, d]
-        fdv = (vals[0] - vals[1]) / (2 * h)
-        scale = max(abs(g64["D"]).max(), 1e-300) if kind == "D" else max(abs(g64[kind]).max(), 1e-300)
+            h = 1e-3 * P[key[kind]][idx]
+            adj = g64[kind][idx]
+        # central differences at h and h/2, Richardson-extrapolated (error O(h^4))
+        fdv = (4 * central(kind, idx, h / 2) - central(kind, idx, h)) / 3
+        scale = max(abs(g64[kind]).max(), 1e-300)
         assert abs(fdv - adj) <= 1e-6 * max(abs(adj), 1e-3 * scale), (kind, idx, fdv, adj)
+    env.set_coefficients(P["D"], P["lam"])
+    env.set_agents(P["pos"], P["vol"], P["sec"], P["upt"], P["sat"], dt)
 
     # FP32 gradients against FP64
     env32 = make(bfb.FP32, P["sec"])
