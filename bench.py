@@ -311,6 +311,22 @@ def run_our_arm(args):
     e1.record(stream)
     e1.synchronize()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+
+    # reverse mode on the same FP32 env: n_adj steps, with and without segment recompute
+    n_adj = 20
+    w = torch.randn(V * S, device=f"cuda:{local}", dtype=torch.float32)
+    adj_ms = {}
+    for Kc in (n_adj, 5):
+        env.set_field(rho0)
+        torch.cuda.synchronize()
+        env.adjoint_run(DT, n_adj, w.data_ptr(), checkpoint_every=Kc)  # warm: workspace
+        env.set_field(rho0)
+        barrier()
+        e0.record(stream)
+        env.adjoint_run(DT, n_adj, w.data_ptr(), checkpoint_every=Kc)
+        e1.record(stream)
+        e1.synchronize()
+        adj_ms[Kc] = max_over_ranks(e0.elapsed_time(e1))
     env.close()
 
     if dist is not None:
@@ -365,6 +381,15 @@ def run_our_arm(args):
                 "path": "bfb_step_host: pinned FP64 host field -> device (FP32) -> 1 LOD step -> host"},
         "gpu_launches": 3 * K,
         "cpu_baseline": cpu,
+        "adjoint": {
+            "workload": f"bfb_adjoint_run, FP32 {NX}^3x{S}, {n_adj} steps, dL/du_final random",
+            "forward_ms_per_step": ms_step,
+            "run_ms_per_step": {f"checkpoint_every_{k}": v / n_adj for k, v in adj_ms.items()},
+            # the run = forward (writing the last segment's stage fields) + recompute of earlier segments + reverse
+            "reverse_ms_per_step": adj_ms[n_adj] / n_adj - ms_step,
+            "reverse_over_forward": (adj_ms[n_adj] / n_adj - ms_step) / ms_step,
+            "run_over_forward": {f"checkpoint_every_{k}": v / n_adj / ms_step for k, v in adj_ms.items()},
+        },
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -469,90 +469,152 @@ __global__ void __launch_bounds__(128) adjoint_solve_contig_pipe_kernel(SweepArg
 // ---------------------------------------------------------------------------
 // The sums of one adjoint sweep: sum_m mu_m y_m and the edge form of
 // mu.Lap y, sum_(m < n-1) (mu_m - mu_(m+1)) (y_m - y_(m+1)), with y's face
-// ends rebuilt (EndFix). Each line is cut into segments of `seg` rows and one
-// thread walks one segment (rows [s*seg, s*seg + seg) and the edge out of its
-// last row). Element m of line l is at (l / inner) * n * inner + (l % inner)
-// + m * inner; thread g takes line g % nlines, segment g / nlines, so
-// consecutive threads read consecutive addresses on the x and y axes and
-// consecutive substrates on z. blockDim = S * 2^p, so a thread's substrate is
-// threadIdx.x % S and the per-substrate block sums are a fixed-order tree.
+// ends rebuilt (EndFix). Each line is cut into segments of `seg` rows; one
+// thread walks one segment of VEC adjacent lines (rows [s*seg, s*seg + seg)
+// and the edge out of its last row) with 16-byte loads when VEC > 1.
+// Element m of line l is at (l / inner) * n * inner + (l % inner) + m * inner;
+// thread g takes lines VEC * (g % (nlines / VEC)) + [0, VEC) and segment
+// g / (nlines / VEC), so consecutive threads read consecutive addresses on
+// the x and y axes and consecutive substrates on z. blockDim = S * 2^p, so
+// slot VEC * threadIdx.x + u of the block belongs to substrate
+// (VEC * threadIdx.x + u) % S and the per-substrate sums are a fixed-order
+// tree.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int VEC>
+__device__ __forceinline__ void load_vec(const T *p, double (&o)[VEC]) {
+    if constexpr (VEC == 1) {
+        o[0] = (double)p[0];
+    } else {
+        static_assert(VEC == 2, "FP64 rows are read 2 at a time");
+        const double2 v = *reinterpret_cast<const double2 *>(p);
+        o[0] = v.x;
+        o[1] = v.y;
+    }
+}
+
+template <typename T, int VEC>
 __global__ void __launch_bounds__(256) adjoint_dots_kernel(const T *__restrict__ mu, const T *__restrict__ y,
                                                            DirFaces<T> dir, int axis, int n, long long inner,
                                                            long long nlines, int seg, AdjTerms t) {
-    __shared__ double s0[256], s1[256];
+    __shared__ double s0[256 * VEC], s1[256 * VEC];
     const int S = dir.S;
     const int tid = threadIdx.x;
-    const int d = tid % S;
+    const long long ngroups = nlines / VEC;
     const long long gidx = (long long)blockIdx.x * blockDim.x + tid;
     const long long nsegs = (long long)((n + seg - 1) / seg);
-    double dl = 0.0, dyy = 0.0;
-    if (gidx < nlines * nsegs) {
-        const long long l = gidx % nlines;
-        const int q0 = (int)(gidx / nlines) * seg;
+    double dl[VEC], dyy[VEC];
+#pragma unroll
+    for (int u = 0; u < VEC; ++u) dl[u] = dyy[u] = 0.0;
+    if (gidx < ngroups * nsegs) {
+        const long long l0 = (gidx % ngroups) * VEC;
+        const int q0 = (int)(gidx / ngroups) * seg;
         const int q1 = min(n, q0 + seg);  // rows [q0, q1); edges (m, m+1) for m in [q0, q1), m + 1 < n
-        const long long outer = l / inner;
-        const size_t base = (size_t)outer * n * inner + (size_t)(l - outer * inner);
+        const long long outer = l0 / inner;
+        const size_t base = (size_t)outer * n * inner + (size_t)(l0 - outer * inner);
         const T *__restrict__ mp = mu + base;
         const T *__restrict__ yp = y + base;
-        const unsigned msk = dir.any ? dir.mask[d] : 0u;
-        const bool lo = msk & (1u << (2 * axis)), hi = msk & (2u << (2 * axis));
-        EndFix fx;
-        // rebuilt ends are read by the segments holding rows 0, n-2 and n-1
-        if ((lo || hi) && (q0 == 0 || q1 >= n - 1)) {
-            const long long v0 = (long long)(base / S);  // voxel of element 0
-            const long long yz = (long long)dir.ny * dir.nz;
-            const int vi = (int)(v0 / yz), vj = (int)((v0 / dir.nz) % dir.ny), vk = (int)(v0 % dir.nz);
-            auto gv = [&](int q) -> double {
-                int ii = vi, jj = vj, kk = vk;
-                if (axis == 0) ii = q; else if (axis == 1) jj = q; else kk = q;
-                return (double)dir_value(dir, ii, jj, kk, d);
-            };
-            fx.make(lo, hi, n, t.c1[d], t.c2[d], gv(0), gv(n - 1), n > 1 ? (double)yp[inner] : 0.0,
-                    n > 1 ? (double)yp[(size_t)(n - 2) * inner] : 0.0);
+        // rebuilt ends, read by the segments holding rows 0, n-2 and n-1
+        EndFix fx[VEC];
+        bool any_fix = false;
+        if (dir.any && (q0 == 0 || q1 >= n - 1)) {
+#pragma unroll
+            for (int u = 0; u < VEC; ++u) {
+                const int d = (int)((l0 + u) % S);
+                const unsigned msk = dir.mask[d];
+                const bool lo = msk & (1u << (2 * axis)), hi = msk & (2u << (2 * axis));
+                if (!(lo || hi)) continue;
+                any_fix = true;
+                const long long v0 = (long long)((base + u) / S);  // voxel of element 0
+                const long long yz = (long long)dir.ny * dir.nz;
+                const int vi = (int)(v0 / yz), vj = (int)((v0 / dir.nz) % dir.ny), vk = (int)(v0 % dir.nz);
+                auto gv = [&](int q) -> double {
+                    int ii = vi, jj = vj, kk = vk;
+                    if (axis == 0) ii = q; else if (axis == 1) jj = q; else kk = q;
+                    return (double)dir_value(dir, ii, jj, kk, d);
+                };
+                fx[u].make(lo, hi, n, t.c1[d], t.c2[d], gv(0), gv(n - 1), n > 1 ? (double)yp[inner + u] : 0.0,
+                           n > 1 ? (double)yp[(size_t)(n - 2) * inner + u] : 0.0);
+            }
         }
-        auto yat = [&](int q) -> double {
-            if (q == 0 && fx.lo) return fx.y0;
-            if (q == n - 1 && fx.hi) return fx.yn;
-            return (double)yp[(size_t)q * inner];
+        auto yrow = [&](int q, double (&o)[VEC]) {
+            load_vec<T, VEC>(yp + (size_t)q * inner, o);
+            if (any_fix) {
+#pragma unroll
+                for (int u = 0; u < VEC; ++u) {
+                    if (q == 0 && fx[u].lo) o[u] = fx[u].y0;
+                    if (q == n - 1 && fx[u].hi) o[u] = fx[u].yn;
+                }
+            }
         };
-        double mprev = (double)mp[(size_t)q0 * inner];
-        double yprev = yat(q0);
-        dyy = mprev * yprev;
-        double dl1 = 0.0, dy1 = 0.0;  // second accumulators: two independent chains
-        const int qe = min(q1 + 1, n);  // last row read (edge partner of row q1 - 1)
+        double mprev[VEC], yprev[VEC], dl2[VEC], dy2[VEC];
+        load_vec<T, VEC>(mp + (size_t)q0 * inner, mprev);
+        yrow(q0, yprev);
+#pragma unroll
+        for (int u = 0; u < VEC; ++u) {
+            dyy[u] = mprev[u] * yprev[u];
+            dl2[u] = dy2[u] = 0.0;
+        }
+        // own interior rows (q0, qa): plain loads, two independent accumulator chains
+        const int qa = min(q1, n - 1);
         int q = q0 + 1;
-        // interior rows (not 0, not n-1): plain loads
-        const int qi = min(qe, n - 1);
 #pragma unroll 2
-        for (; q + 1 < qi; q += 2) {
-            const double ma = (double)mp[(size_t)q * inner], ya = (double)yp[(size_t)q * inner];
-            const double mb = (double)mp[(size_t)(q + 1) * inner], yb = (double)yp[(size_t)(q + 1) * inner];
-            dl += (mprev - ma) * (yprev - ya);
-            dl1 += (ma - mb) * (ya - yb);
-            if (q < q1) dyy += ma * ya;
-            if (q + 1 < q1) dy1 += mb * yb;
-            mprev = mb;
-            yprev = yb;
+        for (; q + 1 < qa; q += 2) {
+            double ma[VEC], ya[VEC], mb[VEC], yb[VEC];
+            load_vec<T, VEC>(mp + (size_t)q * inner, ma);
+            load_vec<T, VEC>(yp + (size_t)q * inner, ya);
+            load_vec<T, VEC>(mp + (size_t)(q + 1) * inner, mb);
+            load_vec<T, VEC>(yp + (size_t)(q + 1) * inner, yb);
+#pragma unroll
+            for (int u = 0; u < VEC; ++u) {
+                dl[u] += (mprev[u] - ma[u]) * (yprev[u] - ya[u]);
+                dyy[u] += ma[u] * ya[u];
+                dl2[u] += (ma[u] - mb[u]) * (ya[u] - yb[u]);
+                dy2[u] += mb[u] * yb[u];
+                mprev[u] = mb[u];
+                yprev[u] = yb[u];
+            }
         }
-        for (; q < qe; ++q) {
-            const double ma = (double)mp[(size_t)q * inner], ya = yat(q);
-            dl += (mprev - ma) * (yprev - ya);
-            if (q < q1) dyy += ma * ya;
-            mprev = ma;
-            yprev = ya;
+        for (; q < qa; ++q) {
+            double ma[VEC], ya[VEC];
+            load_vec<T, VEC>(mp + (size_t)q * inner, ma);
+            load_vec<T, VEC>(yp + (size_t)q * inner, ya);
+#pragma unroll
+            for (int u = 0; u < VEC; ++u) {
+                dl[u] += (mprev[u] - ma[u]) * (yprev[u] - ya[u]);
+                dyy[u] += ma[u] * ya[u];
+                mprev[u] = ma[u];
+                yprev[u] = ya[u];
+            }
         }
-        dl += dl1;
-        dyy += dy1;
+        // row qa closes the segment: its own last row n-1, or the next segment's first row
+        if (qa > q0) {
+            double ma[VEC], ya[VEC];
+            load_vec<T, VEC>(mp + (size_t)qa * inner, ma);
+            yrow(qa, ya);
+            const bool own = qa < q1;
+#pragma unroll
+            for (int u = 0; u < VEC; ++u) {
+                dl[u] += (mprev[u] - ma[u]) * (yprev[u] - ya[u]);
+                if (own) dyy[u] += ma[u] * ya[u];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < VEC; ++u) {
+            dl[u] += dl2[u];
+            dyy[u] += dy2[u];
+        }
     }
-    s0[tid] = dl;
-    s1[tid] = dyy;
+#pragma unroll
+    for (int u = 0; u < VEC; ++u) {
+        s0[VEC * tid + u] = dl[u];
+        s1[VEC * tid + u] = dyy[u];
+    }
     __syncthreads();
-    for (int h = blockDim.x / S / 2; h >= 1; h >>= 1) {
-        if (tid < h * S) {
-            s0[tid] += s0[tid + h * S];
-            s1[tid] += s1[tid + h * S];
+    const int slots = VEC * blockDim.x;
+    for (int h = slots / S / 2; h >= 1; h >>= 1) {
+        for (int i = tid; i < h * S; i += blockDim.x) {
+            s0[i] += s0[i + h * S];
+            s1[i] += s1[i + h * S];
         }
         __syncthreads();
     }
@@ -855,23 +917,36 @@ struct Adjoint {
     }
 
     // the sums of one sweep over the stored y and the new mu
-    static constexpr int kDotSeg = 64;  // rows per thread in the sums kernel
+    // lines per thread (16-byte loads) and rows per thread in the sums kernel;
+    // FP32 runs fastest with 4-byte loads and 64-row segments (measured)
+    static constexpr int kVec = sizeof(T) == 8 ? 2 : 1;
+    static constexpr int kDotSeg = 64 / kVec;
     int dots_threads() const {
         int threads = S;
         while (threads * 2 <= 256) threads *= 2;
         return threads;
     }
+    static int axis_len(const bfb_env_s *e, int axis) { return axis == 0 ? e->nx : (axis == 1 ? e->ny : e->nz); }
+    long long axis_inner(int axis) const {
+        return axis == 0 ? (long long)env->ny * env->nz * S : (axis == 1 ? (long long)env->nz * S : S);
+    }
+    int dots_vec(int axis) const { return axis_inner(axis) % kVec == 0 ? kVec : 1; }
     long long dots_blocks(int axis) const {
-        const int n = axis == 0 ? env->nx : (axis == 1 ? env->ny : env->nz);
-        const long long work = (long long)env->N / n * ((n + kDotSeg - 1) / kDotSeg);
+        const int n = axis_len(env, axis);
+        const int sg = dots_vec(axis) == kVec ? kDotSeg : 64;
+        const long long work = (long long)env->N / n / dots_vec(axis) * ((n + sg - 1) / sg);
         return (work + dots_threads() - 1) / dots_threads();
     }
     int dots(int axis, const SweepArgs<T> &a, const T *mu, const T *y, const AdjTerms &t) {
-        const int n = axis == 0 ? env->nx : (axis == 1 ? env->ny : env->nz);
-        const long long inner = axis == 0 ? (long long)env->ny * env->nz * S : (axis == 1 ? (long long)env->nz * S : S);
+        const int n = axis_len(env, axis);
         const long long nlines = (long long)env->N / n;
-        adjoint_dots_kernel<T><<<(unsigned)dots_blocks(axis), dots_threads(), 0, st>>>(mu, y, a.dir, axis, n, inner,
-                                                                                       nlines, kDotSeg, t);
+        const unsigned blocks = (unsigned)dots_blocks(axis);
+        if (dots_vec(axis) == kVec)
+            adjoint_dots_kernel<T, kVec><<<blocks, dots_threads(), 0, st>>>(mu, y, a.dir, axis, n, axis_inner(axis),
+                                                                             nlines, kDotSeg, t);
+        else
+            adjoint_dots_kernel<T, 1><<<blocks, dots_threads(), 0, st>>>(mu, y, a.dir, axis, n, axis_inner(axis),
+                                                                          nlines, 64, t);
         BFB_CUDA(cudaGetLastError());
         return BFB_OK;
     }
