@@ -275,6 +275,7 @@ def run_our_arm(args):
         env.set_coefficients(D, lam)
         env.set_field(rho0)
         env.set_stream(stream.cuda_stream)
+        tuned, tuned_ms = env.autotune(DT, trials=3)  # launch shapes chosen by the library's autotuner
         env.simulate(DT, warm, bfb.STEP_DIFFUSION)
         barrier()
         clocks = Clocks(local)
@@ -291,7 +292,8 @@ def run_our_arm(args):
         # per-kernel device time (events around every launch, same stream)
         prof = env.profile_steps(DT, min(K, 50), bfb.STEP_DIFFUSION)
         nprof = min(K, 50)
-        results[name] = dict(ms=ms, clocks=clk, prof=prof, nprof=nprof, env=env, elem=4 if prec == bfb.FP32 else 8)
+        results[name] = dict(ms=ms, clocks=clk, prof=prof, nprof=nprof, env=env, elem=4 if prec == bfb.FP32 else 8,
+                             tuning=tuned)
 
     # both envs ran the same steps from the same field: FP32's error against FP64
     n_steps_run = warm + K + min(K, 50)
@@ -374,6 +376,9 @@ def run_our_arm(args):
                  "step_roofline_frac": 6.0 * V * S * 8 / (r64["ms"] / K / 1e3) / 1e9 / peak,
                  "kernel_ms_per_launch": {p: float(x) for p, x in zip(phases, r64["prof"][:3] / r64["nprof"])}},
         "fp32_over_fp64": value / value64,
+        "tuning": {"fp32": r32["tuning"], "fp64": r64["tuning"],
+                   "fields": "per sweep x, y, z: (TMA tiles 1 / cp.async 0, warps per CTA, row groups per tile), "
+                             "chosen by bfb_autotune before the warm-up"},
         "fp32_error_vs_fp64": {"rel_linf": err_linf, "rel_l2": err_l2, "after_steps": n_steps_run},
         "clocks": r32["clocks"],
         "e2e": {"value": world * V * S * K_e2e / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": V * S * 8,

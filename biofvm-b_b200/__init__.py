@@ -51,7 +51,7 @@ EXPORTS = [
     "bfb_compare_fields", "bfb_field_device_ptr", "bfb_set_dirichlet",
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
-    "bfb_checksum", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
+    "bfb_checksum", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
     "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_adjoint_run", "bfb_checksum_noalloc",
 ]
 
@@ -110,6 +110,9 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_step_host": [_vp, _vp, ctypes.c_double, ctypes.c_int],
         "bfb_profile_steps": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp],
         "bfb_checksum": [_vp, _dp],
+        "bfb_set_tuning": [_vp, _ip],
+        "bfb_get_tuning": [_vp, _ip],
+        "bfb_autotune": [_vp, ctypes.c_double, ctypes.c_int, _ip, _dp],
         "bfb_checksum_noalloc": [_vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, _vp, _vp],
         "bfb_batch_create": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)],
         "bfb_batch_destroy": [_vp],
@@ -307,6 +310,26 @@ class Env:
         out = np.zeros(self.S)
         _check(self.L.bfb_checksum(self.h, out.ctypes.data_as(_dp)))
         return out
+
+    # -- launch shape ---------------------------------------------------
+    def get_tuning(self):
+        """[(tma, warps, chunks) for x, y, z]"""
+        v = (ctypes.c_int * 9)()
+        _check(self.L.bfb_get_tuning(self.h, v))
+        return [tuple(v[3 * a:3 * a + 3]) for a in range(3)]
+
+    def set_tuning(self, shape):
+        flat = [int(x) for axis in shape for x in axis]
+        v = (ctypes.c_int * 9)(*flat)
+        _check(self.L.bfb_set_tuning(self.h, v))
+
+    def autotune(self, dt, trials=5):
+        """Times every launch shape of each sweep; keeps and returns the fastest
+        as ([(tma, warps, chunks)] * 3, [ms per launch] * 3)."""
+        v = (ctypes.c_int * 9)()
+        ms = np.zeros(3)
+        _check(self.L.bfb_autotune(self.h, dt, trials, v, ms.ctypes.data_as(_dp)))
+        return [tuple(v[3 * a:3 * a + 3]) for a in range(3)], ms
 
     def adjoint_run(self, dt, n_steps, dL_dfinal_ptr: int, flags=STEP_DIFFUSION, checkpoint_every=None,
                     dL_dinitial_ptr: int = None, final_ptr: int = None, agent_grads=False):

@@ -897,23 +897,26 @@ struct Adjoint {
     double *part_x = nullptr, *part_y = nullptr, *part_z = nullptr;
     long long tiles_z = 0;
 
+    // tensor maps with the env's row-group counts (so the recompute runs the
+    // env's tuned launch shape)
     void map(Buf &b) {
         for (int a = 0; a < 2; ++a)
             b.ok[a] = env->use_tma && make_sweep_tensor_map(&b.map[a], &b.crow[a], b.p, sizeof(T), a, env->nx,
-                                                            env->ny, env->nz, S);
+                                                            env->ny, env->nz, S, env->tuning.chunks[a]);
     }
 
-    // one forward sweep, out of place
+    // one forward sweep, out of place, in the env's launch shape
     int fwd(int axis, Buf &in, Buf &out) {
         SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
         a.f = static_cast<T *>(in.p);
         a.fo = static_cast<T *>(out.p);
+        const int warps = env->tuning.warps[axis];
         if (axis < 2) {
-            const bool tma = in.ok[axis] && out.ok[axis];
-            return launch_strided<T>(a, axis, axis == 0, 1, tma ? &in.map[axis] : nullptr,
+            const bool tma = env->tuning.tma[axis] && in.ok[axis] && out.ok[axis];
+            return launch_strided<T>(a, axis, axis == 0, warps, tma ? &in.map[axis] : nullptr,
                                      tma ? &out.map[axis] : nullptr, in.crow[axis], st);
         }
-        return launch_contig<T>(a, 1, env->use_tma != 0, st);
+        return launch_contig<T>(a, warps, env->use_tma && env->tuning.tma[2], st, env->tuning.chunks[2]);
     }
 
     // the sums of one sweep over the stored y and the new mu

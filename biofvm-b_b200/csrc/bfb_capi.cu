@@ -1,5 +1,6 @@
 // bfb_capi.cu -- the C ABI (include/biofvm_b200.h): handles, coefficients,
 // Dirichlet, bulk, agents, step sequencing and CUDA-graph replay.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -204,20 +205,28 @@ static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
 }
 
 static const CUtensorMap *tma_map(bfb_env_s *env, int axis) {
-    return (env->use_tma && env->tma_ok[axis]) ? &env->tmap[axis] : nullptr;
+    return (env->use_tma && env->tuning.tma[axis] && env->tma_ok[axis]) ? &env->tmap[axis] : nullptr;
+}
+
+// the field's x / y tensor maps for the current row-group counts
+static void encode_field_maps(bfb_env_s *env) {
+    for (int a = 0; a < 2; ++a)
+        env->tma_ok[a] = make_sweep_tensor_map(&env->tmap[a], &env->tma_crow[a], env->field, (int)env->elem, a,
+                                               env->nx, env->ny, env->nz, env->S, env->tuning.chunks[a]);
 }
 
 // One LOD diffusion step; `bulk` fuses a preceding bulk source/sink update
 // into the x-sweep load.
 template <typename T>
 static int run_diffusion(bfb_env_s *env, double dt, bool bulk, cudaStream_t s) {
-    int st = launch_strided<T>(make_args<T>(env, 0, bulk, dt), 0, true, env->tuning.warps_x, tma_map(env, 0),
+    int st = launch_strided<T>(make_args<T>(env, 0, bulk, dt), 0, true, env->tuning.warps[0], tma_map(env, 0),
                                tma_map(env, 0), env->tma_crow[0], s);
     if (st) return st;
-    st = launch_strided<T>(make_args<T>(env, 1, false, dt), 1, false, env->tuning.warps_y, tma_map(env, 1),
+    st = launch_strided<T>(make_args<T>(env, 1, false, dt), 1, false, env->tuning.warps[1], tma_map(env, 1),
                            tma_map(env, 1), env->tma_crow[1], s);
     if (st) return st;
-    return launch_contig<T>(make_args<T>(env, 2, false, dt), env->tuning.warps_z, env->use_tma != 0, s);
+    return launch_contig<T>(make_args<T>(env, 2, false, dt), env->tuning.warps[2],
+                            env->use_tma != 0 && env->tuning.tma[2] != 0, s, env->tuning.chunks[2]);
 }
 
 template <typename T>
@@ -387,10 +396,7 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
         cudaError_t e = cudaMemset(env->d_err, 0, sizeof(int));
         if (e != cudaSuccess) st = cuda_fail(e, "cudaMemset");
     }
-    if (!st)
-        for (int a = 0; a < 2; ++a)
-            env->tma_ok[a] = make_sweep_tensor_map(&env->tmap[a], &env->tma_crow[a], env->field, (int)env->elem, a,
-                                                   nx, ny, nz, n_substrates);
+    if (!st) encode_field_maps(env);
     if (!st) {
         cudaError_t e = cudaStreamCreateWithFlags(&env->own_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaStreamCreateWithFlags");
@@ -854,6 +860,133 @@ BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_step
 
 // Per-phase device time, the counterpart of the reference's -DTIMING CSV
 // (BioFVM_parallel.cpp:695-697, 1259-1392): events around every launch.
+// ---------------------------------------------------------------------------
+// Launch-shape tuning. A shape is, per axis, {TMA tiles or cp.async tiles,
+// warps per CTA, row groups per TMA tile}; all shapes compute the same
+// numbers. bfb_autotune times each candidate of each sweep out of place (the
+// env's field -> a scratch field, so the field is unchanged) and keeps the
+// fastest.
+// ---------------------------------------------------------------------------
+static bool tuning_valid(const int *v) {
+    for (int a = 0; a < 3; ++a) {
+        const int tma = v[3 * a], warps = v[3 * a + 1], chunks = v[3 * a + 2];
+        if (tma < 0 || tma > 1 || warps < 1 || warps > 4 || chunks < 1 || chunks > 16) return false;
+    }
+    return true;
+}
+
+static void apply_tuning(bfb_env_s *env, const int *v) {
+    for (int a = 0; a < 3; ++a) {
+        env->tuning.tma[a] = v[3 * a];
+        env->tuning.warps[a] = v[3 * a + 1];
+        env->tuning.chunks[a] = v[3 * a + 2];
+    }
+    encode_field_maps(env);
+    drop_graph(env);
+    env->epoch++;
+}
+
+BFB_API int bfb_set_tuning(bfb_env env, const int *shape) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!shape) return fail(BFB_ERR_INVALID_ARG, "shape is NULL");
+    if (!tuning_valid(shape)) return fail(BFB_ERR_INVALID_ARG, "tuning: tma 0/1, warps 1..4, chunks 1..16 per axis");
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    apply_tuning(env, shape);
+    return BFB_OK;
+}
+
+BFB_API int bfb_get_tuning(bfb_env env, int *shape) {
+    if (!env) return fail(BFB_ERR_INVALID_ARG, "null bfb_env");
+    if (!shape) return fail(BFB_ERR_INVALID_ARG, "shape is NULL");
+    for (int a = 0; a < 3; ++a) {
+        shape[3 * a] = env->tuning.tma[a];
+        shape[3 * a + 1] = env->tuning.warps[a];
+        shape[3 * a + 2] = env->tuning.chunks[a];
+    }
+    return BFB_OK;
+}
+
+}  // extern "C"
+
+template <typename T>
+static int time_candidates(bfb_env_s *env, double dt, int trials, void *scratch, int *best, double *best_ms) {
+    cudaStream_t s = env->stream;
+    cudaEvent_t e0, e1;
+    BFB_CUDA(cudaEventCreate(&e0));
+    BFB_CUDA(cudaEventCreate(&e1));
+    int st = BFB_OK;
+    for (int axis = 0; axis < 3 && !st; ++axis) {
+        best_ms[axis] = -1.0;
+        for (int tma = 1; tma >= 0 && !st; --tma)
+            for (int warps : {1, 2, 4}) {
+                for (int chunks : {2, 4, 8}) {
+                    if (!tma && chunks != kChunks) continue;  // the cp.async tiles have a fixed stage count
+                    SweepArgs<T> a = make_args<T>(env, axis, false, dt);
+                    a.fo = static_cast<T *>(scratch);
+                    CUtensorMap mi, mo;
+                    int ci = 0, co = 0;
+                    bool maps = false;
+                    if (axis < 2 && tma && env->use_tma)
+                        maps = make_sweep_tensor_map(&mi, &ci, env->field, (int)env->elem, axis, env->nx, env->ny,
+                                                     env->nz, env->S, chunks) &&
+                               make_sweep_tensor_map(&mo, &co, scratch, (int)env->elem, axis, env->nx, env->ny,
+                                                     env->nz, env->S, chunks);
+                    auto launch = [&]() -> int {
+                        if (axis < 2)
+                            return launch_strided<T>(a, axis, axis == 0, warps, maps ? &mi : nullptr,
+                                                     maps ? &mo : nullptr, ci, s);
+                        return launch_contig<T>(a, warps, tma && env->use_tma, s, chunks);
+                    };
+                    if ((st = launch())) break;  // warm
+                    cudaError_t e = cudaEventRecord(e0, s);
+                    for (int q = 0; q < trials && !st && e == cudaSuccess; ++q) st = launch();
+                    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    float ms = 0;
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                    if (e != cudaSuccess) st = cuda_fail(e, "autotune timing");
+                    if (st) break;
+                    const double per = ms / trials;
+                    if (best_ms[axis] < 0 || per < best_ms[axis]) {
+                        best_ms[axis] = per;
+                        best[3 * axis] = tma;
+                        best[3 * axis + 1] = warps;
+                        best[3 * axis + 2] = tma ? chunks : env->tuning.chunks[axis];
+                    }
+                }
+                if (st) break;
+            }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
+}
+
+extern "C" {
+
+BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double *best_ms) {
+    int st = check_env(env);
+    if (st) return st;
+    if (!(dt > 0) || trials < 1) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0 and trials >= 1");
+    if ((st = ensure_factors(env, dt))) return st;
+    BFB_CUDA(cudaStreamSynchronize(env->stream));
+    void *scratch = nullptr;
+    BFB_CUDA(cudaMalloc(&scratch, env->elem * env->N));
+    int best[9];
+    double ms[3];
+    bfb_get_tuning(env, best);
+    st = env->precision == BFB_FP64 ? time_candidates<double>(env, dt, trials, scratch, best, ms)
+                                    : time_candidates<float>(env, dt, trials, scratch, best, ms);
+    cudaFree(scratch);
+    if (st) return st;
+    if ((st = check_device_error(env))) return st;
+    apply_tuning(env, best);
+    if (chosen) std::copy(best, best + 9, chosen);
+    if (best_ms) std::copy(ms, ms + 3, best_ms);
+    return BFB_OK;
+}
+
 BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, double *ms_out) {
     int st = check_env(env);
     if (st) return st;
@@ -881,26 +1014,27 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
         if (flags & BFB_STEP_DIFFUSION) {
             const bool bulk = (flags & BFB_STEP_BULK) != 0;
             st = phase_ms(0, [&] {
-                return fp64 ? launch_strided<double>(make_args<double>(env, 0, bulk, dt), 0, true, env->tuning.warps_x,
+                return fp64 ? launch_strided<double>(make_args<double>(env, 0, bulk, dt), 0, true, env->tuning.warps[0],
                                                      tma_map(env, 0), tma_map(env, 0), env->tma_crow[0], s)
-                            : launch_strided<float>(make_args<float>(env, 0, bulk, dt), 0, true, env->tuning.warps_x,
+                            : launch_strided<float>(make_args<float>(env, 0, bulk, dt), 0, true, env->tuning.warps[0],
                                                     tma_map(env, 0), tma_map(env, 0), env->tma_crow[0], s);
             });
             if (!st)
                 st = phase_ms(1, [&] {
                     return fp64 ? launch_strided<double>(make_args<double>(env, 1, false, dt), 1, false,
-                                                         env->tuning.warps_y, tma_map(env, 1), tma_map(env, 1),
+                                                         env->tuning.warps[1], tma_map(env, 1), tma_map(env, 1),
                                                          env->tma_crow[1], s)
                                 : launch_strided<float>(make_args<float>(env, 1, false, dt), 1, false,
-                                                        env->tuning.warps_y, tma_map(env, 1), tma_map(env, 1),
+                                                        env->tuning.warps[1], tma_map(env, 1), tma_map(env, 1),
                                                         env->tma_crow[1], s);
                 });
             if (!st)
                 st = phase_ms(2, [&] {
-                    return fp64 ? launch_contig<double>(make_args<double>(env, 2, false, dt), env->tuning.warps_z,
-                                                        env->use_tma != 0, s)
-                                : launch_contig<float>(make_args<float>(env, 2, false, dt), env->tuning.warps_z,
-                                                       env->use_tma != 0, s);
+                    const bool tz = env->use_tma != 0 && env->tuning.tma[2] != 0;
+                    return fp64 ? launch_contig<double>(make_args<double>(env, 2, false, dt), env->tuning.warps[2], tz,
+                                                        s, env->tuning.chunks[2])
+                                : launch_contig<float>(make_args<float>(env, 2, false, dt), env->tuning.warps[2], tz, s,
+                                                       env->tuning.chunks[2]);
                 });
         } else if (flags & BFB_STEP_BULK) {
             st = phase_ms(3, [&] {

@@ -51,11 +51,12 @@ struct BulkTerms {
     int on;
 };
 
-// Launch configuration chosen by the autotuner (or defaults).
+// Launch shape of the three sweeps, chosen by bfb_autotune or set by
+// bfb_set_tuning. Every shape computes the same numbers; only speed differs.
 struct SweepTuning {
-    int warps_x = 1;   // warps per CTA of the strided kernels (x and y); one warp
-    int warps_y = 1;   // per CTA packs shared memory tightest
-    int warps_z = 1;   // warps per CTA of the contiguous kernel (z)
+    int tma[3] = {1, 1, 1};     // TMA tiles (when the grid allows them) or cp.async tiles
+    int warps[3] = {1, 1, 1};   // warps (= tiles) per CTA; one packs shared memory tightest
+    int chunks[3] = {4, 4, 4};  // row groups per TMA tile (pipeline stages)
 };
 
 }  // namespace bfb

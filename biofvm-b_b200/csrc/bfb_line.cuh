@@ -7,7 +7,6 @@
 namespace bfb {
 
 constexpr int kMaxSmem = 227 * 1024;  // opt-in dynamic shared memory per CTA on sm_100a
-constexpr int kChunks = 4;            // row groups per strided tile (async copy stages)
 
 // ---------------------------------------------------------------------------
 // cp.async helpers (LDGSTS: global -> shared without staging in registers)

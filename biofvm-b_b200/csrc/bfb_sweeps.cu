@@ -396,7 +396,7 @@ static int go_contig(const SweepArgs<T> &a, const ContigGeom &g, int warps, size
 }
 
 template <typename T>
-int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s) {
+int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s, int chunks) {
     ContigGeom g;
     g.nz = a.nz;
     g.nrows = (long long)a.nx * a.ny;
@@ -413,7 +413,7 @@ int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s
     const bool base16 = (reinterpret_cast<uintptr_t>(a.f) & 15) == 0;
     const int eb = (int)sizeof(T);
     if (use_tma && base16 && (L * eb) % 16 == 0 && ((long long)g.RS * eb) % 16 == 0 && (L * eb) * g.R < (1 << 20)) {
-        const int st = launch_contig_tma<T>(a, g, warps, s);
+        const int st = launch_contig_tma<T>(a, g, warps, s, chunks);
         if (st != kNotApplicable) return st;
     }
     if (base16 && (L * eb) % 16 == 0 && ((long long)g.RS * eb) % 16 == 0) return go_contig<T, 16>(a, g, warps, smem, s);
@@ -480,8 +480,8 @@ template int launch_strided<double>(const SweepArgs<double> &, int, bool, int, c
                                     const CUtensorMap *, int, cudaStream_t);
 template int launch_strided<float>(const SweepArgs<float> &, int, bool, int, const CUtensorMap *, const CUtensorMap *,
                                    int, cudaStream_t);
-template int launch_contig<double>(const SweepArgs<double> &, int, bool, cudaStream_t);
-template int launch_contig<float>(const SweepArgs<float> &, int, bool, cudaStream_t);
+template int launch_contig<double>(const SweepArgs<double> &, int, bool, cudaStream_t, int);
+template int launch_contig<float>(const SweepArgs<float> &, int, bool, cudaStream_t, int);
 template int launch_dirichlet<double>(const SweepArgs<double> &, cudaStream_t);
 template int launch_dirichlet<float>(const SweepArgs<float> &, cudaStream_t);
 template int launch_bulk<double>(const SweepArgs<double> &, long long, cudaStream_t);

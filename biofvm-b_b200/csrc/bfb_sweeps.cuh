@@ -51,6 +51,8 @@
 
 namespace bfb {
 
+constexpr int kChunks = 4;  // default row groups per tile (async copy / TMA stages)
+
 // Per-axis factor tables on the device (see bfb_capi.cu: upload_factors).
 //   FP64: t0 = den, t1 = c (back-substitution coefficient), t2 = RN(1/den)
 //   FP32: t0 = 1/den (hi), t1 = 1/den (lo), t2 = c1/den, t3 = c
@@ -97,7 +99,7 @@ template <typename T>
 int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map,
                    const CUtensorMap *map_out, int crow, cudaStream_t s);
 template <typename T>
-int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s);
+int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s, int chunks = kChunks);
 
 // TMA kernels (bfb_tma.cu); they return kNotApplicable when the tile does
 // not fit in shared memory, and the caller then takes another kernel.
@@ -106,9 +108,10 @@ template <typename T>
 int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map,
                        const CUtensorMap *map_out, int crow, bool fuse_pre, int warps, cudaStream_t s);
 template <typename T>
-int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s);
+int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s, int chunks);
+// `chunks` row groups per tile: box rows = ceil(n / chunks) (<= 256).
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
-                           int S);
+                           int S, int chunks = kChunks);
 void tma_prepare_device();
 template <typename T>
 int launch_dirichlet(const SweepArgs<T> &a, cudaStream_t s);

@@ -393,7 +393,7 @@ int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtens
 }
 
 template <typename T>
-int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s) {
+int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s, int chunks) {
     const size_t wb = (128 + (size_t)g.R * g.RS * sizeof(T) + 127) / 128 * 128;
     while (warps > 1 && wb * warps > (size_t)kMaxSmem) --warps;
     if (wb * warps > (size_t)kMaxSmem) return kNotApplicable;
@@ -405,7 +405,7 @@ int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cud
         const int eb = (int)sizeof(T);
         int q = 16;
         for (int v = a.S * eb; v % 2 == 0 && q > 1; v /= 2) q /= 2;  // q = 16 / gcd(16, S*elem)
-        int kc = (g.nz + kChunks - 1) / kChunks;
+        int kc = (g.nz + chunks - 1) / chunks;
         kc = (kc + q - 1) / q * q;
         switch (a.S) {
         case 1: sweep_contig_pipe_kernel<T, 1><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
@@ -425,8 +425,8 @@ template int launch_strided_tma<double>(const SweepArgs<double> &, const Strided
                                         const CUtensorMap *, int, bool, int, cudaStream_t);
 template int launch_strided_tma<float>(const SweepArgs<float> &, const StridedGeom &, const CUtensorMap *,
                                        const CUtensorMap *, int, bool, int, cudaStream_t);
-template int launch_contig_tma<double>(const SweepArgs<double> &, const ContigGeom &, int, cudaStream_t);
-template int launch_contig_tma<float>(const SweepArgs<float> &, const ContigGeom &, int, cudaStream_t);
+template int launch_contig_tma<double>(const SweepArgs<double> &, const ContigGeom &, int, cudaStream_t, int);
+template int launch_contig_tma<float>(const SweepArgs<float> &, const ContigGeom &, int, cudaStream_t, int);
 
 template <typename K>
 static void opt_in_tma(K k) {
@@ -481,12 +481,13 @@ static EncodeTiledFn encode_fn() {
 // Returns false when the grid does not meet TMA's rules (row pitch a multiple
 // of 16 bytes, box rows <= 256); the cp.async kernels handle those grids.
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
-                           int S) {
+                           int S, int chunks) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
     const int n = axis == 0 ? nx : ny;
     const long long P = axis == 0 ? (long long)ny * nz * S : (long long)nz * S;
-    const int crow = (n + kChunks - 1) / kChunks;
+    if (chunks < 1 || chunks > 16) return false;  // one mbarrier per row group in a 128-byte header
+    const int crow = (n + chunks - 1) / chunks;
     if (crow > 256 || (P * elem) % 16 != 0 || (reinterpret_cast<uintptr_t>(field) & 15)) return false;
     if (P > 0xffffffffLL) return false;
     cuuint64_t dims[3] = {(cuuint64_t)P, (cuuint64_t)n, (cuuint64_t)nx};

@@ -189,6 +189,23 @@ BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_step
 #define BFB_PROFILE_PHASES 5
 BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, double *ms_out);
 
+/* ---- Launch-shape tuning -------------------------------------------------
+ * No counterpart in the reference. The launch shape of the x, y and z sweeps:
+ * shape[3*axis + 0] = 1 for TMA tiles (where the grid allows them), 0 for
+ * cp.async tiles; shape[3*axis + 1] = warps (tiles) per CTA, 1..4;
+ * shape[3*axis + 2] = row groups per TMA tile (pipeline stages), 1..16.
+ * Every shape computes the same numbers (FP64 bit for bit); only the speed
+ * differs. Defaults {1, 1, 4} per axis. bfb_autotune times each candidate
+ * (TMA / cp.async x 1, 2, 4 warps x 2, 4, 8 row groups) of each sweep with
+ * CUDA events over `trials` launches, out of place from the env's field into
+ * a scratch field (the field is unchanged; the scratch is freed on return),
+ * keeps the fastest and returns it in chosen[BFB_TUNING_FIELDS] and its
+ * milliseconds per launch in best_ms[3] (either may be NULL). */
+#define BFB_TUNING_FIELDS 9
+BFB_API int bfb_set_tuning(bfb_env env, const int *shape);
+BFB_API int bfb_get_tuning(bfb_env env, int *shape);
+BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double *best_ms);
+
 /* Per-substrate FP64 sum of the field over all voxels (mass checksum). */
 BFB_API int bfb_checksum(bfb_env env, double *out);
 
