@@ -32,6 +32,8 @@ STEP_CELLS = 4
 OPT_FREEZE_FACTORS = 1
 OPT_USE_GRAPHS = 2
 OPT_USE_TMA = 3
+BATCH_OPT_WARPS_PER_CTA = 1
+BATCH_OPT_TILES_PER_ITEM = 2
 
 ERRORS = {
     -1: "BFB_ERR_INVALID_ARG",
@@ -52,7 +54,8 @@ EXPORTS = [
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
     "bfb_checksum", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
-    "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_adjoint_run", "bfb_checksum_noalloc",
+    "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_batch_autotune", "bfb_adjoint_run",
+    "bfb_checksum_noalloc",
 ]
 
 
@@ -120,6 +123,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_batch_simulate": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_simulate_loop": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_synchronize": [_vp],
+        "bfb_batch_autotune": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp],
         "bfb_adjoint_run": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _dp, _dp,
                             _dp, _dp, _dp],
     }
@@ -376,7 +380,17 @@ class Batch:
             pass
 
     def set_warps(self, w):
-        _check(self.L.bfb_batch_set_option(self.h, 1, w))
+        _check(self.L.bfb_batch_set_option(self.h, BATCH_OPT_WARPS_PER_CTA, w))
+
+    def set_tiles_per_item(self, t):
+        _check(self.L.bfb_batch_set_option(self.h, BATCH_OPT_TILES_PER_ITEM, t))
+
+    def autotune(self, dt, flags=STEP_DIFFUSION, trials=3):
+        """Picks warps per CTA and tiles per item; returns ((warps, tiles), ms per step)."""
+        v = (ctypes.c_int * 2)()
+        ms = ctypes.c_double()
+        _check(self.L.bfb_batch_autotune(self.h, dt, flags, trials, v, ctypes.byref(ms)))
+        return (v[0], v[1]), ms.value
 
     def simulate(self, dt, n, flags=STEP_DIFFUSION):
         _check(self.L.bfb_batch_simulate(self.h, dt, n, flags))

@@ -2,22 +2,29 @@
 //
 // A batch references N envs of uneven shapes and substrate counts (same
 // device and precision). One LOD step of all of them is one launch of
-// batch_step_kernel: a grid of resident one-warp CTAs pulls work items from a
-// device queue (one atomic counter). The items of one step are ordered
-//     [x tiles of env 0..N-1][y tiles ...][z tiles ...][cell chunks ...]
+// batch_step_kernel: a grid of resident CTAs whose warps pull work items from
+// a device queue (one atomic counter). An item is `tiles_per_item` adjacent
+// warp tiles of one env and one stage; the items of one step are ordered
+//     [x items of env 0..N-1][y items ...][z items ...][cell chunks ...]
 // and an item of env k waits (bounded) until env k has finished every item of
 // the previous stage. It only ever waits for items that running warps took
 // earlier, so the launch cannot deadlock, whether or not the whole grid is
-// resident. Each item runs the same warp-level tile code as the single-env
-// kernels (bfb_tiles.cuh). The step (counter resets + launch) is captured
-// once in a CUDA graph and replayed. bfb_batch_simulate_loop runs the same
-// envs one bfb_simulate call at a time, the per-instance launch loop the
-// persistent launch is compared with.
+// resident. Each tile runs the single-env kernels' warp-tile code: the TMA
+// tiles (bfb_tma_tiles.cuh; the env's own tensor maps, read from global
+// memory) where the env's grid and launch shape allow them, else the
+// cp.async tiles (bfb_tiles.cuh). A finished item is published with its bulk
+// stores complete (cp.async.bulk.wait_group 0), a proxy fence and a release;
+// a consumer acquires, then fences before its own tensor loads. The step
+// (counter resets + launch) is captured once in a CUDA graph and replayed.
+// bfb_batch_simulate_loop runs the same envs one bfb_simulate call at a time,
+// the per-instance launch loop the persistent launch is compared with;
+// bfb_batch_autotune picks warps per CTA and tiles per item.
 #include <algorithm>
 #include <vector>
 
 #include "bfb_aux.cuh"
 #include "bfb_tiles.cuh"
+#include "bfb_tma_tiles.cuh"
 
 namespace bfb {
 
@@ -30,7 +37,12 @@ struct BatchInst {
     StridedGeom gx, gy;
     ContigGeom gz;
     int vb16[3];         // 16-byte copies allowed (row pitch alignment) for x, y, z
-    int items[4];        // work items per stage: x tiles, y tiles, z tiles, cell chunks
+    int tiles[3];        // warp tiles per sweep stage
+    int items[4];        // work items per stage: x, y, z (tiles_per_item tiles each), cell chunks
+    int tma[3];          // TMA tiles for x, y (tensor maps) and z (bulk copies)
+    int crow[2];         // rows per TMA box (x, y)
+    int kc;              // z row-group length of the pipelined tile
+    const CUtensorMap *map[2];  // the env field's x / y tensor maps, in global memory
     T *f;
     int S, n_occ;
     const int *seg_start, *seg_voxel;
@@ -46,14 +58,22 @@ struct BatchParams {
     unsigned int *queue;
     int *err;
     int n;
-    int smem_elems;           // per-warp shared-memory elements
+    int warp_bytes;           // per-warp shared memory: 128-byte mbarrier header + the largest tile
     int stages;               // 3 (diffusion) or 4 (diffusion + cells)
+    int tiles_per_item;
 };
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+}
+__device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *m) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<unsigned long long>(m)) : "memory");
 }
 
 template <typename T>
@@ -78,18 +98,44 @@ __device__ void cells_chunk(const BatchInst<T> &I, int chunk) {
     }
 }
 
+// __launch_bounds__(128, 1): without the minimum-blocks hint the compiler
+// holds this kernel (every tile variant inlined) to 80 registers and spills.
 template <typename T>
-__global__ void __launch_bounds__(128) batch_step_kernel(BatchParams<T> p) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    T *sm = reinterpret_cast<T *>(smem_raw) + (size_t)warp * p.smem_elems;
+    unsigned char *wbase = smem_raw + (size_t)warp * p.warp_bytes;
+    T *sm = reinterpret_cast<T *>(wbase + 128);
+    // the warp's row-group mbarriers, reused by every TMA tile it runs: bit c
+    // of `phase` is the parity row group c waits for next
+    if (lane == 0) {
+        for (int c = 0; c < 16; ++c) mbar_init(smem_u32(wbase) + 8 * c, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    unsigned phase = 0;
     const unsigned total = (unsigned)p.stage_base[p.stages];
+    // The item finished last is published lazily: its bulk stores complete
+    // while the warp already loads the next item. It is published before the
+    // warp waits on any dependency (it may be the one waited for) and on exit.
+    int pend_k = -1, pend_stage = 0;
+    auto publish = [&]() {
+        if (pend_k < 0) return;
+        if (lane == 0) {
+            bulk_wait_all();             // its bulk stores have completed ...
+            fence_proxy_async_global();  // ... are ordered with the generic release below ...
+            __threadfence();
+            atomicAdd(p.done + 4 * pend_k + pend_stage, 1);  // ... and published
+        }
+        __syncwarp();
+        pend_k = -1;
+    };
     while (true) {
         unsigned item = 0;
         if (lane == 0) item = atomicAdd(p.queue, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= total) return;
+        if (item >= total) break;
         int stage = 0;
         while (item >= (unsigned)p.stage_base[stage + 1]) ++stage;
         const int r = (int)(item - (unsigned)p.stage_base[stage]);
@@ -100,41 +146,67 @@ __global__ void __launch_bounds__(128) batch_step_kernel(BatchParams<T> p) {
             if (pre[mid] <= r) lo = mid; else hi = mid;
         }
         const int k = lo;
-        const int tile = r - pre[k];
+        const int it = r - pre[k];
         const BatchInst<T> &I = p.inst[k];
+        if (stage < 2 && I.tma[stage] && lane == 0) prefetch_tensormap(I.map[stage]);
         if (stage > 0) {  // env k's previous stage must be complete
             const int need = I.items[stage - 1];
             const int *cnt = p.done + 4 * k + (stage - 1);
-            int it = 0;
-            while (ld_acquire(cnt) < need) {
-                if (++it > kDepWaitLimit) {
-                    if (lane == 0) atomicOr(p.err, 2);
-                    return;
+            if (ld_acquire(cnt) < need) {
+                publish();
+                int polls = 0;
+                while (ld_acquire(cnt) < need) {
+                    if (++polls > kDepWaitLimit) {
+                        if (lane == 0) atomicOr(p.err, 2);
+                        return;
+                    }
+                    __nanosleep(100);
                 }
-                __nanosleep(100);
             }
+            fence_proxy_async_global();  // this warp's tensor loads read what the acquire made visible
         }
-        switch (stage) {
-        case 0:
-            if (I.vb16[0]) strided_tile<T, 16, true, false>(I.ax[0], I.gx, tile, sm);
-            else strided_tile<T, (int)sizeof(T), true, false>(I.ax[0], I.gx, tile, sm);
-            break;
-        case 1:
-            if (I.vb16[1]) strided_tile<T, 16, false, false>(I.ax[1], I.gy, tile, sm);
-            else strided_tile<T, (int)sizeof(T), false, false>(I.ax[1], I.gy, tile, sm);
-            break;
-        case 2:
-            if (I.vb16[2]) contig_tile<T, 16>(I.ax[2], I.gz, tile, sm);
-            else contig_tile<T, (int)sizeof(T)>(I.ax[2], I.gz, tile, sm);
-            break;
-        default: cells_chunk(I, tile); break;
+        bool ok = true;
+        if (stage < 3) {
+            const int t0 = it * p.tiles_per_item, t1 = min(I.tiles[stage], t0 + p.tiles_per_item);
+            for (int tile = t0; tile < t1 && ok; ++tile) {
+                if (stage < 2 && I.tma[stage]) {
+                    const StridedGeom &g = stage == 0 ? I.gx : I.gy;
+                    const int crow = I.crow[stage];
+                    ok = stage == 0 ? strided_tma_tile<T, true, false>(I.map[0], I.map[0], I.ax[0], g, crow, tile,
+                                                                       wbase, phase)
+                                    : strided_tma_tile<T, false, false>(I.map[1], I.map[1], I.ax[1], g, crow, tile,
+                                                                        wbase, phase);
+                    phase ^= (1u << ((g.n + crow - 1) / crow)) - 1u;
+                } else if (stage == 2 && I.tma[2]) {
+                    switch (I.S) {  // the substrate count as a constant where it is a common one
+                    case 1: ok = contig_pipe_tile<T, 1>(I.ax[2], I.gz, I.kc, tile, wbase, phase); break;
+                    case 2: ok = contig_pipe_tile<T, 2>(I.ax[2], I.gz, I.kc, tile, wbase, phase); break;
+                    case 4: ok = contig_pipe_tile<T, 4>(I.ax[2], I.gz, I.kc, tile, wbase, phase); break;
+                    case 8: ok = contig_pipe_tile<T, 8>(I.ax[2], I.gz, I.kc, tile, wbase, phase); break;
+                    default: ok = contig_pipe_tile<T, 0>(I.ax[2], I.gz, I.kc, tile, wbase, phase); break;
+                    }
+                    phase ^= (1u << ((I.gz.nz + I.kc - 1) / I.kc)) - 1u;
+                } else if (stage == 0) {
+                    if (I.vb16[0]) strided_tile<T, 16, true, false>(I.ax[0], I.gx, tile, sm);
+                    else strided_tile<T, (int)sizeof(T), true, false>(I.ax[0], I.gx, tile, sm);
+                } else if (stage == 1) {
+                    if (I.vb16[1]) strided_tile<T, 16, false, false>(I.ax[1], I.gy, tile, sm);
+                    else strided_tile<T, (int)sizeof(T), false, false>(I.ax[1], I.gy, tile, sm);
+                } else {
+                    if (I.vb16[2]) contig_tile<T, 16>(I.ax[2], I.gz, tile, sm);
+                    else contig_tile<T, (int)sizeof(T)>(I.ax[2], I.gz, tile, sm);
+                }
+                __syncwarp();  // the tile's shared memory is reused by the next tile
+            }
+        } else {
+            cells_chunk(I, it);
         }
-        __syncwarp();  // the tile's shared memory is reused by the next item
-        if (lane == 0) {
-            __threadfence();
-            atomicAdd(p.done + 4 * k + stage, 1);
-        }
+        if (!ok) return;  // a bounded wait ran out; the error flag is set
+        publish();        // the item before this one
+        pend_k = k;
+        pend_stage = stage;
     }
+    publish();
 }
 
 }  // namespace bfb
@@ -150,8 +222,10 @@ struct bfb_batch_s {
     int *d_prefix = nullptr, *d_done = nullptr, *d_err = nullptr;
     unsigned int *d_queue = nullptr;
     int stage_base[5][2] = {};  // [stage][flags: 0 = diffusion, 1 = diffusion + cells]
-    int smem_elems = 0;
+    void *d_maps = nullptr;     // [n][2] CUtensorMap (64-byte aligned)
+    int warp_bytes = 0;
     int warps = 1;
+    int tiles_per_item = 2;
     int grid[5] = {0, 0, 0, 0, 0};  // resident CTAs for warps = 1..4
     cudaGraphExec_t graph = nullptr;
     int graph_flags = -1;
@@ -172,18 +246,46 @@ using namespace bfb;
 template <typename T>
 static int batch_upload(bfb_batch_s *b, double dt) {
     std::vector<BatchInst<T>> inst(b->n);
+    std::vector<CUtensorMap> maps(2 * (size_t)b->n);
     std::vector<int> prefix(4 * (size_t)(b->n + 1), 0);
-    size_t smem = 0;
+    const int eb = (int)sizeof(T);
+    size_t tile_bytes = 0;
+    const CUtensorMap *dmaps = static_cast<const CUtensorMap *>(b->d_maps);
     for (int k = 0; k < b->n; ++k) {
         bfb_env_s *e = b->envs[k];
         BatchInst<T> &I = inst[k];
         for (int a = 0; a < 3; ++a) I.ax[a] = env_sweep_args<T>(e, a, dt);
         int st = env_tile_plan(e, sizeof(T), &I.gx, &I.gy, &I.gz, I.vb16);
         if (st) return st;
-        I.items[0] = I.gx.n_slabs * I.gx.ncb;
-        I.items[1] = I.gy.n_slabs * I.gy.ncb;
-        I.items[2] = (int)((I.gz.nrows + I.gz.R - 1) / I.gz.R);
+        I.tiles[0] = I.gx.n_slabs * I.gx.ncb;
+        I.tiles[1] = I.gy.n_slabs * I.gy.ncb;
+        I.tiles[2] = (int)((I.gz.nrows + I.gz.R - 1) / I.gz.R);
+        for (int a = 0; a < 3; ++a) I.items[a] = (I.tiles[a] + b->tiles_per_item - 1) / b->tiles_per_item;
         I.items[3] = (int)(((long long)e->n_occ * e->S + kCellChunk - 1) / kCellChunk);
+        // TMA tiles where the env's own launch shape would use them
+        for (int a = 0; a < 2; ++a) {
+            const StridedGeom &g = a == 0 ? I.gx : I.gy;
+            I.tma[a] = e->use_tma && e->tuning.tma[a] && e->tma_ok[a] &&
+                       strided_tma_warp_bytes(g.n, e->tma_crow[a], eb) <= (size_t)kMaxSmem;
+            I.crow[a] = e->tma_crow[a];
+            maps[2 * (size_t)k + a] = e->tmap[a];
+            I.map[a] = dmaps + 2 * (size_t)k + a;
+            tile_bytes = std::max(tile_bytes, I.tma[a] ? strided_tma_warp_bytes(g.n, I.crow[a], eb) - 128
+                                                       : (size_t)g.n * 32 * eb);
+        }
+        {
+            const long long L = (long long)e->nz * e->S;
+            const bool base16 = (reinterpret_cast<uintptr_t>(e->field) & 15) == 0;
+            I.tma[2] = e->use_tma && e->tuning.tma[2] && e->S <= 32 && base16 && (L * eb) % 16 == 0 &&
+                       ((long long)I.gz.RS * eb) % 16 == 0 && (L * eb) * I.gz.R < (1 << 20);
+            int q = 16;
+            for (int v = e->S * eb; v % 2 == 0 && q > 1; v /= 2) q /= 2;  // q = 16 / gcd(16, S*elem)
+            const int chunks = e->tuning.chunks[2];
+            const int kc = (e->nz + chunks - 1) / chunks;
+            I.kc = (kc + q - 1) / q * q;
+            if ((e->nz + I.kc - 1) / I.kc > 16) I.tma[2] = 0;  // one mbarrier per row group
+            tile_bytes = std::max(tile_bytes, (size_t)I.gz.R * I.gz.RS * eb);
+        }
         I.f = static_cast<T *>(e->field);
         I.S = e->S;
         I.n_occ = e->n_occ;
@@ -192,12 +294,10 @@ static int batch_upload(bfb_batch_s *b, double dt) {
         I.t1 = static_cast<const T *>(e->ag_t1);
         I.t2 = static_cast<const T *>(e->ag_t2);
         for (int s = 0; s < 4; ++s) prefix[(size_t)s * (b->n + 1) + k + 1] = prefix[(size_t)s * (b->n + 1) + k] + I.items[s];
-        smem = std::max(smem, (size_t)I.gx.n * 32);
-        smem = std::max(smem, (size_t)I.gy.n * 32);
-        smem = std::max(smem, (size_t)I.gz.R * I.gz.RS);
     }
-    if (smem * sizeof(T) > 227 * 1024) return fail(BFB_ERR_UNSUPPORTED, "batch: an env's tile does not fit in shared memory");
-    b->smem_elems = (int)smem;
+    const size_t warp_bytes = (128 + tile_bytes + 127) / 128 * 128;
+    if (warp_bytes > (size_t)kMaxSmem) return fail(BFB_ERR_UNSUPPORTED, "batch: an env's tile does not fit in shared memory");
+    b->warp_bytes = (int)warp_bytes;
     for (int f = 0; f < 2; ++f) {
         b->stage_base[0][f] = 0;
         for (int s = 0; s < 4; ++s) {
@@ -205,19 +305,20 @@ static int batch_upload(bfb_batch_s *b, double dt) {
             b->stage_base[s + 1][f] = b->stage_base[s][f] + cnt;
         }
     }
+    BFB_CUDA(cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice));
     BFB_CUDA(cudaMemcpy(b->d_inst, inst.data(), sizeof(BatchInst<T>) * b->n, cudaMemcpyHostToDevice));
     BFB_CUDA(cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice));
-    BFB_CUDA(cudaFuncSetAttribute(batch_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    BFB_CUDA(cudaFuncSetAttribute(batch_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    int sms = 0;
+    BFB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
     for (int w = 1; w <= 4; ++w) {
         int per_sm = 0;
-        const size_t bytes = (size_t)w * smem * sizeof(T);
-        if (bytes > 227 * 1024) {
+        const size_t bytes = (size_t)w * warp_bytes;
+        if (bytes > (size_t)kMaxSmem) {
             b->grid[w] = 0;
             continue;
         }
         BFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel<T>, 32 * w, bytes));
-        int sms = 0;
-        BFB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
         b->grid[w] = per_sm * sms;
     }
     return BFB_OK;
@@ -234,12 +335,14 @@ static int batch_launch(bfb_batch_s *b, int flags, cudaStream_t s) {
     p.queue = b->d_queue;
     p.err = b->d_err;
     p.n = b->n;
-    p.smem_elems = b->smem_elems;
+    p.warp_bytes = b->warp_bytes;
     p.stages = f ? 4 : 3;
+    p.tiles_per_item = b->tiles_per_item;
     BFB_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), s));
     BFB_CUDA(cudaMemsetAsync(b->d_done, 0, sizeof(int) * 4 * b->n, s));
-    const int w = b->warps;
-    const size_t bytes = (size_t)w * b->smem_elems * sizeof(T);
+    int w = b->warps;
+    while (w > 1 && b->grid[w] == 0) --w;  // the widest CTA that fits
+    const size_t bytes = (size_t)w * b->warp_bytes;
     const int grid = std::max(1, b->grid[w]);
     batch_step_kernel<T><<<grid, 32 * w, bytes, s>>>(p);
     BFB_CUDA(cudaGetLastError());
@@ -275,6 +378,7 @@ BFB_API int bfb_batch_create(bfb_batch *out, int n_envs, const bfb_env *envs) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_done, sizeof(int) * 4 * n_envs);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_maps, sizeof(CUtensorMap) * 2 * n_envs);  // 256-byte aligned
     if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -297,6 +401,7 @@ BFB_API int bfb_batch_destroy(bfb_batch b) {
     cudaFree(b->d_done);
     cudaFree(b->d_err);
     cudaFree(b->d_queue);
+    cudaFree(b->d_maps);
     if (b->own_stream) cudaStreamDestroy(b->own_stream);
     delete b;
     return BFB_OK;
@@ -304,9 +409,12 @@ BFB_API int bfb_batch_destroy(bfb_batch b) {
 
 BFB_API int bfb_batch_set_option(bfb_batch b, int option, int value) {
     if (!b) return fail(BFB_ERR_INVALID_ARG, "null bfb_batch");
-    if (option != BFB_BATCH_OPT_WARPS_PER_CTA || value < 1 || value > 4)
+    if (option == BFB_BATCH_OPT_WARPS_PER_CTA && value >= 1 && value <= 4)
+        b->warps = value;
+    else if (option == BFB_BATCH_OPT_TILES_PER_ITEM && value >= 1 && value <= 64)
+        b->tiles_per_item = value;
+    else
         return fail(BFB_ERR_INVALID_ARG, "bfb_batch_set_option: unknown option or value");
-    b->warps = value;
     batch_drop_graph(b);
     return BFB_OK;
 }
@@ -367,6 +475,75 @@ BFB_API int bfb_batch_simulate(bfb_batch b, double dt, int n_steps, int flags) {
         for (bfb_env e : b->envs) BFB_CUDA(cudaStreamSynchronize(e->stream));
     }
     for (int q = 0; q < n_steps; ++q) BFB_CUDA(cudaGraphLaunch(b->graph, b->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, int *chosen, double *best_ms) {
+    if (!b) return fail(BFB_ERR_INVALID_ARG, "null bfb_batch");
+    if (!(dt > 0) || trials < 1) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0 and trials >= 1");
+    BFB_CUDA(cudaSetDevice(b->device));
+    // the trial steps advance the fields: keep copies and put them back
+    std::vector<void *> saved(b->n, nullptr);
+    int st = BFB_OK;
+    for (int k = 0; k < b->n && !st; ++k) {
+        bfb_env_s *e = b->envs[k];
+        cudaError_t ce = cudaStreamSynchronize(e->stream);
+        if (ce == cudaSuccess) ce = cudaMalloc(&saved[k], e->elem * e->N);
+        if (ce == cudaSuccess) ce = cudaMemcpy(saved[k], e->field, e->elem * e->N, cudaMemcpyDeviceToDevice);
+        if (ce != cudaSuccess) st = cuda_fail(ce, "bfb_batch_autotune: field copy");
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!st) {
+        cudaError_t ce = cudaEventCreate(&e0);
+        if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+        if (ce != cudaSuccess) st = cuda_fail(ce, "cudaEventCreate");
+    }
+    const int old_w = b->warps, old_t = b->tiles_per_item;
+    int best_w = old_w, best_t = old_t;
+    double best = -1.0;
+    for (int w : {1, 2, 4}) {
+        for (int tpi : {1, 2, 4, 8}) {
+            if (st) break;
+            b->warps = w;
+            b->tiles_per_item = tpi;
+            batch_drop_graph(b);
+            if ((st = bfb_batch_simulate(b, dt, 1, flags))) break;  // builds the graph; warm
+            cudaError_t ce = cudaEventRecord(e0, b->stream);
+            if (ce == cudaSuccess && (st = bfb_batch_simulate(b, dt, trials, flags))) break;
+            if (ce == cudaSuccess) ce = cudaEventRecord(e1, b->stream);
+            if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+            float ms = 0;
+            if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+            if (ce != cudaSuccess) {
+                st = cuda_fail(ce, "bfb_batch_autotune: timing");
+                break;
+            }
+            if (best < 0 || ms / trials < best) {
+                best = ms / trials;
+                best_w = w;
+                best_t = tpi;
+            }
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (!st) st = bfb_batch_synchronize(b);
+    for (int k = 0; k < b->n; ++k) {
+        if (!saved[k]) continue;
+        bfb_env_s *e = b->envs[k];
+        const cudaError_t ce = cudaMemcpy(e->field, saved[k], e->elem * e->N, cudaMemcpyDeviceToDevice);
+        if (ce != cudaSuccess && !st) st = cuda_fail(ce, "bfb_batch_autotune: field restore");
+        cudaFree(saved[k]);
+    }
+    b->warps = st ? old_w : best_w;
+    b->tiles_per_item = st ? old_t : best_t;
+    batch_drop_graph(b);
+    if (st) return st;
+    if (chosen) {
+        chosen[0] = best_w;
+        chosen[1] = best_t;
+    }
+    if (best_ms) *best_ms = best;
     return BFB_OK;
 }
 

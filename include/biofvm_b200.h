@@ -220,13 +220,21 @@ BFB_API int bfb_checksum(bfb_env env, double *out);
  * bfb_simulate call per env (the per-instance launch loop). Not in the
  * reference, which runs one Microenvironment per MPI job. */
 typedef struct bfb_batch_s *bfb_batch;
-#define BFB_BATCH_OPT_WARPS_PER_CTA 1 /* 1..4, default 1 */
+#define BFB_BATCH_OPT_WARPS_PER_CTA 1   /* 1..4, default 1 */
+#define BFB_BATCH_OPT_TILES_PER_ITEM 2  /* warp tiles per queue item, 1..64, default 2 */
 BFB_API int bfb_batch_create(bfb_batch *out, int n_envs, const bfb_env *envs);
 BFB_API int bfb_batch_destroy(bfb_batch batch);
 BFB_API int bfb_batch_set_option(bfb_batch batch, int option, int value);
 BFB_API int bfb_batch_simulate(bfb_batch batch, double dt, int n_steps, int flags);
 BFB_API int bfb_batch_simulate_loop(bfb_batch batch, double dt, int n_steps, int flags);
 BFB_API int bfb_batch_synchronize(bfb_batch batch);
+/* Times bfb_batch_simulate for warps per CTA {1, 2, 4} x tiles per item
+ * {1, 2, 4, 8} (one warm step and `trials` timed steps each, CUDA events),
+ * keeps the fastest and returns it in chosen[2] = {warps, tiles per item}
+ * and its milliseconds per step in *best_ms (either may be NULL). The trial
+ * steps advance the envs' fields, so every field is saved first and restored
+ * before returning. Not in the reference. */
+BFB_API int bfb_batch_autotune(bfb_batch batch, double dt, int flags, int trials, int *chosen, double *best_ms);
 
 /* ---- Reverse mode ---------------------------------------------------------
  * No counterpart in the reference. Runs n_steps steps of `flags`

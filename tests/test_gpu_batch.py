@@ -70,6 +70,56 @@ def test_batch_small_fp64_bitexact(bfb, oracle, warps):
         assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps)), spec["shape"]
 
 
+def make_aligned_instance(bfb, rng, prec, dt, n_agents=400):
+    """Shapes whose row pitches suit TMA on every axis (edges multiples of 8,
+    S in {2, 4}), so every stage of the persistent kernel runs TMA tiles."""
+    shape = tuple(int(v) * 8 for v in rng.integers(2, 7, 3))
+    S = int(rng.choice([2, 4]))
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    rho0 = rng.random((*shape, S))
+    fm = np.zeros((6, S), np.uint8)
+    fm[:, 0] = [1, 1, 0, 1, 1, 0]
+    act = np.zeros(S, np.uint8)
+    act[0] = 1
+    box = np.array(shape) * 20.0
+    pos = rng.random((n_agents, 3)) * box
+    vol = np.full(n_agents, 4.0 / 3.0 * math.pi * 125.0)
+    sec, upt, sat = log_uniform(rng, 1e-2, 10.0, (3, n_agents, S))
+    spec = dict(shape=shape, S=S, D=D, lam=lam, rho0=rho0, fm=fm, act=act, pos=pos, vol=vol, sec=sec, upt=upt,
+                sat=sat, box=(0, 0, 0, *box))
+    return spec, build(bfb, spec, prec, dt)
+
+
+@pytest.mark.parametrize("warps,tiles", [(1, 1), (2, 3), (4, 8), (1, 64)])
+def test_batch_tma_items_fp64_bitexact(bfb, oracle, warps, tiles):
+    rng = np.random.default_rng(900 + warps * 10 + tiles)
+    dt, steps = 0.01, 3
+    specs, envs = zip(*[make_aligned_instance(bfb, rng, bfb.FP64, dt) for _ in range(6)])
+    batch = bfb.Batch(envs)
+    batch.set_warps(warps)
+    batch.set_tiles_per_item(tiles)
+    batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
+    batch.synchronize()
+    for spec, env in zip(specs, envs):
+        assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps)), spec["shape"]
+
+
+def test_batch_autotune_restores_fields(bfb, oracle):
+    rng = np.random.default_rng(31)
+    dt, steps = 0.01, 2
+    specs, envs = zip(*[make_aligned_instance(bfb, rng, bfb.FP64, dt) for _ in range(5)])
+    batch = bfb.Batch(envs)
+    before = [e.get_field_raw() for e in envs]
+    (w, t), ms = batch.autotune(dt, bfb.STEP_DIFFUSION | bfb.STEP_CELLS, trials=1)
+    assert w in (1, 2, 4) and t in (1, 2, 4, 8) and ms > 0
+    for e, b0 in zip(envs, before):
+        assert np.array_equal(e.get_field_raw(), b0)
+    batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
+    batch.synchronize()
+    for spec, env in zip(specs, envs):
+        assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps))
+
+
 def test_batch_fp32_equals_per_instance_loop(bfb):
     rng = np.random.default_rng(405)
     dt, steps = 0.01, 5
@@ -98,6 +148,7 @@ def test_config4_batch_vs_loop_and_fp64_check(bfb):
     vs = sum(int(np.prod(sp["shape"])) * sp["S"] for sp in specs)
     flags = bfb.STEP_DIFFUSION | bfb.STEP_CELLS
     batch = bfb.Batch(envs)
+    tuned, _ = batch.autotune(dt, flags, trials=2)  # warps per CTA and tiles per item
     batch.simulate(dt, 2, flags)  # warm-up (graph capture)
     batch.synchronize()
     t0 = time.perf_counter()
@@ -121,6 +172,6 @@ def test_config4_batch_vs_loop_and_fp64_check(bfb):
         errs.append(envs[q].compare(e64)[0])
         e64.close()
     print(f"\nconfig 4 (256 envs, {vs / 1e6:.0f} M voxel*substrates, 200 steps): persistent batch "
-          f"{t_batch * 1e3:.3f} ms/step ({vs / t_batch:.3e} vox*sub/s), per-instance loop {t_loop * 1e3:.3f} ms/step "
+          f"(warps, tiles per item = {tuned}) {t_batch * 1e3:.3f} ms/step ({vs / t_batch:.3e} vox*sub/s), per-instance loop {t_loop * 1e3:.3f} ms/step "
           f"({vs / t_loop:.3e}); FP32 vs FP64 rel Linf on 8 envs: max {max(errs):.2e}")
     assert max(errs) <= 1e-5
