@@ -71,7 +71,8 @@ def config(extra=None):
     c = {"workload": f"LOD diffusion-decay step, {NX}^3 voxels x {S} substrates, dt={DT}, dx={DX}, "
                      "no Dirichlet, no agents",
          "grid": [NX, NY, NZ], "substrates": S, "dt": DT,
-         "l2": "inputs larger than L2 (field 537 MB FP32 / 1074 MB FP64 > 126 MB)",
+         "l2": f"inputs larger than L2 (field {NX * NY * NZ * S * 4 / 1e6:.0f} MB FP32 / "
+               f"{NX * NY * NZ * S * 8 / 1e6:.0f} MB FP64 > 126 MB)",
          "parallelism": "replicas only (one grid per GPU)"}
     if extra:
         c.update(extra)
@@ -275,7 +276,10 @@ def run_our_arm(args):
         env.set_coefficients(D, lam)
         env.set_field(rho0)
         env.set_stream(stream.cuda_stream)
-        tuned, tuned_ms = env.autotune(DT, trials=3)  # launch shapes chosen by the library's autotuner
+        if args.no_autotune:  # the library's default launch shapes (profiling runs: ncu distorts the tuner's timing)
+            tuned = env.get_tuning()
+        else:
+            tuned, _ = env.autotune(DT, trials=3)  # launch shapes chosen by the library's autotuner
         env.simulate(DT, warm, bfb.STEP_DIFFUSION)
         barrier()
         clocks = Clocks(local)
@@ -366,7 +370,8 @@ def run_our_arm(args):
         "data": "synthetic (seeded U[0,1) field, log-uniform D/lambda)",
         "config": config(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": ncu_traffic(f"fp32_{phases[dom]}"), "kernel": phases[dom],
+                     "traffic": ncu_traffic(f"fp32_{phases[dom]}") if (NX, S) == (256, 8) else None,
+                     "kernel": phases[dom],
                      "algorithmic_bytes_per_launch": bytes_launch, "peak_source": peak_src,
                      "ms_per_launch": float(per[dom])},
         "step_roofline": {"achieved": step_bytes / (ms_step / 1e3) / 1e9, "frac": step_bytes / (ms_step / 1e3) / 1e9 / peak,
@@ -378,7 +383,7 @@ def run_our_arm(args):
         "fp32_over_fp64": value / value64,
         "tuning": {"fp32": r32["tuning"], "fp64": r64["tuning"],
                    "fields": "per sweep x, y, z: (TMA tiles 1 / cp.async 0, warps per CTA, row groups per tile), "
-                             "chosen by bfb_autotune before the warm-up"},
+                             + ("the library defaults" if args.no_autotune else "chosen by bfb_autotune before the warm-up")},
         "fp32_error_vs_fp64": {"rel_linf": err_linf, "rel_l2": err_l2, "after_steps": n_steps_run},
         "clocks": r32["clocks"],
         "e2e": {"value": world * V * S * K_e2e / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": V * S * 8,
@@ -411,6 +416,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=256, help="edge of the cubic grid (profiling small cases)")
     ap.add_argument("--substrates", type=int, default=8)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes (for profiler runs, whose timing would mislead the tuner)")
     args = ap.parse_args()
     global NX, NY, NZ, S
     NX = NY = NZ = args.grid

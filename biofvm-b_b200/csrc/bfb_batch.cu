@@ -69,6 +69,33 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
     return v;
 }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// Waits until at most `newer` of this thread's most recent bulk groups are
+// still pending (the older ones have completed); counts above 16 wait for 16.
+template <int N>
+__device__ __forceinline__ void bulk_wait_group() {
+    asm volatile("cp.async.bulk.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_older(int newer) {
+    switch (newer) {
+    case 0: bulk_wait_group<0>(); break;
+    case 1: bulk_wait_group<1>(); break;
+    case 2: bulk_wait_group<2>(); break;
+    case 3: bulk_wait_group<3>(); break;
+    case 4: bulk_wait_group<4>(); break;
+    case 5: bulk_wait_group<5>(); break;
+    case 6: bulk_wait_group<6>(); break;
+    case 7: bulk_wait_group<7>(); break;
+    case 8: bulk_wait_group<8>(); break;
+    case 9: bulk_wait_group<9>(); break;
+    case 10: bulk_wait_group<10>(); break;
+    case 11: bulk_wait_group<11>(); break;
+    case 12: bulk_wait_group<12>(); break;
+    case 13: bulk_wait_group<13>(); break;
+    case 14: bulk_wait_group<14>(); break;
+    case 15: bulk_wait_group<15>(); break;
+    default: bulk_wait_group<16>(); break;
+    }
+}
 __device__ __forceinline__ void fence_proxy_async_global() {
     asm volatile("fence.proxy.async.global;\n" ::: "memory");
 }
@@ -120,10 +147,11 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
     // while the warp already loads the next item. It is published before the
     // warp waits on any dependency (it may be the one waited for) and on exit.
     int pend_k = -1, pend_stage = 0;
+    int groups = 0;  // bulk store groups the current item has committed so far
     auto publish = [&]() {
         if (pend_k < 0) return;
         if (lane == 0) {
-            bulk_wait_all();             // its bulk stores have completed ...
+            bulk_wait_older(groups);     // its bulk stores (older than the current item's) have completed ...
             fence_proxy_async_global();  // ... are ordered with the generic release below ...
             __threadfence();
             atomicAdd(p.done + 4 * pend_k + pend_stage, 1);  // ... and published
@@ -148,6 +176,7 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
         const int k = lo;
         const int it = r - pre[k];
         const BatchInst<T> &I = p.inst[k];
+        groups = 0;
         if (stage < 2 && I.tma[stage] && lane == 0) prefetch_tensormap(I.map[stage]);
         if (stage > 0) {  // env k's previous stage must be complete
             const int need = I.items[stage - 1];
@@ -177,6 +206,7 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
                                     : strided_tma_tile<T, false, false>(I.map[1], I.map[1], I.ax[1], g, crow, tile,
                                                                         wbase, phase);
                     phase ^= (1u << ((g.n + crow - 1) / crow)) - 1u;
+                    groups += (g.n + crow - 1) / crow;  // one store group per row group
                 } else if (stage == 2 && I.tma[2]) {
                     switch (I.S) {  // the substrate count as a constant where it is a common one
                     case 1: ok = contig_pipe_tile<T, 1>(I.ax[2], I.gz, I.kc, tile, wbase, phase); break;
@@ -186,6 +216,7 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
                     default: ok = contig_pipe_tile<T, 0>(I.ax[2], I.gz, I.kc, tile, wbase, phase); break;
                     }
                     phase ^= (1u << ((I.gz.nz + I.kc - 1) / I.kc)) - 1u;
+                    groups += (I.gz.nz + I.kc - 1) / I.kc;
                 } else if (stage == 0) {
                     if (I.vb16[0]) strided_tile<T, 16, true, false>(I.ax[0], I.gx, tile, sm);
                     else strided_tile<T, (int)sizeof(T), true, false>(I.ax[0], I.gx, tile, sm);
@@ -202,9 +233,10 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
             cells_chunk(I, it);
         }
         if (!ok) return;  // a bounded wait ran out; the error flag is set
-        publish();        // the item before this one
+        publish();        // the item before this one; this item's stores stay in flight
         pend_k = k;
         pend_stage = stage;
+        groups = 0;
     }
     publish();
 }

@@ -56,7 +56,7 @@ struct BulkTerms {
 struct SweepTuning {
     int tma[3] = {1, 1, 1};     // TMA tiles (when the grid allows them) or cp.async tiles
     int warps[3] = {1, 1, 1};   // warps (= tiles) per CTA; one packs shared memory tightest
-    int chunks[3] = {4, 4, 4};  // row groups per TMA tile (pipeline stages)
+    int chunks[3] = {2, 2, 2};  // row groups per TMA tile (pipeline stages); 2 measured fastest
 };
 
 }  // namespace bfb

@@ -195,7 +195,7 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
  * cp.async tiles; shape[3*axis + 1] = warps (tiles) per CTA, 1..4;
  * shape[3*axis + 2] = row groups per TMA tile (pipeline stages), 1..16.
  * Every shape computes the same numbers (FP64 bit for bit); only the speed
- * differs. Defaults {1, 1, 4} per axis. bfb_autotune times each candidate
+ * differs. Defaults {1, 1, 2} per axis. bfb_autotune times each candidate
  * (TMA / cp.async x 1, 2, 4 warps x 2, 4, 8 row groups) of each sweep with
  * CUDA events over `trials` launches, out of place from the env's field into
  * a scratch field (the field is unchanged; the scratch is freed on return),

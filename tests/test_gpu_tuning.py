@@ -126,5 +126,5 @@ def test_set_tuning_rejects_bad_shapes(bfb, bad):
     env = bfb.Env((8, 8, 8), 1, precision=bfb.FP64)
     with pytest.raises(bfb.BFBError):
         env.set_tuning(bad)
-    assert env.get_tuning() == [(1, 1, 4)] * 3
+    assert env.get_tuning() == [(1, 1, 2)] * 3
     env.close()
