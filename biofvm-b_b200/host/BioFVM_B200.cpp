@@ -329,6 +329,38 @@ void Microenvironment::sync_to_device() {
     report(upload_all_if_needed(), "sync_to_device");
 }
 
+// compute_all_gradient_vectors (BioFVM_microenvironment.cpp:1243-1402): all
+// voxels at once on the device; the per-voxel compute_gradient_vector
+// (:1404-1535) gives the same values on the uniform mesh, so a request for
+// one voxel also fills every voxel.
+void Microenvironment::compute_all_gradient_vectors() {
+    const int V = number_of_voxels(), S = number_of_densities();
+    std::vector<double> flat(3 * (size_t)V * S);
+    int st = upload_all_if_needed();
+    if (!st) st = bfb_get_gradients(env_, flat.data());
+    report(st, "compute_all_gradient_vectors");
+    if (st) return;
+    gradient_vectors_.assign(V, std::vector<gradient>(S, gradient(3, 0.0)));
+    for (int n = 0; n < V; ++n)
+        for (int q = 0; q < S; ++q)
+            for (int c = 0; c < 3; ++c) gradient_vectors_[n][q][c] = flat[((size_t)n * S + q) * 3 + c];
+    gradients_valid_ = true;
+}
+
+// reset_all_gradient_vectors (BioFVM_microenvironment.cpp:1543-1553): marks
+// every voxel not computed, so the next access computes again. As in the
+// reference, a later step alone does not invalidate stored gradients.
+void Microenvironment::reset_all_gradient_vectors() {
+    gradient_vectors_.assign(number_of_voxels(), std::vector<gradient>(number_of_densities(), gradient(3, 0.0)));
+    gradients_valid_ = false;
+}
+
+std::vector<Microenvironment::gradient> &Microenvironment::gradient_vector(int n) {
+    if (!gradients_valid_) compute_all_gradient_vectors();
+    if (gradient_vectors_.empty()) reset_all_gradient_vectors();  // a failed computation still returns storage
+    return gradient_vectors_[n];
+}
+
 std::vector<double> Microenvironment::checksum() {
     std::vector<double> out(number_of_densities(), 0.0);
     int st = upload_all_if_needed();

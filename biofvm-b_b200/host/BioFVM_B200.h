@@ -124,6 +124,19 @@ class Microenvironment {
     // y-lo, y-hi, z-lo, z-hi), ANDed with the per-substrate activation.
     void set_dirichlet_face_mask(const std::vector<uint8_t> &mask);
 
+    // ---- gradients (BioFVM_microenvironment.cpp:1195-1554): computed on the
+    // device, held on the host in the reference's nested layout
+    typedef std::vector<double> gradient;
+    void compute_all_gradient_vectors();
+    void compute_gradient_vector(int n) { (void)n; compute_all_gradient_vectors(); }
+    void reset_all_gradient_vectors();
+    std::vector<gradient> &gradient_vector(int n);
+    std::vector<gradient> &gradient_vector(int i, int j, int k) { return gradient_vector(voxel_index(i, j, k)); }
+    std::vector<gradient> &gradient_vector(int i, int j) { return gradient_vector(voxel_index(i, j, 0)); }
+    std::vector<gradient> &nearest_gradient_vector(std::vector<double> &position) {
+        return gradient_vector(nearest_voxel_index(position));
+    }
+
     // ---- the hot path
     void simulate_diffusion_decay(double dt, int mpi_Size = 1, int mpi_Rank = 0, int *mpi_Coords = nullptr,
                                   int *mpi_Dims = nullptr, MPI_Comm comm = 0);
@@ -169,6 +182,8 @@ class Microenvironment {
     bool agents_dirty_ = true;
     int status = BFB_OK;
     std::vector<double> D_uploaded_, lambda_uploaded_;
+    std::vector<std::vector<gradient>> gradient_vectors_;  // [V][S] of 3
+    bool gradients_valid_ = false;
     friend class Basic_Agent;
 };
 

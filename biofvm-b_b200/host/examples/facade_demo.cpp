@@ -5,9 +5,11 @@
 // them exactly and check the output field against the oracle.
 //
 //   facade_demo <out.bin> <precision 0=FP64|1=FP32> <host sync 0=every step|1=lazy> [steps]
+// writes the field to out.bin and its gradient vectors to out.bin.grad
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "BioFVM_B200.h"
@@ -72,6 +74,13 @@ int main(int argc, char **argv) {
     if (!f) return 1;
     std::fwrite(M.p_density_vectors->data(), sizeof(double), M.p_density_vectors->size(), f);
     std::fclose(f);
+    // chemotaxis-style consumer: the gradient vectors after the last step
+    M.compute_all_gradient_vectors();
+    std::FILE *g = std::fopen((std::string(argv[1]) + ".grad").c_str(), "wb");
+    if (!g) return 1;
+    for (int n = 0; n < M.number_of_voxels(); ++n)
+        for (int d = 0; d < S; ++d) std::fwrite(M.gradient_vector(n)[d].data(), sizeof(double), 3, g);
+    std::fclose(g);
     std::printf("facade_demo: %d x %d x %d x %d, %d steps, checksum %.17g\n", M.mesh.x_size, M.mesh.y_size,
                 M.mesh.z_size, S, steps, M.checksum()[0]);
     return 0;

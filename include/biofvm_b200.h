@@ -206,6 +206,18 @@ BFB_API int bfb_set_tuning(bfb_env env, const int *shape);
 BFB_API int bfb_get_tuning(bfb_env env, int *shape);
 BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double *best_ms);
 
+/* Gradient vectors of every substrate at every voxel, replacing
+ * Microenvironment::compute_all_gradient_vectors (BioFVM_microenvironment.cpp:
+ * 1243-1402) and the per-voxel compute_gradient_vector (:1404-1535), which
+ * agree on the uniform mesh: out[(n*S + q)*3 + c] is the central difference
+ * along axis c over 2*dx inside the grid and the one-sided difference over dx
+ * at its two ends; 0 on an axis of one voxel. bfb_compute_gradients writes
+ * 3*V*S elements of the env's precision to device memory, on the env's
+ * stream (returns without waiting); bfb_get_gradients returns host doubles.
+ * FP64 is bit-exact with the reference. */
+BFB_API int bfb_compute_gradients(bfb_env env, void *out_dev);
+BFB_API int bfb_get_gradients(bfb_env env, double *out_host);
+
 /* Per-substrate FP64 sum of the field over all voxels (mass checksum). */
 BFB_API int bfb_checksum(bfb_env env, double *out);
 

@@ -358,3 +358,50 @@ void orc_lod_step_adjoint(const double *rho_in, double *lam, int nx, int ny, int
     free(s);
     free(c1);
 }
+
+/* Microenvironment::compute_all_gradient_vectors (BioFVM_microenvironment.cpp:
+ * 1243-1402): per voxel and substrate, out[(n*S + q)*3 + c] =
+ *   (rho[+1] - rho[-1]) / (2*h)   inside the axis,
+ *   (rho[+1] - rho[ 0]) / h       at the low end,
+ *   (rho[ 0] - rho[-1]) / h       at the high end,
+ * with h = dx on every axis (uniform mesh; the reference's two_dx is the
+ * first call's mesh.dx doubled, :1245-1255), neighbours along x / y / z at
+ * ny*nz*S / nz*S / S elements (thomas_i/j/k_jump, BioFVM_parallel.cpp:724-726),
+ * each value formed as `g = rho[a]; g -= rho[b]; g /= h` (no contraction).
+ * An axis of one voxel has no neighbour: the reference leaves z untouched
+ * there (:1352-1354) and reads out of range for x or y; the oracle writes 0
+ * for every such axis. */
+void orc_gradients(const double *rho, int nx, int ny, int nz, int S, double dx, double *out)
+{
+    const int ns[3] = {nx, ny, nz};
+    const size_t jump[3] = {(size_t)ny * nz * S, (size_t)nz * S, (size_t)S};
+    const double two_dx = dx * 2.0;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                const int pos[3] = {i, j, k};
+                const size_t n = ((size_t)i * ny + j) * nz + k;
+                for (int q = 0; q < S; ++q) {
+                    const size_t e = n * S + q;
+                    for (int c = 0; c < 3; ++c) {
+                        double g = 0.0;
+                        if (ns[c] > 1) {
+                            if (pos[c] == 0) {
+                                g = rho[e + jump[c]];
+                                g -= rho[e];
+                                g /= dx;
+                            } else if (pos[c] == ns[c] - 1) {
+                                g = rho[e];
+                                g -= rho[e - jump[c]];
+                                g /= dx;
+                            } else {
+                                g = rho[e + jump[c]];
+                                g -= rho[e - jump[c]];
+                                g /= two_dx;
+                            }
+                        }
+                        out[e * 3 + c] = g;
+                    }
+                }
+            }
+}

@@ -68,6 +68,10 @@ void orc_cells_step(double *rho, int S, int n, const int *voxel, const double *t
 /* Per-substrate sum of rho over voxels, FP64, voxel order. */
 void orc_checksum(const double *rho, int64_t V, int S, double *out);
 
+/* Gradient vectors of every substrate at every voxel, out[(n*S + q)*3 + c]
+ * (compute_all_gradient_vectors, BioFVM_microenvironment.cpp:1243-1402). */
+void orc_gradients(const double *rho, int nx, int ny, int nz, int S, double dx, double *out);
+
 /* Reverse-mode of one orc_lod_step: given lam = dL/d(rho_out), on return
  * lam = dL/d(rho_in); gD[d], gL[d] are incremented by dL/dD_d, dL/dlambda_d.
  * rho_in is the step's input field (left unchanged). */

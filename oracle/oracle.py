@@ -70,6 +70,7 @@ class Oracle:
                                           ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, _dp]
         L.orc_cells_step.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _ip, _dp, _dp, _up]
         L.orc_checksum.argtypes = [_dp, ctypes.c_int64, ctypes.c_int, _dp]
+        L.orc_gradients.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]
         L.orc_lod_step_adjoint.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _up, _dp, _dp]
 
@@ -155,6 +156,14 @@ class Oracle:
         self.lib.orc_checksum(_d(rho), rho.size // S, S, _d(out))
         return out
 
+    def gradients(self, rho, dx):
+        """(nx, ny, nz, S, 3) gradient vectors (orc_gradients)."""
+        rho = f64(rho)
+        nx, ny, nz, S = rho.shape
+        out = np.zeros((nx, ny, nz, S, 3))
+        self.lib.orc_gradients(_d(rho), nx, ny, nz, S, dx, _d(out))
+        return out
+
     def lod_step_adjoint(self, rho_in, lam_out, dt, dx, D, lam_rates, dir_values=None, face_mask=None):
         rho_in = f64(rho_in)
         nx, ny, nz, S = rho_in.shape
@@ -201,6 +210,8 @@ class RefLib:
         L.ref_add_agents.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, ctypes.c_double]
         L.ref_agent_voxels.argtypes = [ctypes.c_void_p, _ip]
         L.ref_cells_step.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.ref_gradients.argtypes = [ctypes.c_void_p, _dp]
+        L.ref_gradients_per_voxel.argtypes = [ctypes.c_void_p, _dp]
 
 
 class RefEnv:
@@ -275,6 +286,14 @@ class RefEnv:
 
     def cells_step(self, dt):
         self.ref.lib.ref_cells_step(self.h, dt)
+
+    def gradients(self, per_voxel=False):
+        """(nx, ny, nz, S, 3) gradient vectors from compute_all_gradient_vectors,
+        or from the per-voxel accessor path."""
+        out = np.zeros((*self.shape, 3))
+        fn = self.ref.lib.ref_gradients_per_voxel if per_voxel else self.ref.lib.ref_gradients
+        fn(self.h, _d(out))
+        return out
 
 
 def set_threads(ref: RefLib, n: int):

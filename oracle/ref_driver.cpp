@@ -222,6 +222,33 @@ void ref_agent_voxels(void *h, int *out) {
 }
 
 // Serial secretion/uptake in creation order (see the file header).
+// compute_all_gradient_vectors (BioFVM_microenvironment.cpp:1243-1402), then
+// the public accessor gradient_vector(n) per voxel: out[(n*S + q)*3 + c]. The
+// jumps it uses are set by the first solver call, so call ref_step first.
+void ref_gradients(void *h, double *out) {
+    Microenvironment *M = (Microenvironment *)h;
+    M->compute_all_gradient_vectors();
+    const int V = (int)M->mesh.voxels.size(), S = M->number_of_densities();
+    for (int n = 0; n < V; ++n) {
+        std::vector<gradient> &g = M->gradient_vector(n);
+        for (int q = 0; q < S; ++q)
+            for (int c = 0; c < 3; ++c) out[((size_t)n * S + q) * 3 + c] = g[q][c];
+    }
+}
+
+// The per-voxel path: reset, then gradient_vector(n) computes each voxel on
+// demand with compute_gradient_vector (BioFVM_microenvironment.cpp:1404-1535).
+void ref_gradients_per_voxel(void *h, double *out) {
+    Microenvironment *M = (Microenvironment *)h;
+    M->reset_all_gradient_vectors();
+    const int V = (int)M->mesh.voxels.size(), S = M->number_of_densities();
+    for (int n = 0; n < V; ++n) {
+        std::vector<gradient> &g = M->gradient_vector(n);
+        for (int q = 0; q < S; ++q)
+            for (int c = 0; c < 3; ++c) out[((size_t)n * S + q) * 3 + c] = g[q][c];
+    }
+}
+
 void ref_cells_step(void *h, double dt) {
     Microenvironment *M = (Microenvironment *)h;
     RefEnv *e = env_of(M);

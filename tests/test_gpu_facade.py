@@ -53,7 +53,11 @@ def test_facade_demo_matches_oracle(bfb, oracle, tmp_path, precision, sync):
     assert r.returncode == 0, r.stdout + r.stderr
     got = np.fromfile(out, dtype=np.float64).reshape(20, 18, 16, 2)
     want = oracle_demo(oracle, 10)
+    grad = np.fromfile(str(out) + ".grad", dtype=np.float64).reshape(20, 18, 16, 2, 3)
     if precision == 0:
         assert np.array_equal(got, want)
+        assert np.array_equal(grad, oracle.gradients(want, 20.0))
     else:
         assert np.abs(got - want).max() / np.abs(want).max() <= 1e-5
+        # gradients of the FP32 field itself, rounded once to FP32
+        assert np.array_equal(grad, oracle.gradients(got, 20.0).astype(np.float32).astype(np.float64))

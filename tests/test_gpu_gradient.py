@@ -1,0 +1,75 @@
+"""Gradient vectors (bfb_compute_gradients / bfb_get_gradients) against the
+oracle's compute_all_gradient_vectors restatement, which is pinned bit for bit
+to the reference library (tests/test_oracle.py)."""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+from conftest import log_uniform
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _env(bfb, shape, S, prec, rng, steps=3):
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    env = bfb.Env(shape, S, dx=20.0, precision=prec)
+    env.set_coefficients(D, lam)
+    env.set_field(rng.random((*shape, S)) * 10)
+    act = np.ones(S, np.uint8)
+    env.set_dirichlet(act, values=rng.random((*shape, S)) * 5)
+    env.simulate(0.01, steps)
+    return env
+
+
+@pytest.mark.parametrize("shape,S", [((5, 4, 6), 2), ((2, 3, 2), 1), ((7, 5, 3), 3), ((3, 6, 1), 2),
+                                     ((1, 4, 5), 2), ((4, 1, 3), 1), ((33, 17, 40), 5), ((64, 48, 80), 8)])
+def test_gradients_fp64_bitexact(bfb, oracle, shape, S):
+    rng = np.random.default_rng(sum(shape) * 10 + S)
+    env = _env(bfb, shape, S, bfb.FP64, rng)
+    field = env.get_field()
+    assert np.array_equal(env.gradients(), oracle.gradients(field, 20.0))
+    env.close()
+
+
+@pytest.mark.parametrize("shape,S", [((5, 4, 6), 2), ((33, 17, 40), 5), ((64, 48, 80), 8)])
+def test_gradients_fp32_is_the_fp32_field_gradient_rounded_once(bfb, oracle, shape, S):
+    rng = np.random.default_rng(3 + S)
+    env = _env(bfb, shape, S, bfb.FP32, rng)
+    field = env.get_field_raw().astype(np.float64)
+    want = oracle.gradients(field, 20.0).astype(np.float32)
+    dev = torch.empty(3 * field.size, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    env.compute_gradients_device(dev.data_ptr())
+    env.synchronize()
+    assert np.array_equal(dev.cpu().numpy().reshape(want.shape), want)
+    assert np.array_equal(env.gradients(), want.astype(np.float64))
+    env.close()
+
+
+def test_gradients_256cube_bandwidth(bfb):
+    """The chemotaxis consumer at the bench size: one read of the field,
+    three writes; reported, not asserted against a roofline."""
+    rng = np.random.default_rng(1)
+    S = 8
+    env = bfb.Env((256, 256, 256), S, precision=bfb.FP32)
+    env.set_coefficients(log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S))
+    n = 256 ** 3 * S
+    out = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(3):
+        env.compute_gradients_device(out.data_ptr())
+    env.synchronize()
+    # the env works on its own stream: host time around 10 calls, synchronised
+    t0 = time.perf_counter()
+    for _ in range(10):
+        env.compute_gradients_device(out.data_ptr())
+    env.synchronize()
+    ms = (time.perf_counter() - t0) / 10 * 1e3
+    gbs = 4 * n * 4 / (ms / 1e3) / 1e9
+    print(f"\ngradients 256^3 x 8 FP32: {ms:.3f} ms per call, {gbs:.0f} GB/s of algorithmic traffic (1 read + 3 writes)")
+    assert ms < 5.0
+    env.close()

@@ -209,3 +209,25 @@ def test_oracle_multistep_adjoint_with_agents_matches_finite_differences(oracle,
         e[idx] = 1e-3
         fd = (loss(r=rho + e) - loss(r=rho - e)) / 2e-3
         assert abs(fd - g["initial"][idx]) <= 1e-9
+
+
+@needs_ref
+@pytest.mark.parametrize("shape,S", [((5, 4, 6), 2), ((2, 3, 2), 1), ((7, 5, 3), 3), ((3, 6, 1), 2)])
+def test_gradients_oracle_bitexact_with_reference(oracle, rng, shape, S):
+    """compute_all_gradient_vectors of the live reference (after one solver
+    step, which sets the neighbour jumps) equals orc_gradients bit for bit,
+    and so does the per-voxel accessor path on this uniform mesh."""
+    ref = RefLib()
+    dx = 20.0
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-2, 1.0, S)
+    e = RefEnv(ref, (0.0, 0.0, 0.0, shape[0] * dx, shape[1] * dx, shape[2] * dx), dx, D, lam)
+    e.set_dirichlet([0] * S)
+    e.set_field(rng.random((*shape, S)))
+    e.step(0.01, 1)
+    rho = e.field()
+    want = oracle.gradients(rho, dx)
+    got = e.gradients()
+    if shape[2] == 1:  # the reference leaves z untouched (0) when nz == 1
+        assert np.all(got[..., 2] == 0.0)
+    assert np.array_equal(got, want)
+    assert np.array_equal(e.gradients(per_voxel=True), want)
