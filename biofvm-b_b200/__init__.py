@@ -53,7 +53,7 @@ EXPORTS = [
     "bfb_compare_fields", "bfb_field_device_ptr", "bfb_set_dirichlet",
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
-    "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
+    "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_write_matlab", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
     "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_batch_autotune", "bfb_adjoint_run",
     "bfb_checksum_noalloc",
 ]
@@ -115,6 +115,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_checksum": [_vp, _dp],
         "bfb_compute_gradients": [_vp, _vp],
         "bfb_get_gradients": [_vp, _dp],
+        "bfb_write_matlab": [_vp, ctypes.c_char_p],
         "bfb_set_tuning": [_vp, _ip],
         "bfb_get_tuning": [_vp, _ip],
         "bfb_autotune": [_vp, ctypes.c_double, ctypes.c_int, _ip, _dp],
@@ -322,6 +323,10 @@ class Env:
         out = np.empty((*self.shape, 3), dtype=np.float64)
         _check(self.L.bfb_get_gradients(self.h, out.ctypes.data_as(_dp)))
         return out
+
+    def write_matlab(self, filename):
+        """The reference's MATLAB v4 snapshot of the field (bfb_write_matlab)."""
+        _check(self.L.bfb_write_matlab(self.h, str(filename).encode()))
 
     def compute_gradients_device(self, ptr: int):
         """Gradient vectors into a device array of 3*V*S env-precision elements."""

@@ -361,6 +361,12 @@ std::vector<Microenvironment::gradient> &Microenvironment::gradient_vector(int n
     return gradient_vectors_[n];
 }
 
+void Microenvironment::write_to_matlab(std::string filename) {
+    int st = upload_all_if_needed();
+    if (!st) st = bfb_write_matlab(env_, filename.c_str());
+    report(st, "write_to_matlab");
+}
+
 std::vector<double> Microenvironment::checksum() {
     std::vector<double> out(number_of_densities(), 0.0);
     int st = upload_all_if_needed();

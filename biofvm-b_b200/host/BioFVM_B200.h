@@ -145,6 +145,14 @@ class Microenvironment {
     void simulate_cell_sources_and_sinks(double dt);
 
     void display_information(std::ostream &os);
+    // MATLAB v4 snapshot (BioFVM_microenvironment.cpp:1079-1107), packed on the device
+    void write_to_matlab(std::string filename);
+    void write_to_matlab(std::string filename, int rank, int size, MPI_Comm comm) {
+        (void)rank;
+        (void)size;
+        (void)comm;
+        write_to_matlab(filename);
+    }
 
     // ---- B200 additions
     void set_precision(Precision p);  // before the first step

@@ -5,7 +5,8 @@
 // them exactly and check the output field against the oracle.
 //
 //   facade_demo <out.bin> <precision 0=FP64|1=FP32> <host sync 0=every step|1=lazy> [steps]
-// writes the field to out.bin and its gradient vectors to out.bin.grad
+// writes the field to out.bin, its gradient vectors to out.bin.grad and the
+// reference's MATLAB v4 snapshot to out.bin.mat
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -81,6 +82,7 @@ int main(int argc, char **argv) {
     for (int n = 0; n < M.number_of_voxels(); ++n)
         for (int d = 0; d < S; ++d) std::fwrite(M.gradient_vector(n)[d].data(), sizeof(double), 3, g);
     std::fclose(g);
+    M.write_to_matlab(std::string(argv[1]) + ".mat");
     std::printf("facade_demo: %d x %d x %d x %d, %d steps, checksum %.17g\n", M.mesh.x_size, M.mesh.y_size,
                 M.mesh.z_size, S, steps, M.checksum()[0]);
     return 0;

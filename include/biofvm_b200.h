@@ -218,6 +218,15 @@ BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double
 BFB_API int bfb_compute_gradients(bfb_env env, void *out_dev);
 BFB_API int bfb_get_gradients(bfb_env env, double *out_host);
 
+/* MATLAB v4 snapshot of the field, the file Microenvironment::write_to_matlab
+ * writes (BioFVM_microenvironment.cpp:1079-1107, BioFVM_matlab.cpp:535-584;
+ * BioFVM_parallel.cpp:528-678 at one rank): a (4 + S) x V double matrix named
+ * "multiscale_microenvironment", one column per voxel holding the voxel
+ * centre, its volume and its S densities. Packed on the device, copied to
+ * pinned host memory and written; returns when the file is closed. FP64 files
+ * are byte-identical to the reference's. */
+BFB_API int bfb_write_matlab(bfb_env env, const char *filename);
+
 /* Per-substrate FP64 sum of the field over all voxels (mass checksum). */
 BFB_API int bfb_checksum(bfb_env env, double *out);
 

@@ -211,6 +211,7 @@ class RefLib:
         L.ref_agent_voxels.argtypes = [ctypes.c_void_p, _ip]
         L.ref_cells_step.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.ref_gradients.argtypes = [ctypes.c_void_p, _dp]
+        L.ref_write_matlab.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.ref_gradients_per_voxel.argtypes = [ctypes.c_void_p, _dp]
 
 
@@ -286,6 +287,9 @@ class RefEnv:
 
     def cells_step(self, dt):
         self.ref.lib.ref_cells_step(self.h, dt)
+
+    def write_matlab(self, filename):
+        self.ref.lib.ref_write_matlab(self.h, str(filename).encode())
 
     def gradients(self, per_voxel=False):
         """(nx, ny, nz, S, 3) gradient vectors from compute_all_gradient_vectors,

@@ -222,6 +222,13 @@ void ref_agent_voxels(void *h, int *out) {
 }
 
 // Serial secretion/uptake in creation order (see the file header).
+// The serial MATLAB v4 writer, Microenvironment::write_to_matlab(filename)
+// (BioFVM_microenvironment.cpp:1079-1107).
+void ref_write_matlab(void *h, const char *filename) {
+    Microenvironment *M = (Microenvironment *)h;
+    M->write_to_matlab(std::string(filename));
+}
+
 // compute_all_gradient_vectors (BioFVM_microenvironment.cpp:1243-1402), then
 // the public accessor gradient_vector(n) per voxel: out[(n*S + q)*3 + c]. The
 // jumps it uses are set by the first solver call, so call ref_step first.

@@ -54,6 +54,11 @@ def test_facade_demo_matches_oracle(bfb, oracle, tmp_path, precision, sync):
     got = np.fromfile(out, dtype=np.float64).reshape(20, 18, 16, 2)
     want = oracle_demo(oracle, 10)
     grad = np.fromfile(str(out) + ".grad", dtype=np.float64).reshape(20, 18, 16, 2, 3)
+    raw = (tmp_path / "field.bin.mat").read_bytes()
+    hdr = np.frombuffer(raw[:20], dtype="<u4")
+    assert list(hdr) == [0, 6, 20 * 18 * 16, 0, 27] and raw[20:47] == b"multiscale_microenvironment"
+    mat = np.frombuffer(raw[47:], dtype="<f8").reshape(-1, 6)
+    assert np.array_equal(mat[:, 4:], got.reshape(-1, 2))  # the field the demo wrote, in voxel columns
     if precision == 0:
         assert np.array_equal(got, want)
         assert np.array_equal(grad, oracle.gradients(want, 20.0))
