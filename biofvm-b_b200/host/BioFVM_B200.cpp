@@ -421,16 +421,28 @@ void Microenvironment::simulate_bulk_sources_and_sinks(double dt) {
         bulk_uptake_rate_function == zero_function)
         return;
     const int S = number_of_densities(), V = number_of_voxels();
-    bulk_S_.assign((size_t)V * S, 0.0);
-    bulk_T_.assign((size_t)V * S, 0.0);
-    bulk_U_.assign((size_t)V * S, 0.0);
-    for (int n = 0; n < V; ++n) {
-        bulk_supply_rate_function(this, n, &bulk_S_[(size_t)n * S]);
-        bulk_supply_target_densities_function(this, n, &bulk_T_[(size_t)n * S]);
-        bulk_uptake_rate_function(this, n, &bulk_U_[(size_t)n * S]);
-    }
+    const bool same_fns = bulk_fns_used_[0] == bulk_supply_rate_function &&
+                          bulk_fns_used_[1] == bulk_supply_target_densities_function &&
+                          bulk_fns_used_[2] == bulk_uptake_rate_function;
+    const bool tabulate = bulk_tabulation_ == BulkTabulation::EveryCall || bulk_dirty || !same_fns;
     int st = upload_all_if_needed();
-    if (!st) st = bfb_set_bulk(env_, bulk_S_.data(), bulk_T_.data(), bulk_U_.data());
+    if (tabulate) {
+        bulk_S_.assign((size_t)V * S, 0.0);
+        bulk_T_.assign((size_t)V * S, 0.0);
+        bulk_U_.assign((size_t)V * S, 0.0);
+        for (int n = 0; n < V; ++n) {
+            bulk_supply_rate_function(this, n, &bulk_S_[(size_t)n * S]);
+            bulk_supply_target_densities_function(this, n, &bulk_T_[(size_t)n * S]);
+            bulk_uptake_rate_function(this, n, &bulk_U_[(size_t)n * S]);
+        }
+        if (!st) st = bfb_set_bulk(env_, bulk_S_.data(), bulk_T_.data(), bulk_U_.data());
+        if (!st) {
+            bulk_dirty = false;
+            bulk_fns_used_[0] = bulk_supply_rate_function;
+            bulk_fns_used_[1] = bulk_supply_target_densities_function;
+            bulk_fns_used_[2] = bulk_uptake_rate_function;
+        }
+    }
     if (!st) st = bfb_bulk_step(env_, dt);
     report(st, "simulate_bulk_sources_and_sinks");
     if (!st) after_device_step();

@@ -44,6 +44,11 @@ class Microenvironment;
 class Basic_Agent;
 
 enum class HostSync { EveryStep, Lazy };
+// When the bulk callbacks are evaluated: on every simulate_bulk_sources_and_sinks
+// call, as the reference does (BioFVM_microenvironment.cpp:1110-1153), or once
+// and then reused from device memory until the callbacks change or
+// mark_bulk_modified() is called (sources that do not vary in time).
+enum class BulkTabulation { EveryCall, Once };
 enum class Precision { FP64 = BFB_FP64, FP32 = BFB_FP32 };
 
 struct Voxel {
@@ -157,6 +162,8 @@ class Microenvironment {
     // ---- B200 additions
     void set_precision(Precision p);  // before the first step
     void set_host_sync(HostSync p) { host_sync = p; }
+    void set_bulk_tabulation(BulkTabulation p) { bulk_tabulation_ = p; }
+    void mark_bulk_modified() { bulk_dirty = true; }
     void sync_to_host();
     void sync_to_device();
     void mark_host_modified() { host_newer = true; }
@@ -184,6 +191,8 @@ class Microenvironment {
     bool device_newer = false;  // device copy changed since the last download
     bool params_dirty = true;   // D, lambda, Dirichlet need uploading
     bool bulk_dirty = true;
+    BulkTabulation bulk_tabulation_ = BulkTabulation::EveryCall;
+    void (*bulk_fns_used_[3])(Microenvironment *, int, double *) = {nullptr, nullptr, nullptr};
     std::vector<double> bulk_S_, bulk_T_, bulk_U_;
     const void *agents_uploaded_for_ = nullptr;
     size_t agents_uploaded_n_ = 0;

@@ -5,6 +5,7 @@
 // them exactly and check the output field against the oracle.
 //
 //   facade_demo <out.bin> <precision 0=FP64|1=FP32> <host sync 0=every step|1=lazy> [steps]
+//               [bulk 0=none|1=callbacks every call|2=callbacks tabulated once]
 // writes the field to out.bin, its gradient vectors to out.bin.grad and the
 // reference's MATLAB v4 snapshot to out.bin.mat
 #include <cmath>
@@ -25,12 +26,24 @@ static double hash01(unsigned a, unsigned b) {
     return (double)(h % 100003u) / 100003.0;
 }
 
+// time-invariant bulk source/sink callbacks (the reference's signature)
+static void supply_rate(Microenvironment *M, int n, double *out) {
+    for (int d = 0; d < M->number_of_densities(); ++d) out[d] = 2.0 * hash01(n, 50 + d);
+}
+static void supply_target(Microenvironment *M, int n, double *out) {
+    for (int d = 0; d < M->number_of_densities(); ++d) out[d] = 5.0 * hash01(n, 60 + d);
+}
+static void uptake_rate(Microenvironment *M, int n, double *out) {
+    for (int d = 0; d < M->number_of_densities(); ++d) out[d] = 0.5 * hash01(n, 70 + d);
+}
+
 int main(int argc, char **argv) {
     if (argc < 4) {
         std::printf("usage: %s <out.bin> <precision 0|1> <host sync 0|1> [steps]\n", argv[0]);
         return 2;
     }
     const int steps = argc > 4 ? std::atoi(argv[4]) : 10;
+    const int bulk = argc > 5 ? std::atoi(argv[5]) : 0;
     const double dt = 0.01;
     Microenvironment M;
     M.set_precision(std::atoi(argv[2]) ? Precision::FP32 : Precision::FP64);
@@ -65,7 +78,14 @@ int main(int argc, char **argv) {
         p->set_internal_uptake_constants(dt);
     }
 
+    if (bulk) {
+        M.bulk_supply_rate_function = supply_rate;
+        M.bulk_supply_target_densities_function = supply_target;
+        M.bulk_uptake_rate_function = uptake_rate;
+        M.set_bulk_tabulation(bulk == 2 ? BulkTabulation::Once : BulkTabulation::EveryCall);
+    }
     for (int s = 0; s < steps; ++s) {
+        if (bulk) M.simulate_bulk_sources_and_sinks(dt);
         M.simulate_diffusion_decay(dt, 1, 0, coords, dims, 0);
         M.simulate_cell_sources_and_sinks(dt);
         if (M.last_status() != BFB_OK) return 1;

@@ -20,7 +20,7 @@ def hash01(a, b):
     return (h % 100003) / 100003.0
 
 
-def oracle_demo(oracle, steps):
+def oracle_demo(oracle, steps, bulk=False):
     shape, S, dx, dt = (20, 18, 16), 2, 20.0, 0.01
     D, lam = [1e5, 3e3], [0.1, 0.01]
     V = shape[0] * shape[1] * shape[2]
@@ -37,7 +37,13 @@ def oracle_demo(oracle, steps):
     vox = oracle.bin_agents(pos, (0, 0, 0, 400, 360, 320), dx, shape)
     assert (vox >= 0).all()
     t1, t2 = oracle.agent_constants(dt, dx, vol, sec, upt, sat)
+    if bulk:
+        Sr = np.array([[2.0 * hash01(n, 50 + d) for d in range(S)] for n in range(V)]).reshape(*shape, S)
+        Tt = np.array([[5.0 * hash01(n, 60 + d) for d in range(S)] for n in range(V)]).reshape(*shape, S)
+        Ur = np.array([[0.5 * hash01(n, 70 + d) for d in range(S)] for n in range(V)]).reshape(*shape, S)
     for _ in range(steps):
+        if bulk:
+            rho = oracle.bulk_step(rho, dt, Sr, Tt, Ur)
         rho = oracle.lod_steps(rho, dt, dx, D, lam, 1, vals, face_mask_all([1, 0]))
         rho = oracle.cells_step(rho, vox, t1, t2)
     return rho
@@ -66,3 +72,15 @@ def test_facade_demo_matches_oracle(bfb, oracle, tmp_path, precision, sync):
         assert np.abs(got - want).max() / np.abs(want).max() <= 1e-5
         # gradients of the FP32 field itself, rounded once to FP32
         assert np.array_equal(grad, oracle.gradients(got, 20.0).astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("mode", [1, 2], ids=["callbacks_every_call", "callbacks_tabulated_once"])
+def test_facade_bulk_callbacks(bfb, oracle, tmp_path, mode):
+    """simulate_bulk_sources_and_sinks with the reference's callback signature,
+    evaluated every call (the reference's semantics) or tabulated once."""
+    demo = bfb.PKG / "lib" / "facade_demo"
+    out = tmp_path / "field.bin"
+    r = subprocess.run([str(demo), str(out), "0", "1", "6", str(mode)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = np.fromfile(out, dtype=np.float64).reshape(20, 18, 16, 2)
+    assert np.array_equal(got, oracle_demo(oracle, 6, bulk=True))
