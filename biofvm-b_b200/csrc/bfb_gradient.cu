@@ -14,9 +14,9 @@
 //
 // FP64: each value is the reference's `g = rho[a]; g -= rho[b]; g /= h`, the
 // division correctly rounded from r = RN(1/h) with one residual correction
-// (div_rcp), bit for bit with the IEEE quotient. FP32: the difference is
-// formed in FP64 from the two FP32 values and the quotient rounded once to
-// FP32.
+// (div_rcp), bit for bit with the IEEE quotient. FP32: the same operations
+// in FP32, h and 2h rounded once to FP32, the quotient by the binary32 form of
+// the same correction (bit for bit with IEEE FP32 division).
 //
 // One block per (i, j) row of nz*S contiguous elements; a thread takes
 // elements t, t + blockDim, ... of the row. The x and y neighbours are the
@@ -32,10 +32,19 @@ namespace bfb {
 __device__ __forceinline__ double grad_diff(double a, double b, double h, double rh) {
     return div_rcp(__dsub_rn(a, b), h, rh);
 }
+// binary32 version of div_rcp: the correctly rounded t/h from r = RN(1/h)
+// with one residual correction (Markstein), as IEEE division gives it
+__device__ __forceinline__ float grad_diff(float a, float b, float h, float rh) {
+    const float t = __fsub_rn(a, b);
+    const float q0 = __fmul_rn(t, rh);
+    const float e = __fmaf_rn(-q0, h, t);
+    return __fmaf_rn(e, rh, q0);
+}
 
-template <typename T>
+template <typename T, int SC>  // SC: the substrate count when a compile-time constant (else 0)
 __global__ void __launch_bounds__(256) gradient_kernel(const T *__restrict__ f, T *__restrict__ out, int nx, int ny,
-                                                       int nz, int S, double h1, double r1, double h2, double r2) {
+                                                       int nz, int S_, T h1, T r1, T h2, T r2) {
+    const int S = SC > 0 ? SC : S_;
     const long long row = blockIdx.x;  // i * ny + j
     const int i = (int)(row / ny), j = (int)(row - (long long)i * ny);
     const int L = nz * S;
@@ -45,26 +54,26 @@ __global__ void __launch_bounds__(256) gradient_kernel(const T *__restrict__ f, 
     T *__restrict__ o = out + base * 3;
     for (int t = threadIdx.x; t < L; t += blockDim.x) {
         const int k = t / S;
-        const double v = (double)fr[t];
-        double gx = 0.0, gy = 0.0, gz = 0.0;
+        const T v = fr[t];
+        T gx = T(0), gy = T(0), gz = T(0);
         if (nx > 1) {
-            if (i == 0) gx = grad_diff((double)fr[t + jx], v, h1, r1);
-            else if (i == nx - 1) gx = grad_diff(v, (double)fr[t - jx], h1, r1);
-            else gx = grad_diff((double)fr[t + jx], (double)fr[t - jx], h2, r2);
+            if (i == 0) gx = grad_diff(fr[t + jx], v, h1, r1);
+            else if (i == nx - 1) gx = grad_diff(v, fr[t - jx], h1, r1);
+            else gx = grad_diff(fr[t + jx], fr[t - jx], h2, r2);
         }
         if (ny > 1) {
-            if (j == 0) gy = grad_diff((double)fr[t + jy], v, h1, r1);
-            else if (j == ny - 1) gy = grad_diff(v, (double)fr[t - jy], h1, r1);
-            else gy = grad_diff((double)fr[t + jy], (double)fr[t - jy], h2, r2);
+            if (j == 0) gy = grad_diff(fr[t + jy], v, h1, r1);
+            else if (j == ny - 1) gy = grad_diff(v, fr[t - jy], h1, r1);
+            else gy = grad_diff(fr[t + jy], fr[t - jy], h2, r2);
         }
         if (nz > 1) {
-            if (k == 0) gz = grad_diff((double)fr[t + S], v, h1, r1);
-            else if (k == nz - 1) gz = grad_diff(v, (double)fr[t - S], h1, r1);
-            else gz = grad_diff((double)fr[t + S], (double)fr[t - S], h2, r2);
+            if (k == 0) gz = grad_diff(fr[t + S], v, h1, r1);
+            else if (k == nz - 1) gz = grad_diff(v, fr[t - S], h1, r1);
+            else gz = grad_diff(fr[t + S], fr[t - S], h2, r2);
         }
-        o[3 * (size_t)t] = (T)gx;
-        o[3 * (size_t)t + 1] = (T)gy;
-        o[3 * (size_t)t + 2] = (T)gz;
+        o[3 * (size_t)t] = gx;
+        o[3 * (size_t)t + 1] = gy;
+        o[3 * (size_t)t + 2] = gz;
     }
 }
 
@@ -74,23 +83,32 @@ using namespace bfb;
 
 namespace {
 
-int launch_gradients(bfb_env_s *env, void *out) {
-    // h = dx; 2h = dx * 2.0 exactly as the reference forms two_dx (:1245-1255)
-    const double h1 = env->dx, h2 = env->dx * 2.0;
-    const double r1 = 1.0 / h1, r2 = 1.0 / h2;
+template <typename T>
+int launch_typed(bfb_env_s *env, void *out, T h1, T r1, T h2, T r2) {
     const unsigned rows = (unsigned)((long long)env->nx * env->ny);
     const int L = env->nz * env->S;
     const int threads = L >= 256 ? 256 : ((L + 31) / 32) * 32;
-    if (env->precision == BFB_FP64)
-        gradient_kernel<double><<<rows, threads, 0, env->stream>>>(static_cast<const double *>(env->field),
-                                                                   static_cast<double *>(out), env->nx, env->ny,
-                                                                   env->nz, env->S, h1, r1, h2, r2);
-    else
-        gradient_kernel<float><<<rows, threads, 0, env->stream>>>(static_cast<const float *>(env->field),
-                                                                  static_cast<float *>(out), env->nx, env->ny, env->nz,
-                                                                  env->S, h1, r1, h2, r2);
+    const T *f = static_cast<const T *>(env->field);
+    T *o = static_cast<T *>(out);
+    cudaStream_t s = env->stream;
+    const int nx = env->nx, ny = env->ny, nz = env->nz, S = env->S;
+    switch (S) {
+    case 1: gradient_kernel<T, 1><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
+    case 2: gradient_kernel<T, 2><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
+    case 4: gradient_kernel<T, 4><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
+    case 8: gradient_kernel<T, 8><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
+    default: gradient_kernel<T, 0><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
+    }
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
+}
+
+int launch_gradients(bfb_env_s *env, void *out) {
+    // h = dx; 2h = dx * 2.0 exactly as the reference forms two_dx (:1245-1255)
+    const double h1 = env->dx, h2 = env->dx * 2.0;
+    if (env->precision == BFB_FP64) return launch_typed<double>(env, out, h1, 1.0 / h1, h2, 1.0 / h2);
+    const float f1 = (float)h1, f2 = (float)h2;
+    return launch_typed<float>(env, out, f1, 1.0f / f1, f2, 1.0f / f2);
 }
 
 }  // namespace

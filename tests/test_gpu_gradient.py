@@ -35,12 +35,32 @@ def test_gradients_fp64_bitexact(bfb, oracle, shape, S):
     env.close()
 
 
-@pytest.mark.parametrize("shape,S", [((5, 4, 6), 2), ((33, 17, 40), 5), ((64, 48, 80), 8)])
-def test_gradients_fp32_is_the_fp32_field_gradient_rounded_once(bfb, oracle, shape, S):
+def fp32_gradients(f, dx):
+    """The reference's arithmetic in IEEE FP32 (numpy float32 operations)."""
+    f = np.asarray(f, np.float32)
+    h1, h2 = np.float32(dx), np.float32(dx * 2.0)
+    out = np.zeros((*f.shape, 3), np.float32)
+    for c in range(3):
+        n = f.shape[c]
+        if n == 1:
+            continue
+        a = np.moveaxis(f, c, 0)
+        g = np.empty_like(a)
+        g[0] = (a[1] - a[0]) / h1
+        g[-1] = (a[-1] - a[-2]) / h1
+        if n > 2:
+            g[1:-1] = (a[2:] - a[:-2]) / h2
+        out[..., c] = np.moveaxis(g, 0, c)
+    return out
+
+
+@pytest.mark.parametrize("shape,S", [((5, 4, 6), 2), ((33, 17, 40), 5), ((64, 48, 80), 8), ((2, 1, 3), 1)])
+def test_gradients_fp32_bitexact_with_fp32_arithmetic(bfb, shape, S):
+    """FP32 envs compute in FP32; checked bit for bit against numpy float32."""
     rng = np.random.default_rng(3 + S)
     env = _env(bfb, shape, S, bfb.FP32, rng)
-    field = env.get_field_raw().astype(np.float64)
-    want = oracle.gradients(field, 20.0).astype(np.float32)
+    field = env.get_field_raw()
+    want = fp32_gradients(field, 20.0)
     dev = torch.empty(3 * field.size, dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
     env.compute_gradients_device(dev.data_ptr())
