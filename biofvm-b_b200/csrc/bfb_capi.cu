@@ -132,11 +132,20 @@ static int upload_factors(bfb_env_s *env, int axis, int n, const std::vector<dou
             flat.insert(flat.end(), nS, 0.0);
         }
     }
+    // the head rows [0, m0) again, [table][substrate][row], rows padded to hpad
+    const int hpad = (m0 + 3) / 4 * 4;
+    std::vector<double> head(4 * (size_t)S * hpad, 0.0);
+    for (size_t k = 0; k < tabs.size(); ++k)
+        for (int d = 0; d < S; ++d)
+            for (int m = 0; m < std::min(hpad, n); ++m) head[(k * S + d) * hpad + m] = tabs[k][(size_t)m * S + d];
     int st = upload_table(env, env->fac_tab[axis], flat);
     if (st) return st;
     st = upload_table(env, env->fac_tail[axis], tail);
     if (st) return st;
+    st = upload_table(env, env->fac_head[axis], head);
+    if (st) return st;
     env->fac_m0[axis] = m0;
+    env->fac_hpad[axis] = hpad;
     return BFB_OK;
 }
 
@@ -186,7 +195,9 @@ static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
     a.fac.t2 = tab + 2 * nS;
     a.fac.t3 = tab + 3 * nS;
     a.fac.tail = static_cast<const T *>(env->fac_tail[axis]);
+    a.fac.head = static_cast<const T *>(env->fac_head[axis]);
     a.fac.m0 = env->fac_m0[axis];
+    a.fac.hpad = env->fac_hpad[axis];
     a.c1 = static_cast<const T *>(env->c1);
     a.g = static_cast<const T *>(env->g);
     for (int f = 0; f < 6; ++f) a.dir.face[f] = static_cast<const T *>(env->faces[f]);
@@ -387,6 +398,7 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
     for (int a = 0; a < 3; ++a) {
         alloc(&env->fac_tab[a], env->elem * 4 * (size_t)ns[a] * n_substrates);
         alloc(&env->fac_tail[a], env->elem * 4 * (size_t)n_substrates);
+        alloc(&env->fac_head[a], env->elem * 4 * (size_t)n_substrates * ((ns[a] + 3) / 4 * 4));
     }
     alloc(&env->c1, env->elem * n_substrates);
     alloc(&env->g, env->elem * 2 * n_substrates);
@@ -446,6 +458,7 @@ BFB_API int bfb_destroy(bfb_env env) {
     for (int a = 0; a < 3; ++a) {
         cudaFree(env->fac_tab[a]);
         cudaFree(env->fac_tail[a]);
+        cudaFree(env->fac_head[a]);
     }
     cudaFree(env->c1);
     cudaFree(env->g);

@@ -88,6 +88,8 @@ struct bfb_env_s {
     // 1/den lo, c1/den, c) and tail values [4][S] for rows [m0, n-2]
     void *fac_tab[3] = {nullptr, nullptr, nullptr};
     void *fac_tail[3] = {nullptr, nullptr, nullptr};
+    void *fac_head[3] = {nullptr, nullptr, nullptr};
+    int fac_hpad[3] = {4, 4, 4};
     int fac_m0[3] = {1, 1, 1};
     void *c1 = nullptr;                  // [S] (FP64)
     void *g = nullptr;                   // [2*S] (FP32): 1/(1 + c2) as hi, lo

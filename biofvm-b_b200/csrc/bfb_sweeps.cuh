@@ -57,11 +57,15 @@ constexpr int kChunks = 4;  // default row groups per tile (async copy / TMA sta
 //   FP64: t0 = den, t1 = c (back-substitution coefficient), t2 = RN(1/den)
 //   FP32: t0 = 1/den (hi), t1 = 1/den (lo), t2 = c1/den, t3 = c
 // tail[q*S + d] = value of table q on rows [m0, n-2] (valid when m0 <= n-2).
+// head[(q*S + d)*hpad + m] = table q, substrate d, row m < hpad: the rows
+// below m0 again, one substrate's rows contiguous (hpad a multiple of 4), so
+// that a lane reads four rows of a table with one 16-byte load.
 template <typename T>
 struct Factors {
     const T *t0, *t1, *t2, *t3;
     const T *tail;
-    int m0;
+    const T *head;
+    int m0, hpad;
 };
 
 template <typename T>

@@ -25,7 +25,7 @@ namespace bfb {
 // Strided sweep with TMA (rank 2: x, rank 3: y).
 // ---------------------------------------------------------------------------
 template <typename T, bool FUSE_PRE, bool BULK>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 1)
     sweep_strided_tma_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap map_out,
                              SweepArgs<T> a, StridedGeom g, int crow) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128)
 // Contiguous z sweep with 1-D bulk copies.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(128) sweep_contig_tma_kernel(SweepArgs<T> a, ContigGeom g) {
+__global__ void __launch_bounds__(128, 1) sweep_contig_tma_kernel(SweepArgs<T> a, ContigGeom g) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(128) sweep_contig_tma_kernel(SweepArgs<T> a, C
 // (S <= 32 gives R = 32/S rows per warp).
 // ---------------------------------------------------------------------------
 template <typename T, int SC>
-__global__ void __launch_bounds__(128) sweep_contig_pipe_kernel(SweepArgs<T> a, ContigGeom g, int kc) {
+__global__ void __launch_bounds__(128, 1) sweep_contig_pipe_kernel(SweepArgs<T> a, ContigGeom g, int kc) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;

@@ -106,9 +106,8 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
         if (ch > ref_ch && !wait_group(ch)) return false;
         const int rend = min(n - 1, (ch + 1) * crow);
         const int hend = min(rend, m0);
-        for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(load(r), r);
-#pragma unroll 8
-        for (; r < rend; ++r) sm[r * 32 + lane] = L.template fwd<true>(load(r), r);
+        r = head_forward(L, r, hend, load, [&](int q, T v) { sm[q * 32 + lane] = v; });
+        r = tail_forward(L, r, rend, load, [&](int q, T v) { sm[q * 32 + lane] = v; });
     }
     if (n > 1) {
         T x = load(n - 1);
@@ -127,10 +126,11 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
     for (int ch = nch - 1; ch >= 0; --ch) {
         const int rlo = ch * crow;
         const int tstop = max(rlo, tl);
-#pragma unroll 8
-        for (; r >= tstop; --r) sm[r * 32 + lane] = L.template bwd<true>(sm[r * 32 + lane], r);
+        r = tail_backward(L, r, tstop, [&](int q) { return sm[q * 32 + lane]; },
+                          [&](int q, T v) { sm[q * 32 + lane] = v; });
         const int hstop = max(rlo, 1);
-        for (; r >= hstop; --r) sm[r * 32 + lane] = L.template bwd<false>(sm[r * 32 + lane], r);
+        r = head_backward(L, r, hstop, [&](int q) { return sm[q * 32 + lane]; },
+                          [&](int q, T v) { sm[q * 32 + lane] = v; });
         if (rlo == 0 && n > 1) {
             T y = L.template bwd<false>(sm[lane], 0);
             if (lo_dir) y = vox_dir(0);
@@ -210,9 +210,8 @@ __device__ __forceinline__ bool contig_pipe_tile(const SweepArgs<T> &a, const Co
         const int kend = min(nz - 1, (c + 1) * kc);
         if (active) {
             const int hend = min(kend, m0);
-            for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(line[k * S], k);
-#pragma unroll 8
-            for (; k < kend; ++k) line[k * S] = Ls.template fwd<true>(line[k * S], k);
+            k = head_forward(Ls, k, hend, [&](int q) { return line[q * S]; }, [&](int q, T v) { line[q * S] = v; });
+            k = tail_forward(Ls, k, kend, [&](int q) { return line[q * S]; }, [&](int q, T v) { line[q * S] = v; });
         }
         k = max(k, kend);
     }
@@ -229,10 +228,9 @@ __device__ __forceinline__ bool contig_pipe_tile(const SweepArgs<T> &a, const Co
         const int klo = c * kc;
         if (active) {
             const int tstop = max(klo, tl);
-#pragma unroll 8
-            for (; k >= tstop; --k) line[k * S] = Ls.template bwd<true>(line[k * S], k);
+            k = tail_backward(Ls, k, tstop, [&](int q) { return line[q * S]; }, [&](int q, T v) { line[q * S] = v; });
             const int hstop = max(klo, 1);
-            for (; k >= hstop; --k) line[k * S] = Ls.template bwd<false>(line[k * S], k);
+            k = head_backward(Ls, k, hstop, [&](int q) { return line[q * S]; }, [&](int q, T v) { line[q * S] = v; });
             if (klo == 0 && nz > 1) {
                 const T y = Ls.template bwd<false>(line[0], 0);
                 line[0] = lo_dir ? dir_value(a.dir, i, j, 0, d) : y;
