@@ -139,7 +139,7 @@ __device__ __forceinline__ void dots_at(int m, int n, double mu, YV yv, double &
 // ones are computed). The sums over mu and y are left to adjoint_dots_kernel.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 1)
     adjoint_solve_strided_tma_kernel(const __grid_constant__ CUtensorMap map_l,
                                      const __grid_constant__ CUtensorMap map_mu, SweepArgs<T> a, StridedGeom g,
                                      int crow) {
@@ -225,9 +225,9 @@ __global__ void __launch_bounds__(128)
         if (ch > ref_ch && !wait_group(ch)) return;
         const int rend = min(n - 1, (ch + 1) * crow);
         const int hend = min(rend, m0);
-        for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(xin(r), r);
-#pragma unroll 8
-        for (; r < rend; ++r) sm[r * 32 + lane] = L.template fwd<true>(xin(r), r);
+        auto st = [&](int q, T v) { sm[q * 32 + lane] = v; };
+        r = head_forward(L, r, hend, xin, st);
+        r = tail_forward(L, r, rend, xin, st);
     }
     if (n > 1) L.template fwd<false>(xend(n - 1), n - 1);
 
@@ -238,10 +238,10 @@ __global__ void __launch_bounds__(128)
     for (int ch = nch - 1; ch >= 0; --ch) {
         const int rlo = ch * crow;
         const int tstop = max(rlo, tl);
-#pragma unroll 8
-        for (; r >= tstop; --r) sm[r * 32 + lane] = L.template bwd<true>(sm[r * 32 + lane], r);
-        const int hstop = max(rlo, 1);
-        for (; r >= hstop; --r) sm[r * 32 + lane] = L.template bwd<false>(sm[r * 32 + lane], r);
+        auto ld = [&](int q) { return sm[q * 32 + lane]; };
+        auto st = [&](int q, T v) { sm[q * 32 + lane] = v; };
+        r = tail_backward(L, r, tstop, ld, st);
+        r = head_backward(L, r, max(rlo, 1), ld, st);
         if (rlo == 0 && n > 1) sm[lane] = L.template bwd<false>(sm[lane], 0);
         fence_async_smem();
         __syncwarp();
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(32) adjoint_strided_kernel(SweepArgs<T> a, con
 // compile-time constant.
 // ---------------------------------------------------------------------------
 template <typename T, int SC>
-__global__ void __launch_bounds__(128) adjoint_solve_contig_pipe_kernel(SweepArgs<T> a, ContigGeom g, int kc) {
+__global__ void __launch_bounds__(128, 1) adjoint_solve_contig_pipe_kernel(SweepArgs<T> a, ContigGeom g, int kc) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -431,9 +431,9 @@ __global__ void __launch_bounds__(128) adjoint_solve_contig_pipe_kernel(SweepArg
         const int kend = min(nz - 1, (c + 1) * kc);
         if (active) {
             const int hend = min(kend, m0);
-            for (; k < hend; ++k) line[k * S] = Ls.template fwd<false>(xin(k), k);
-#pragma unroll 8
-            for (; k < kend; ++k) line[k * S] = Ls.template fwd<true>(xin(k), k);
+            auto st = [&](int q, T v) { line[q * S] = v; };
+            k = head_forward(Ls, k, hend, xin, st);
+            k = tail_forward(Ls, k, kend, xin, st);
         }
         k = max(k, kend);
     }
@@ -446,10 +446,10 @@ __global__ void __launch_bounds__(128) adjoint_solve_contig_pipe_kernel(SweepArg
         const int klo = c * kc;
         if (active) {
             const int tstop = max(klo, tl);
-#pragma unroll 8
-            for (; k >= tstop; --k) line[k * S] = Ls.template bwd<true>(line[k * S], k);
-            const int hstop = max(klo, 1);
-            for (; k >= hstop; --k) line[k * S] = Ls.template bwd<false>(line[k * S], k);
+            auto ld = [&](int q) { return line[q * S]; };
+            auto st = [&](int q, T v) { line[q * S] = v; };
+            k = tail_backward(Ls, k, tstop, ld, st);
+            k = head_backward(Ls, k, max(klo, 1), ld, st);
             if (klo == 0 && nz > 1) line[0] = Ls.template bwd<false>(line[0], 0);
         }
         k = min(k, klo - 1);
@@ -485,10 +485,16 @@ __device__ __forceinline__ void load_vec(const T *p, double (&o)[VEC]) {
     if constexpr (VEC == 1) {
         o[0] = (double)p[0];
     } else {
-        static_assert(VEC == 2, "FP64 rows are read 2 at a time");
-        const double2 v = *reinterpret_cast<const double2 *>(p);
-        o[0] = v.x;
-        o[1] = v.y;
+        if constexpr (sizeof(T) == 8) {
+            static_assert(VEC == 2, "FP64 rows are read 2 at a time");
+            const double2 v = *reinterpret_cast<const double2 *>(p);
+            o[0] = v.x;
+            o[1] = v.y;
+        } else {
+            static_assert(VEC == 4, "FP32 rows are read 4 at a time");
+            const float4 v = *reinterpret_cast<const float4 *>(p);
+            o[0] = v.x, o[1] = v.y, o[2] = v.z, o[3] = v.w;
+        }
     }
 }
 
@@ -920,10 +926,11 @@ struct Adjoint {
     }
 
     // the sums of one sweep over the stored y and the new mu
-    // lines per thread (16-byte loads) and rows per thread in the sums kernel;
-    // FP32 runs fastest with 4-byte loads and 64-row segments (measured)
-    static constexpr int kVec = sizeof(T) == 8 ? 2 : 1;
-    static constexpr int kDotSeg = 64 / kVec;
+    // lines per thread (16-byte loads) and rows per thread in the sums kernel
+    // (measured at 256^3 x 8 FP32: 4 lines x 64 rows beats 1 x 64, 4 x 16 and
+    // 4 x 32, and ties with 4 x 128)
+    static constexpr int kVec = sizeof(T) == 8 ? 2 : 4;
+    static constexpr int kDotSeg = sizeof(T) == 8 ? 32 : 64;
     int dots_threads() const {
         int threads = S;
         while (threads * 2 <= 256) threads *= 2;
