@@ -34,6 +34,9 @@ OPT_USE_GRAPHS = 2
 OPT_USE_TMA = 3
 BATCH_OPT_WARPS_PER_CTA = 1
 BATCH_OPT_TILES_PER_ITEM = 2
+BATCH_OPT_MODE = 3
+BATCH_MODE_PERSISTENT = 0
+BATCH_MODE_STAGED = 1
 
 ERRORS = {
     -1: "BFB_ERR_INVALID_ARG",
@@ -53,7 +56,7 @@ EXPORTS = [
     "bfb_compare_fields", "bfb_field_device_ptr", "bfb_set_dirichlet",
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
-    "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_write_matlab", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_simulate",
+    "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_write_matlab", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_get_option", "bfb_batch_simulate",
     "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_batch_autotune", "bfb_adjoint_run",
     "bfb_checksum_noalloc",
 ]
@@ -123,6 +126,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_batch_create": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)],
         "bfb_batch_destroy": [_vp],
         "bfb_batch_set_option": [_vp, ctypes.c_int, ctypes.c_int],
+        "bfb_batch_get_option": [_vp, ctypes.c_int, _ip],
         "bfb_batch_simulate": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_simulate_loop": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_synchronize": [_vp],
@@ -375,7 +379,9 @@ class Env:
 
 
 class Batch:
-    """Many envs stepped by one persistent launch per step (a ``bfb_batch``)."""
+    """Many envs stepped together (a ``bfb_batch``): one launch per stage over
+    every env's tiles (``BATCH_MODE_STAGED``, the default) or one persistent
+    launch per step (``BATCH_MODE_PERSISTENT``)."""
 
     def __init__(self, envs):
         self.L = load_library()
@@ -402,8 +408,21 @@ class Batch:
     def set_tiles_per_item(self, t):
         _check(self.L.bfb_batch_set_option(self.h, BATCH_OPT_TILES_PER_ITEM, t))
 
+    def set_mode(self, m):
+        _check(self.L.bfb_batch_set_option(self.h, BATCH_OPT_MODE, m))
+
+    def get_option(self, option):
+        v = ctypes.c_int()
+        _check(self.L.bfb_batch_get_option(self.h, option, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def mode(self):
+        return self.get_option(BATCH_OPT_MODE)
+
     def autotune(self, dt, flags=STEP_DIFFUSION, trials=3):
-        """Picks warps per CTA and tiles per item; returns ((warps, tiles), ms per step)."""
+        """Picks the mode, warps per CTA and tiles per item; returns ((warps, tiles), ms per step).
+        The chosen mode is ``self.mode`` afterwards."""
         v = (ctypes.c_int * 2)()
         ms = ctypes.c_double()
         _check(self.L.bfb_batch_autotune(self.h, dt, flags, trials, v, ctypes.byref(ms)))

@@ -224,8 +224,8 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
                     if (I.vb16[1]) strided_tile<T, 16, false, false>(I.ax[1], I.gy, tile, sm);
                     else strided_tile<T, (int)sizeof(T), false, false>(I.ax[1], I.gy, tile, sm);
                 } else {
-                    if (I.vb16[2]) contig_tile<T, 16>(I.ax[2], I.gz, tile, sm);
-                    else contig_tile<T, (int)sizeof(T)>(I.ax[2], I.gz, tile, sm);
+                    if (I.vb16[2]) contig_tile_any<T, 16>(I.ax[2], I.gz, tile, sm);
+                    else contig_tile_any<T, (int)sizeof(T)>(I.ax[2], I.gz, tile, sm);
                 }
                 __syncwarp();  // the tile's shared memory is reused by the next tile
             }
@@ -239,6 +239,73 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
         groups = 0;
     }
     publish();
+}
+
+// One stage of a class of envs of a batch as one launch (the staged mode).
+// The stage's envs are listed in `perm` by tile path and by the shared memory
+// their tiles need, and tpre[j] counts the stage's tiles (agent chunks for
+// STAGE 3) of the listed envs before j. A launch covers the envs
+// perm[lo .. hi): one tile path (PATH: kPathTma, kPathCp16 or kPathCpElem,
+// compiled alone so that the kernel needs no more registers than that path)
+// and similar tile sizes (so that its shared memory per warp fits them
+// without waste). Warp g of its grid runs tile tpre[lo] + g - tpre[j] of env
+// perm[j], where tpre[j] <= tpre[lo] + g < tpre[j + 1], with that env's own
+// tile code, as bfb_simulate's kernels do; the stages follow one another in
+// stream order, so no warp waits for another.
+constexpr int kPathTma = 0, kPathCp16 = 1, kPathCpElem = 2;
+template <typename T, int STAGE, int PATH>
+__global__ void __launch_bounds__(128, 1)
+    batch_stage_kernel(const BatchInst<T> *__restrict__ inst, const int *__restrict__ perm,
+                       const int *__restrict__ tpre, int lo, int hi, int warp_bytes) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int gt = __ldg(tpre + lo) + blockIdx.x * (blockDim.x >> 5) + warp;
+    if (gt >= __ldg(tpre + hi)) return;
+    while (hi - lo > 1) {  // j with tpre[j] <= gt < tpre[j + 1]
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(tpre + mid) <= gt) lo = mid; else hi = mid;
+    }
+    const BatchInst<T> &I = inst[__ldg(perm + lo)];
+    const int tile = gt - __ldg(tpre + lo);
+    if constexpr (STAGE == 3) {
+        cells_chunk(I, tile);
+    } else {
+        unsigned char *wbase = smem_raw + (size_t)warp * warp_bytes;
+        T *sm = reinterpret_cast<T *>(wbase + 128);
+        const SweepArgs<T> ax = I.ax[STAGE];
+        if constexpr (PATH == kPathTma) {
+            const int nch = STAGE < 2 ? ((STAGE == 0 ? I.gx.n : I.gy.n) + I.crow[STAGE] - 1) / I.crow[STAGE]
+                                      : (I.gz.nz + I.kc - 1) / I.kc;
+            if (lane == 0) {
+                for (int c = 0; c < nch; ++c) mbar_init(smem_u32(wbase) + 8 * c, 1);
+                fence_mbar_init();
+            }
+            __syncwarp();
+            if constexpr (STAGE < 2) {
+                const StridedGeom g = STAGE == 0 ? I.gx : I.gy;
+                const CUtensorMap *mp = I.map[STAGE];
+                strided_tma_tile<T, STAGE == 0, false>(mp, mp, ax, g, I.crow[STAGE], tile, wbase, 0u);
+            } else {
+                const ContigGeom gz = I.gz;
+                switch (I.S) {  // the substrate count as a constant where it is a common one
+                case 1: contig_pipe_tile<T, 1>(ax, gz, I.kc, tile, wbase, 0u); break;
+                case 2: contig_pipe_tile<T, 2>(ax, gz, I.kc, tile, wbase, 0u); break;
+                case 4: contig_pipe_tile<T, 4>(ax, gz, I.kc, tile, wbase, 0u); break;
+                case 8: contig_pipe_tile<T, 8>(ax, gz, I.kc, tile, wbase, 0u); break;
+                default: contig_pipe_tile<T, 0>(ax, gz, I.kc, tile, wbase, 0u); break;
+                }
+            }
+        } else {
+            constexpr int VB = PATH == kPathCp16 ? 16 : (int)sizeof(T);
+            if constexpr (STAGE < 2) {
+                const StridedGeom g = STAGE == 0 ? I.gx : I.gy;
+                strided_tile<T, VB, STAGE == 0, false>(ax, g, tile, sm);
+            } else {
+                contig_tile_any<T, VB>(ax, I.gz, tile, sm);
+            }
+        }
+    }
 }
 
 }  // namespace bfb
@@ -258,7 +325,24 @@ struct bfb_batch_s {
     int warp_bytes = 0;
     int warps = 1;
     int tiles_per_item = 2;
+    int mode = BFB_BATCH_MODE_STAGED;
     int grid[5] = {0, 0, 0, 0, 0};  // resident CTAs for warps = 1..4
+    // staged mode, per stage s: envs listed by tile size (d_perm[s]), tiles before
+    // list entry j (d_tpre[s][j]), and classes of list entries [lo, hi) launched
+    // together with `bytes` of shared memory per warp
+    int *d_tpre = nullptr;  // [4][n+1]
+    int *d_perm = nullptr;  // [4][n]
+    struct StageClass {
+        int lo, hi, bytes, total, path, group;
+    };
+    std::vector<StageClass> classes[4];
+    // the env groups run side by side on these streams, each its own chain of
+    // stage launches (forked from and joined to the batch stream inside the
+    // captured graph)
+    static constexpr int kSide = 8;
+    int n_groups = 1;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kSide] = {};
     cudaGraphExec_t graph = nullptr;
     int graph_flags = -1;
     double graph_dt = 0;
@@ -279,7 +363,9 @@ template <typename T>
 static int batch_upload(bfb_batch_s *b, double dt) {
     std::vector<BatchInst<T>> inst(b->n);
     std::vector<CUtensorMap> maps(2 * (size_t)b->n);
-    std::vector<int> prefix(4 * (size_t)(b->n + 1), 0);
+    std::vector<int> prefix(4 * (size_t)(b->n + 1), 0), tpre(4 * (size_t)(b->n + 1), 0), perm(4 * (size_t)b->n);
+    std::vector<size_t> ebytes(3 * (size_t)b->n, 0);  // shared memory of env k's tile in stage s
+    std::vector<int> epath(3 * (size_t)b->n, 0);      // tile path of env k in stage s
     const int eb = (int)sizeof(T);
     size_t tile_bytes = 0;
     const CUtensorMap *dmaps = static_cast<const CUtensorMap *>(b->d_maps);
@@ -302,8 +388,9 @@ static int batch_upload(bfb_batch_s *b, double dt) {
             I.crow[a] = e->tma_crow[a];
             maps[2 * (size_t)k + a] = e->tmap[a];
             I.map[a] = dmaps + 2 * (size_t)k + a;
-            tile_bytes = std::max(tile_bytes, I.tma[a] ? strided_tma_warp_bytes(g.n, I.crow[a], eb) - 128
-                                                       : (size_t)g.n * 32 * eb);
+            const size_t tb = I.tma[a] ? strided_tma_warp_bytes(g.n, I.crow[a], eb) - 128 : (size_t)g.n * 32 * eb;
+            tile_bytes = std::max(tile_bytes, tb);
+            ebytes[(size_t)a * b->n + k] = tb;
         }
         {
             const long long L = (long long)e->nz * e->S;
@@ -317,6 +404,7 @@ static int batch_upload(bfb_batch_s *b, double dt) {
             I.kc = (kc + q - 1) / q * q;
             if ((e->nz + I.kc - 1) / I.kc > 16) I.tma[2] = 0;  // one mbarrier per row group
             tile_bytes = std::max(tile_bytes, (size_t)I.gz.R * I.gz.RS * eb);
+            ebytes[2 * (size_t)b->n + k] = (size_t)I.gz.R * I.gz.RS * eb;
         }
         I.f = static_cast<T *>(e->field);
         I.S = e->S;
@@ -326,6 +414,65 @@ static int batch_upload(bfb_batch_s *b, double dt) {
         I.t1 = static_cast<const T *>(e->ag_t1);
         I.t2 = static_cast<const T *>(e->ag_t2);
         for (int s = 0; s < 4; ++s) prefix[(size_t)s * (b->n + 1) + k + 1] = prefix[(size_t)s * (b->n + 1) + k] + I.items[s];
+    }
+    // staged mode: envs in up to kSide groups of about equal work (largest
+    // first, each to the least loaded group); per stage, each group's envs by
+    // tile path, then by decreasing tile size, cut into classes of one path
+    // whose smallest tile needs more than half the class's largest (at most 4
+    // classes per group and path)
+    auto warp_of = [](size_t bytes) { return (int)((128 + bytes + 127) / 128 * 128); };
+    std::vector<int> group(b->n, 0);
+    {
+        b->n_groups = std::min(b->n, (int)bfb_batch_s::kSide);
+        std::vector<int> order(b->n);
+        for (int k = 0; k < b->n; ++k) order[k] = k;
+        auto work = [&](int k) { return (double)b->envs[k]->N; };
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) > work(y); });
+        std::vector<double> load(b->n_groups, 0.0);
+        for (int k : order) {
+            const int gsel = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            group[k] = gsel;
+            load[gsel] += work(k);
+        }
+    }
+    for (int k = 0; k < b->n; ++k)
+        for (int s = 0; s < 3; ++s) {
+            const BatchInst<T> &I = inst[k];
+            epath[(size_t)s * b->n + k] = I.tma[s] ? kPathTma : (I.vb16[s] ? kPathCp16 : kPathCpElem);
+        }
+    for (int s = 0; s < 4; ++s) {
+        int *ps = perm.data() + (size_t)s * b->n;
+        for (int k = 0; k < b->n; ++k) ps[k] = k;
+        const size_t *bs = s < 3 ? ebytes.data() + (size_t)s * b->n : nullptr;
+        const int *pa = s < 3 ? epath.data() + (size_t)s * b->n : nullptr;
+        std::stable_sort(ps, ps + b->n, [&](int x, int y) {
+            if (group[x] != group[y]) return group[x] < group[y];
+            if (!bs) return false;
+            return pa[x] != pa[y] ? pa[x] < pa[y] : bs[x] > bs[y];
+        });
+        int *ts = tpre.data() + (size_t)s * (b->n + 1);
+        for (int j = 0; j < b->n; ++j) {
+            const BatchInst<T> &I = inst[ps[j]];
+            ts[j + 1] = ts[j] + (s < 3 ? I.tiles[s] : I.items[3]);
+        }
+        b->classes[s].clear();
+        for (int j = 0; j < b->n;) {
+            const int path = pa ? pa[ps[j]] : kPathTma, grp = group[ps[j]];
+            int end = j + 1;  // the group's envs of this path are [j, end)
+            while (end < b->n && group[ps[end]] == grp && (!pa || pa[ps[end]] == path)) ++end;
+            for (int cls = 0; j < end; ++cls) {
+                int hi = j + 1;
+                if (bs) {
+                    while (hi < end && 2 * bs[ps[hi]] > bs[ps[j]]) ++hi;
+                    if (cls == 3) hi = end;  // at most 4 classes per path
+                } else {
+                    hi = end;
+                }
+                const int total = ts[hi] - ts[j];
+                if (total > 0) b->classes[s].push_back({j, hi, bs ? warp_of(bs[ps[j]]) : 0, total, path, grp});
+                j = hi;
+            }
+        }
     }
     const size_t warp_bytes = (128 + tile_bytes + 127) / 128 * 128;
     if (warp_bytes > (size_t)kMaxSmem) return fail(BFB_ERR_UNSUPPORTED, "batch: an env's tile does not fit in shared memory");
@@ -340,7 +487,16 @@ static int batch_upload(bfb_batch_s *b, double dt) {
     BFB_CUDA(cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice));
     BFB_CUDA(cudaMemcpy(b->d_inst, inst.data(), sizeof(BatchInst<T>) * b->n, cudaMemcpyHostToDevice));
     BFB_CUDA(cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice));
+    BFB_CUDA(cudaMemcpy(b->d_tpre, tpre.data(), sizeof(int) * tpre.size(), cudaMemcpyHostToDevice));
+    BFB_CUDA(cudaMemcpy(b->d_perm, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice));
     BFB_CUDA(cudaFuncSetAttribute(batch_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    for (const void *k :
+         {(const void *)batch_stage_kernel<T, 0, kPathTma>, (const void *)batch_stage_kernel<T, 0, kPathCp16>,
+          (const void *)batch_stage_kernel<T, 0, kPathCpElem>, (const void *)batch_stage_kernel<T, 1, kPathTma>,
+          (const void *)batch_stage_kernel<T, 1, kPathCp16>, (const void *)batch_stage_kernel<T, 1, kPathCpElem>,
+          (const void *)batch_stage_kernel<T, 2, kPathTma>, (const void *)batch_stage_kernel<T, 2, kPathCp16>,
+          (const void *)batch_stage_kernel<T, 2, kPathCpElem>})
+        BFB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
     int sms = 0;
     BFB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
     for (int w = 1; w <= 4; ++w) {
@@ -356,8 +512,59 @@ static int batch_upload(bfb_batch_s *b, double dt) {
     return BFB_OK;
 }
 
+// The staged mode: one launch per stage, each over every env's tiles.
+template <typename T>
+static int batch_launch_staged(bfb_batch_s *b, int flags, cudaStream_t s) {
+    const BatchInst<T> *inst = static_cast<const BatchInst<T> *>(b->d_inst);
+    const int stages = (flags & BFB_STEP_CELLS) ? 4 : 3;
+    cudaStream_t main = s;
+    // one group: the batch stream; several: a side stream per group, forked
+    // here and joined after the step's last stage
+    const int nside = b->n_groups > 1 ? b->n_groups : 0;
+    if (nside) {
+        BFB_CUDA(cudaEventRecord(b->fork_ev, main));
+        for (int i = 0; i < nside; ++i) BFB_CUDA(cudaStreamWaitEvent(b->side[i], b->fork_ev, 0));
+    }
+    for (int q = 0; q < stages; ++q) {
+        const int *tp = b->d_tpre + (size_t)q * (b->n + 1);
+        const int *pm = b->d_perm + (size_t)q * b->n;
+        const int ncls = (int)b->classes[q].size();
+        for (int ci = 0; ci < ncls; ++ci) {
+            const auto &c = b->classes[q][ci];
+            s = nside ? b->side[c.group] : main;
+            int w = b->warps;
+            while (w > 1 && (size_t)w * c.bytes > (size_t)kMaxSmem) --w;
+            const unsigned blocks = (unsigned)((c.total + w - 1) / w);
+            const size_t bytes = (size_t)w * c.bytes;
+#define BFB_STAGE_LAUNCH(Q, PATH) \
+    batch_stage_kernel<T, Q, PATH><<<blocks, 32 * w, Q < 3 ? bytes : 0, s>>>(inst, pm, tp, c.lo, c.hi, c.bytes)
+            const int key = 3 * q + (q < 3 ? c.path : 0);
+            switch (key) {
+            case 0: BFB_STAGE_LAUNCH(0, kPathTma); break;
+            case 1: BFB_STAGE_LAUNCH(0, kPathCp16); break;
+            case 2: BFB_STAGE_LAUNCH(0, kPathCpElem); break;
+            case 3: BFB_STAGE_LAUNCH(1, kPathTma); break;
+            case 4: BFB_STAGE_LAUNCH(1, kPathCp16); break;
+            case 5: BFB_STAGE_LAUNCH(1, kPathCpElem); break;
+            case 6: BFB_STAGE_LAUNCH(2, kPathTma); break;
+            case 7: BFB_STAGE_LAUNCH(2, kPathCp16); break;
+            case 8: BFB_STAGE_LAUNCH(2, kPathCpElem); break;
+            default: BFB_STAGE_LAUNCH(3, kPathTma); break;
+            }
+#undef BFB_STAGE_LAUNCH
+            BFB_CUDA(cudaGetLastError());
+        }
+    }
+    for (int i = 0; i < nside; ++i) {
+        BFB_CUDA(cudaEventRecord(b->join_ev[i], b->side[i]));
+        BFB_CUDA(cudaStreamWaitEvent(main, b->join_ev[i], 0));
+    }
+    return BFB_OK;
+}
+
 template <typename T>
 static int batch_launch(bfb_batch_s *b, int flags, cudaStream_t s) {
+    if (b->mode == BFB_BATCH_MODE_STAGED) return batch_launch_staged<T>(b, flags, s);
     const int f = (flags & BFB_STEP_CELLS) ? 1 : 0;
     BatchParams<T> p;
     p.inst = static_cast<const BatchInst<T> *>(b->d_inst);
@@ -407,12 +614,19 @@ BFB_API int bfb_batch_create(bfb_batch *out, int n_envs, const bfb_env *envs) {
     const size_t inst_bytes = prec == BFB_FP64 ? sizeof(BatchInst<double>) : sizeof(BatchInst<float>);
     cudaError_t e = cudaMalloc(&b->d_inst, inst_bytes * n_envs);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_prefix, sizeof(int) * 4 * (n_envs + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tpre, sizeof(int) * 4 * (n_envs + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_perm, sizeof(int) * 4 * n_envs);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_done, sizeof(int) * 4 * n_envs);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_maps, sizeof(CUtensorMap) * 2 * n_envs);  // 256-byte aligned
     if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
+    for (int i = 0; i < bfb_batch_s::kSide && e == cudaSuccess; ++i) {
+        e = cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         const int st = cuda_fail(e, "bfb_batch_create");
         bfb_batch_destroy(b);
@@ -430,11 +644,18 @@ BFB_API int bfb_batch_destroy(bfb_batch b) {
     batch_drop_graph(b);
     cudaFree(b->d_inst);
     cudaFree(b->d_prefix);
+    cudaFree(b->d_tpre);
+    cudaFree(b->d_perm);
     cudaFree(b->d_done);
     cudaFree(b->d_err);
     cudaFree(b->d_queue);
     cudaFree(b->d_maps);
     if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    for (int i = 0; i < bfb_batch_s::kSide; ++i) {
+        if (b->side[i]) cudaStreamDestroy(b->side[i]);
+        if (b->join_ev[i]) cudaEventDestroy(b->join_ev[i]);
+    }
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
     delete b;
     return BFB_OK;
 }
@@ -445,9 +666,24 @@ BFB_API int bfb_batch_set_option(bfb_batch b, int option, int value) {
         b->warps = value;
     else if (option == BFB_BATCH_OPT_TILES_PER_ITEM && value >= 1 && value <= 64)
         b->tiles_per_item = value;
+    else if (option == BFB_BATCH_OPT_MODE && (value == BFB_BATCH_MODE_PERSISTENT || value == BFB_BATCH_MODE_STAGED))
+        b->mode = value;
     else
         return fail(BFB_ERR_INVALID_ARG, "bfb_batch_set_option: unknown option or value");
     batch_drop_graph(b);
+    return BFB_OK;
+}
+
+BFB_API int bfb_batch_get_option(bfb_batch b, int option, int *value) {
+    if (!b || !value) return fail(BFB_ERR_INVALID_ARG, "bfb_batch_get_option: null argument");
+    if (option == BFB_BATCH_OPT_WARPS_PER_CTA)
+        *value = b->warps;
+    else if (option == BFB_BATCH_OPT_TILES_PER_ITEM)
+        *value = b->tiles_per_item;
+    else if (option == BFB_BATCH_OPT_MODE)
+        *value = b->mode;
+    else
+        return fail(BFB_ERR_INVALID_ARG, "bfb_batch_get_option: unknown option");
     return BFB_OK;
 }
 
@@ -530,12 +766,22 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
         if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
         if (ce != cudaSuccess) st = cuda_fail(ce, "cudaEventCreate");
     }
-    const int old_w = b->warps, old_t = b->tiles_per_item;
-    int best_w = old_w, best_t = old_t;
+    const int old_w = b->warps, old_t = b->tiles_per_item, old_m = b->mode;
+    int best_w = old_w, best_t = old_t, best_m = old_m;
     double best = -1.0;
-    for (int w : {1, 2, 4}) {
-        for (int tpi : {1, 2, 4, 8}) {
+    // staged: warps per CTA only (tiles per item is a persistent-mode knob)
+    struct Shape {
+        int mode, w, tpi;
+    };
+    std::vector<Shape> shapes;
+    for (int w : {1, 2, 4}) shapes.push_back({BFB_BATCH_MODE_STAGED, w, old_t});
+    for (int w : {1, 2, 4})
+        for (int tpi : {1, 2, 4, 8}) shapes.push_back({BFB_BATCH_MODE_PERSISTENT, w, tpi});
+    for (const Shape &sh : shapes) {
+        {
+            const int w = sh.w, tpi = sh.tpi;
             if (st) break;
+            b->mode = sh.mode;
             b->warps = w;
             b->tiles_per_item = tpi;
             batch_drop_graph(b);
@@ -554,6 +800,7 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
                 best = ms / trials;
                 best_w = w;
                 best_t = tpi;
+                best_m = sh.mode;
             }
         }
     }
@@ -569,6 +816,7 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
     }
     b->warps = st ? old_w : best_w;
     b->tiles_per_item = st ? old_t : best_t;
+    b->mode = st ? old_m : best_m;
     batch_drop_graph(b);
     if (st) return st;
     if (chosen) {

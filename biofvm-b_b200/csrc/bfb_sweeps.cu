@@ -155,7 +155,7 @@ __device__ __forceinline__ LineFactors32 line_factors(const SweepArgs<float> &a,
 // column lying wholly on an active face is overwritten after its solve.
 // ---------------------------------------------------------------------------
 template <typename T, int VB, bool FUSE_PRE, bool BULK>
-__global__ void __launch_bounds__(128) sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
+__global__ void __launch_bounds__(128, 1) sweep_strided_kernel(SweepArgs<T> a, StridedGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5;
     const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
@@ -167,12 +167,21 @@ __global__ void __launch_bounds__(128) sweep_strided_kernel(SweepArgs<T> a, Stri
 // Contiguous sweep (z). One warp = R consecutive (i,j) rows of nz*S elements.
 // ---------------------------------------------------------------------------
 template <typename T, int VB>
-__global__ void __launch_bounds__(128) sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
+__global__ void __launch_bounds__(128, 1) sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5;
     const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
     if (tile * g.R >= g.nrows) return;
     contig_tile<T, VB>(a, g, tile, reinterpret_cast<T *>(smem_raw) + (size_t)warp * g.R * g.RS);
+}
+// The same for S > 32 (a lane solves several lines of the tile).
+template <typename T, int VB>
+__global__ void __launch_bounds__(128, 1) sweep_contig_wide_kernel(SweepArgs<T> a, ContigGeom g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5;
+    const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (tile * g.R >= g.nrows) return;
+    contig_tile_wide<T, VB>(a, g, tile, reinterpret_cast<T *>(smem_raw) + (size_t)warp * g.R * g.RS);
 }
 
 // ---------------------------------------------------------------------------
@@ -390,7 +399,10 @@ template <typename T, int VB>
 static int go_contig(const SweepArgs<T> &a, const ContigGeom &g, int warps, size_t smem, cudaStream_t s) {
     const long long tiles = (g.nrows + g.R - 1) / g.R;
     const long long blocks = (tiles + warps - 1) / warps;
-    sweep_contig_kernel<T, VB><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
+    if (a.S > 32)
+        sweep_contig_wide_kernel<T, VB><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
+    else
+        sweep_contig_kernel<T, VB><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
 }
@@ -472,6 +484,11 @@ void sweeps_prepare_device() {
     opt_in(sweep_contig_kernel<float, 16>);
     opt_in(sweep_contig_kernel<float, 8>);
     opt_in(sweep_contig_kernel<float, 4>);
+    opt_in(sweep_contig_wide_kernel<double, 16>);
+    opt_in(sweep_contig_wide_kernel<double, 8>);
+    opt_in(sweep_contig_wide_kernel<float, 16>);
+    opt_in(sweep_contig_wide_kernel<float, 8>);
+    opt_in(sweep_contig_wide_kernel<float, 4>);
     tma_prepare_device();
     done |= 1ull << (dev & 63);
 }

@@ -110,13 +110,13 @@ __device__ __forceinline__ void strided_tile(const SweepArgs<T> &a, const Stride
     for (int ch = 0; ch <= ref_ch; ++ch) wait(ch);
     sm[lane] = L.first(xin(0), xin(rref));
     int r = 1;
+    auto st_sm = [&](int q, T v) { sm[q * 32 + lane] = v; };
     for (int ch = 0; ch < nch; ++ch) {
         if (ch > ref_ch) wait(ch);
         const int rend = min(n - 1, (ch + 1) * crow);
         const int hend = min(rend, m0);
-        for (; r < hend; ++r) sm[r * 32 + lane] = L.template fwd<false>(load(r), r);
-#pragma unroll 8
-        for (; r < rend; ++r) sm[r * 32 + lane] = L.template fwd<true>(load(r), r);
+        r = head_forward(L, r, hend, load, st_sm);
+        r = tail_forward(L, r, rend, load, st_sm);
     }
     if (n > 1) {
         T x = load(n - 1);
@@ -132,30 +132,25 @@ __device__ __forceinline__ void strided_tile(const SweepArgs<T> &a, const Stride
         *gp = y;
     }
     const int tl = max(m0, 1);
-    r = n - 2;
-#pragma unroll 8
-    for (; r >= tl; --r) {
-        gp -= P;
-        *gp = L.template bwd<true>(sm[r * 32 + lane], r);
-    }
-    for (; r >= 1; --r) {
-        gp -= P;
-        *gp = L.template bwd<false>(sm[r * 32 + lane], r);
-    }
+    T *__restrict__ go = obase + lane;
+    auto ld_sm = [&](int q) { return sm[q * 32 + lane]; };
+    auto st_g = [&](int q, T v) { go[(size_t)q * P] = v; };
+    r = tail_backward(L, n - 2, tl, ld_sm, st_g);
+    r = head_backward(L, r, 1, ld_sm, st_g);
     if (n > 1) {
         T y = L.template bwd<false>(sm[lane], 0);
         if (lo_dir) y = vox_dir(0);
-        gp -= P;
-        *gp = y;
+        go[0] = y;
     }
     if (col_dir)  // the whole column is on an active face of another axis
         for (int q = 0; q < n; ++q) obase[lane + (size_t)q * P] = vox_dir(q);
 }
 
-// One contiguous tile (R rows) by the calling warp; sm is the warp's region
-// of R*RS elements. Used by the single-env kernel below and by bfb_batch.cu.
+// One contiguous tile (R rows) by the calling warp, any S (lanes loop over
+// the tile's lines); sm is the warp's region of R*RS elements. The S > 32
+// kernel runs it, and contig_tile_any for S > 32.
 template <typename T, int VB>
-__device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigGeom &g, long long tile, T *sm) {
+__device__ __forceinline__ void contig_tile_wide(const SweepArgs<T> &a, const ContigGeom &g, long long tile, T *sm) {
     const int lane = threadIdx.x & 31;
     const long long row0 = tile * g.R;
     const int nr = (int)min((long long)g.R, g.nrows - row0);
@@ -232,6 +227,127 @@ __device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigG
             }
         }
     }
+}
+
+// One contiguous tile (R = 32/S rows) by the calling warp for S <= 32; sm is
+// the warp's region of R*RS elements. Used by the single-env cp.async kernel
+// (bfb_sweeps.cu) and, through contig_tile_any, by bfb_batch.cu. Each row's k range is cut into two
+// row groups, each one cp.async commit group of VB-byte copies (every row
+// group starts VB-aligned), so the forward elimination starts on group 0
+// while group 1 lands; the back substitution finishes group 1 first and the
+// warp writes it out while it computes group 0. Lane (r, d) solves line
+// (row0 + r, d) with the blocked row loops of bfb_line.cuh.
+template <typename T, int VB>
+__device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigGeom &g, long long tile, T *sm) {
+    const int S = a.S;
+    const int lane = threadIdx.x & 31;
+    const long long row0 = tile * g.R;
+    const int nr = (int)min((long long)g.R, g.nrows - row0);
+    const int nz = g.nz;
+    const int L = nz * S;
+    const int RS = g.RS;
+    T *__restrict__ base = a.f + (size_t)row0 * L;
+    T *__restrict__ obase = a.fo + (size_t)row0 * L;
+    constexpr int EPV = VB / (int)sizeof(T);
+    // k rows per group: a multiple of EPV / gcd(EPV, S), so that k0*S is a multiple of EPV
+    int qa = EPV;
+    for (int v = S; v % 2 == 0 && qa > 1; v /= 2) qa /= 2;
+    int kc = (nz + 1) / 2;
+    kc = (kc + qa - 1) / qa * qa;
+    const int nch = (nz + kc - 1) / kc;  // 1 or 2
+
+    for (int c = 0; c < nch; ++c) {
+        const int k0 = c * kc, span = (min(nz, k0 + kc) - k0) * S, vspan = span / EPV;
+        for (int r = 0; r < nr; ++r) {
+            T *dst = sm + (size_t)r * RS + (size_t)k0 * S;
+            const T *src = base + (size_t)r * L + (size_t)k0 * S;
+            for (int v = lane; v < vspan; v += 32) cp_async<VB>(dst + v * EPV, src + v * EPV);
+        }
+        cp_commit();
+    }
+    auto wait_c = [&](int c) {
+        cp_wait_dyn(nch - 1 - c);
+        __syncwarp();
+    };
+    auto store_c = [&](int c) {  // row group c of every row, shared -> global
+        const int k0 = c * kc, span = (min(nz, k0 + kc) - k0) * S, vspan = span / EPV;
+        for (int r = 0; r < nr; ++r) {
+            const T *src = sm + (size_t)r * RS + (size_t)k0 * S;
+            T *dst = obase + (size_t)r * L + (size_t)k0 * S;
+            for (int v = lane; v < vspan; v += 32) {
+                if constexpr (VB == 16) {
+                    *reinterpret_cast<int4 *>(dst + v * EPV) = *reinterpret_cast<const int4 *>(src + v * EPV);
+                } else if constexpr (VB == 8) {
+                    *reinterpret_cast<int2 *>(dst + v * EPV) = *reinterpret_cast<const int2 *>(src + v * EPV);
+                } else {
+                    dst[v] = src[v];
+                }
+            }
+        }
+    };
+
+    const bool active = lane < nr * S;
+    const int r = active ? lane / S : 0;
+    const int d = active ? lane - r * S : 0;
+    const long long row = row0 + r;
+    const int i = (int)(row / a.ny), j = (int)(row % a.ny);
+    const unsigned m = (a.dir.any && active) ? a.dir.mask[d] : 0u;
+    const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
+                          ((m & 8u) && j == a.ny - 1);
+    const bool lo_dir = m & 16u, hi_dir = m & 32u;
+    T *line = sm + (size_t)r * RS + d;
+    LineSolver<T> Ls(a, d);
+    const int m0 = a.fac.m0;
+    auto ld = [&](int q) { return line[q * S]; };
+    auto st = [&](int q, T v) { line[q * S] = v; };
+
+    // ---- forward
+    const int kref = min(1, nz - 1);  // row of the deviation reference
+    const int ref_c = kref / kc;
+    for (int c = 0; c <= ref_c; ++c) wait_c(c);
+    if (active) line[0] = Ls.first(line[0], line[kref * S]);
+    int k = 1;
+    for (int c = 0; c < nch; ++c) {
+        if (c > ref_c) wait_c(c);
+        const int kend = min(nz - 1, (c + 1) * kc);
+        if (active) {
+            k = head_forward(Ls, k, min(kend, m0), ld, st);
+            k = tail_forward(Ls, k, kend, ld, st);
+        }
+        k = max(k, kend);
+    }
+    if (active && nz > 1) Ls.template fwd<false>(line[(nz - 1) * S], nz - 1);
+
+    // ---- backward; each finished row group is written out for all rows
+    if (active) {
+        const T y = Ls.out_last();  // also seeds the back substitution
+        line[(nz - 1) * S] = (hi_dir || (lo_dir && nz == 1)) ? dir_value(a.dir, i, j, nz - 1, d) : y;
+    }
+    const int tl = max(m0, 1);
+    k = nz - 2;
+    for (int c = nch - 1; c >= 0; --c) {
+        const int klo = c * kc;
+        if (active) {
+            k = tail_backward(Ls, k, max(klo, tl), ld, st);
+            k = head_backward(Ls, k, max(klo, 1), ld, st);
+            if (klo == 0 && nz > 1) {
+                const T y = Ls.template bwd<false>(line[0], 0);
+                line[0] = lo_dir ? dir_value(a.dir, i, j, 0, d) : y;
+            }
+            if (line_dir)
+                for (int q = klo; q < min(nz, klo + kc); ++q) line[q * S] = dir_value(a.dir, i, j, q, d);
+        }
+        k = min(k, klo - 1);
+        __syncwarp();
+        store_c(c);
+    }
+}
+
+// contig_tile for S <= 32, contig_tile_wide otherwise.
+template <typename T, int VB>
+__device__ __forceinline__ void contig_tile_any(const SweepArgs<T> &a, const ContigGeom &g, long long tile, T *sm) {
+    if (a.S > 32) contig_tile_wide<T, VB>(a, g, tile, sm);
+    else contig_tile<T, VB>(a, g, tile, sm);
 }
 
 }  // namespace bfb

@@ -233,27 +233,37 @@ BFB_API int bfb_checksum(bfb_env env, double *out);
 /* ---- Batched ensembles ---------------------------------------------------
  * Many independent envs (uneven shapes and substrate counts; one device and
  * one precision) stepped together: bfb_batch_simulate runs one LOD step of
- * every env -- and, with BFB_STEP_CELLS, its agents -- as ONE persistent
- * kernel launch whose warps pull (env, stage, tile) work items from a device
- * queue, replayed from a CUDA graph. The batch references the envs; they must
- * outlive it, and their own settings (coefficients, Dirichlet, agents) are
- * the ones used. bfb_batch_simulate_loop runs the same steps as one
- * bfb_simulate call per env (the per-instance launch loop). Not in the
- * reference, which runs one Microenvironment per MPI job. */
+ * every env -- and, with BFB_STEP_CELLS, its agents -- replayed from a CUDA
+ * graph, in one of two modes:
+ *   BFB_BATCH_MODE_STAGED (default): one launch per stage (x, y, z sweeps,
+ *     agents), each a flat grid over every env's tiles, one warp per tile;
+ *   BFB_BATCH_MODE_PERSISTENT: ONE persistent kernel launch per step whose
+ *     warps pull (env, stage, tile) work items from a device queue.
+ * The batch references the envs; they must outlive it, and their own settings
+ * (coefficients, Dirichlet, agents) are the ones used.
+ * bfb_batch_simulate_loop runs the same steps as one bfb_simulate call per
+ * env (the per-instance launch loop). Not in the reference, which runs one
+ * Microenvironment per MPI job. */
 typedef struct bfb_batch_s *bfb_batch;
 #define BFB_BATCH_OPT_WARPS_PER_CTA 1   /* 1..4, default 1 */
-#define BFB_BATCH_OPT_TILES_PER_ITEM 2  /* warp tiles per queue item, 1..64, default 2 */
+#define BFB_BATCH_OPT_TILES_PER_ITEM 2  /* warp tiles per queue item (persistent mode), 1..64, default 2 */
+#define BFB_BATCH_OPT_MODE 3            /* BFB_BATCH_MODE_STAGED (default) or BFB_BATCH_MODE_PERSISTENT */
+#define BFB_BATCH_MODE_PERSISTENT 0
+#define BFB_BATCH_MODE_STAGED 1
 BFB_API int bfb_batch_create(bfb_batch *out, int n_envs, const bfb_env *envs);
 BFB_API int bfb_batch_destroy(bfb_batch batch);
 BFB_API int bfb_batch_set_option(bfb_batch batch, int option, int value);
+BFB_API int bfb_batch_get_option(bfb_batch batch, int option, int *value);
 BFB_API int bfb_batch_simulate(bfb_batch batch, double dt, int n_steps, int flags);
 BFB_API int bfb_batch_simulate_loop(bfb_batch batch, double dt, int n_steps, int flags);
 BFB_API int bfb_batch_synchronize(bfb_batch batch);
-/* Times bfb_batch_simulate for warps per CTA {1, 2, 4} x tiles per item
+/* Times bfb_batch_simulate in the staged mode with warps per CTA {1, 2, 4}
+ * and in the persistent mode with warps per CTA {1, 2, 4} x tiles per item
  * {1, 2, 4, 8} (one warm step and `trials` timed steps each, CUDA events),
  * keeps the fastest and returns it in chosen[2] = {warps, tiles per item}
- * and its milliseconds per step in *best_ms (either may be NULL). The trial
- * steps advance the envs' fields, so every field is saved first and restored
+ * (the mode: bfb_batch_get_option with BFB_BATCH_OPT_MODE) and its
+ * milliseconds per step in *best_ms (either may be NULL). The trial steps
+ * advance the envs' fields, so every field is saved first and restored
  * before returning. Not in the reference. */
 BFB_API int bfb_batch_autotune(bfb_batch batch, double dt, int flags, int trials, int *chosen, double *best_ms);
 

@@ -1,4 +1,5 @@
-"""Batched ensembles: one persistent launch per step over many uneven envs."""
+"""Batched ensembles over many uneven envs, in both modes: one launch per
+stage over every env's tiles (staged) and one persistent launch per step."""
 from __future__ import annotations
 
 import math
@@ -57,12 +58,14 @@ def oracle_run(oracle, spec, dt, steps):
     return rho
 
 
+@pytest.mark.parametrize("mode", ["staged", "persistent"])
 @pytest.mark.parametrize("warps", [1, 2])
-def test_batch_small_fp64_bitexact(bfb, oracle, warps):
+def test_batch_small_fp64_bitexact(bfb, oracle, warps, mode):
     rng = np.random.default_rng(404)
     dt, steps = 0.01, 4
     specs, envs = zip(*[make_instance(bfb, rng, 2, 24, 300, bfb.FP64, dt) for _ in range(12)])
     batch = bfb.Batch(envs)
+    batch.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
     batch.set_warps(warps)
     batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
     batch.synchronize()
@@ -90,12 +93,15 @@ def make_aligned_instance(bfb, rng, prec, dt, n_agents=400):
     return spec, build(bfb, spec, prec, dt)
 
 
-@pytest.mark.parametrize("warps,tiles", [(1, 1), (2, 3), (4, 8), (1, 64)])
-def test_batch_tma_items_fp64_bitexact(bfb, oracle, warps, tiles):
+@pytest.mark.parametrize("mode,warps,tiles", [("persistent", 1, 1), ("persistent", 2, 3), ("persistent", 4, 8),
+                                              ("persistent", 1, 64), ("staged", 1, 2), ("staged", 4, 2)])
+def test_batch_tma_items_fp64_bitexact(bfb, oracle, mode, warps, tiles):
     rng = np.random.default_rng(900 + warps * 10 + tiles)
     dt, steps = 0.01, 3
     specs, envs = zip(*[make_aligned_instance(bfb, rng, bfb.FP64, dt) for _ in range(6)])
     batch = bfb.Batch(envs)
+    batch.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
+    assert batch.mode == (bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
     batch.set_warps(warps)
     batch.set_tiles_per_item(tiles)
     batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
@@ -112,6 +118,7 @@ def test_batch_autotune_restores_fields(bfb, oracle):
     before = [e.get_field_raw() for e in envs]
     (w, t), ms = batch.autotune(dt, bfb.STEP_DIFFUSION | bfb.STEP_CELLS, trials=1)
     assert w in (1, 2, 4) and t in (1, 2, 4, 8) and ms > 0
+    assert batch.mode in (bfb.BATCH_MODE_STAGED, bfb.BATCH_MODE_PERSISTENT)
     for e, b0 in zip(envs, before):
         assert np.array_equal(e.get_field_raw(), b0)
     batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
@@ -120,7 +127,8 @@ def test_batch_autotune_restores_fields(bfb, oracle):
         assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps))
 
 
-def test_batch_fp32_equals_per_instance_loop(bfb):
+@pytest.mark.parametrize("mode", ["staged", "persistent"])
+def test_batch_fp32_equals_per_instance_loop(bfb, mode):
     rng = np.random.default_rng(405)
     dt, steps = 0.01, 5
     made = [make_instance(bfb, rng, 3, 40, 800, bfb.FP32, dt) for _ in range(10)]
@@ -128,6 +136,7 @@ def test_batch_fp32_equals_per_instance_loop(bfb):
     envs_b = [m[1] for m in made]
     envs_l = [build(bfb, sp, bfb.FP32, dt) for sp in specs]
     b = bfb.Batch(envs_b)
+    b.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
     b.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
     b.synchronize()
     lp = bfb.Batch(envs_l)
@@ -138,8 +147,9 @@ def test_batch_fp32_equals_per_instance_loop(bfb):
 
 def test_config4_batch_vs_loop_and_fp64_check(bfb):
     """Config 4: 256 envs, edges U{32..160} per axis, 1-6 substrates, 0-20k
-    agents each, 200 steps in FP32; FP64 check on 8 sampled envs; one
-    persistent launch per step against the per-instance launch loop."""
+    agents each, 200 steps in FP32; FP64 check on 8 sampled envs; the batch
+    (staged launches, and one persistent launch per step) against the
+    per-instance launch loop."""
     rng = np.random.default_rng(4)
     dt, steps = 0.01, 200
     made = [make_instance(bfb, rng, 32, 160, 20_000, bfb.FP32, dt) for _ in range(256)]
@@ -148,13 +158,24 @@ def test_config4_batch_vs_loop_and_fp64_check(bfb):
     vs = sum(int(np.prod(sp["shape"])) * sp["S"] for sp in specs)
     flags = bfb.STEP_DIFFUSION | bfb.STEP_CELLS
     batch = bfb.Batch(envs)
-    tuned, _ = batch.autotune(dt, flags, trials=2)  # warps per CTA and tiles per item
-    batch.simulate(dt, 2, flags)  # warm-up (graph capture)
-    batch.synchronize()
-    t0 = time.perf_counter()
-    batch.simulate(dt, steps, flags)
-    batch.synchronize()
-    t_batch = (time.perf_counter() - t0) / steps
+
+    def timed(n):
+        batch.simulate(dt, 2, flags)  # warm-up (graph capture)
+        batch.synchronize()
+        t0 = time.perf_counter()
+        batch.simulate(dt, n, flags)
+        batch.synchronize()
+        return (time.perf_counter() - t0) / n
+
+    batch.set_mode(bfb.BATCH_MODE_PERSISTENT)
+    batch.set_warps(1)
+    batch.set_tiles_per_item(4)
+    t_pers = timed(20)
+    batch.set_mode(bfb.BATCH_MODE_STAGED)
+    t_staged = timed(20)
+    tuned, _ = batch.autotune(dt, flags, trials=2)  # mode, warps per CTA and tiles per item
+    mode = "staged" if batch.mode == bfb.BATCH_MODE_STAGED else "persistent"
+    t_batch = timed(steps - 44)  # 202 steps in all (3 x 2 warm + 20 + 20 + 156), as the FP64 check below
     # per-instance launch loop over fresh copies of the same envs
     loop_envs = [build(bfb, sp, bfb.FP32, dt) for sp in specs]
     loop = bfb.Batch(loop_envs)
@@ -171,7 +192,9 @@ def test_config4_batch_vs_loop_and_fp64_check(bfb):
         e64.synchronize()
         errs.append(envs[q].compare(e64)[0])
         e64.close()
-    print(f"\nconfig 4 (256 envs, {vs / 1e6:.0f} M voxel*substrates, 200 steps): persistent batch "
-          f"(warps, tiles per item = {tuned}) {t_batch * 1e3:.3f} ms/step ({vs / t_batch:.3e} vox*sub/s), per-instance loop {t_loop * 1e3:.3f} ms/step "
-          f"({vs / t_loop:.3e}); FP32 vs FP64 rel Linf on 8 envs: max {max(errs):.2e}")
+    print(f"\nconfig 4 (256 envs, {vs / 1e6:.0f} M voxel*substrates, 200 steps): batch, autotuned "
+          f"({mode}, warps, tiles per item = {tuned}) {t_batch * 1e3:.3f} ms/step ({vs / t_batch:.3e} vox*sub/s); "
+          f"staged (1 warp) {t_staged * 1e3:.3f}, persistent (1 warp, 4 tiles) {t_pers * 1e3:.3f}; "
+          f"per-instance loop {t_loop * 1e3:.3f} ms/step ({vs / t_loop:.3e}); "
+          f"FP32 vs FP64 rel Linf on 8 envs: max {max(errs):.2e}")
     assert max(errs) <= 1e-5
