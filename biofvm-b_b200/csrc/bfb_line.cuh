@@ -19,6 +19,14 @@ __device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
 }
+// the same with the shared-memory address already in the shared window
+template <int BYTES>
+__device__ __forceinline__ void cp_async_s(unsigned s, const void *gmem) {
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -101,7 +109,8 @@ struct LineSolver;
 // factors read four rows at a time from the head tables; the operations are
 // those of fwd<false> / bwd<false>. ld(q) reads row q's value, st(q, v)
 // writes it. head_forward covers rows [r, end) and returns end;
-// head_backward covers rows r, r-1, ..., stop and returns stop - 1.
+// head_backward covers rows r, r-1, ..., stop and returns stop - 1, calling
+// st for those rows in that order.
 template <typename T, typename LD, typename ST>
 __device__ __forceinline__ int head_forward(LineSolver<T> &L, int r, int end, LD ld, ST st) {
     int q = r;
@@ -121,7 +130,8 @@ __device__ __forceinline__ int head_forward(LineSolver<T> &L, int r, int end, LD
 // bstep) runs row after row; the operations are those of fwd<true> /
 // bwd<true>. ld(q) reads row q's input, st(q, v) writes its output.
 // tail_forward covers rows [r, end) and returns end; tail_backward covers
-// rows r, r-1, ..., stop and returns stop - 1.
+// rows r, r-1, ..., stop and returns stop - 1, calling st for those rows in
+// that order (callers may rely on it).
 constexpr int kTailBlock = 24;  // measured: 4 < 8 < 16 < 24 > 32 at 256^3 x 8
 template <typename T, typename LD, typename ST>
 __device__ __forceinline__ int tail_forward(LineSolver<T> &L, int r, int end, LD ld, ST st) {

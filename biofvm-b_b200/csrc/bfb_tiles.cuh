@@ -36,7 +36,12 @@ __device__ __forceinline__ void strided_tile(const SweepArgs<T> &a, const Stride
                 cp_async<VB>(sm + r * 32 + q, base + (size_t)r * P + q);
             }
         } else if (lane < ncols) {
-            for (int r = r0; r < r1; ++r) cp_async<sizeof(T)>(sm + r * 32 + lane, base + (size_t)r * P + lane);
+            // one element per lane and row: 32-bit shared addresses and a
+            // global pointer stepped by the row pitch
+            const T *gp = base + (size_t)r0 * P + lane;
+            unsigned sp = (unsigned)__cvta_generic_to_shared(sm + r0 * 32 + lane);
+#pragma unroll 4
+            for (int r = r0; r < r1; ++r, gp += P, sp += 32 * (unsigned)sizeof(T)) cp_async_s<sizeof(T)>(sp, gp);
         }
         cp_commit();
     }
@@ -134,7 +139,14 @@ __device__ __forceinline__ void strided_tile(const SweepArgs<T> &a, const Stride
     const int tl = max(m0, 1);
     T *__restrict__ go = obase + lane;
     auto ld_sm = [&](int q) { return sm[q * 32 + lane]; };
-    auto st_g = [&](int q, T v) { go[(size_t)q * P] = v; };
+    // tail_backward and head_backward store rows n-2, n-3, ..., 1 in this
+    // order: a pointer stepped down by the pitch replaces a 64-bit index
+    // product per row
+    T *gw = go + (size_t)max(n - 2, 0) * P;
+    auto st_g = [&](int, T v) {
+        *gw = v;
+        gw -= P;
+    };
     r = tail_backward(L, n - 2, tl, ld_sm, st_g);
     r = head_backward(L, r, 1, ld_sm, st_g);
     if (n > 1) {
@@ -259,9 +271,10 @@ __device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigG
     for (int c = 0; c < nch; ++c) {
         const int k0 = c * kc, span = (min(nz, k0 + kc) - k0) * S, vspan = span / EPV;
         for (int r = 0; r < nr; ++r) {
-            T *dst = sm + (size_t)r * RS + (size_t)k0 * S;
-            const T *src = base + (size_t)r * L + (size_t)k0 * S;
-            for (int v = lane; v < vspan; v += 32) cp_async<VB>(dst + v * EPV, src + v * EPV);
+            const T *src = base + (size_t)r * L + (size_t)k0 * S + lane * EPV;
+            unsigned dst = (unsigned)__cvta_generic_to_shared(sm + (size_t)r * RS + (size_t)k0 * S + lane * EPV);
+#pragma unroll 4
+            for (int v = lane; v < vspan; v += 32, src += 32 * EPV, dst += 32 * VB) cp_async_s<VB>(dst, src);
         }
         cp_commit();
     }
