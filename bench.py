@@ -257,17 +257,14 @@ def run_our_arm(args):
     D, lam, rng = coefficients()
     rho0 = initial_field(rng)
 
+    ranks = importlib.import_module("biofvm_b_b200.ranks")  # barrier and max over ranks (no-ops in one process)
+    dev = torch.device("cuda", local)
+
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        ranks.barrier(dev)
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max_over_ranks(x, dev)
 
     results = {}
     stream = torch.cuda.Stream()
