@@ -110,6 +110,31 @@ def test_batch_tma_items_fp64_bitexact(bfb, oracle, mode, warps, tiles):
         assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps)), spec["shape"]
 
 
+@pytest.mark.parametrize("mode", ["staged", "persistent"])
+def test_batch_wide_substrates_fp64_bitexact(bfb, oracle, mode):
+    """Envs with more than 32 substrates (a lane solves several z lines) next
+    to ordinary ones in one batch."""
+    rng = np.random.default_rng(77)
+    dt, steps = 0.01, 3
+    specs, envs = [], []
+    for shape, S in (((6, 5, 7), 40), ((9, 4, 6), 33), ((8, 8, 8), 3)):
+        D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+        fm = np.zeros((6, S), np.uint8)
+        fm[0, 0] = fm[1, 0] = 1
+        act = np.zeros(S, np.uint8)
+        act[0] = 1
+        spec = dict(shape=shape, S=S, D=D, lam=lam, rho0=rng.random((*shape, S)), fm=fm, act=act,
+                    pos=np.zeros((0, 3)), vol=np.zeros(0), sec=None, upt=None, sat=None, box=None)
+        specs.append(spec)
+        envs.append(build(bfb, spec, bfb.FP64, dt))
+    batch = bfb.Batch(envs)
+    batch.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
+    batch.simulate(dt, steps, bfb.STEP_DIFFUSION)
+    batch.synchronize()
+    for spec, env in zip(specs, envs):
+        assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps)), (spec["shape"], spec["S"])
+
+
 def test_batch_autotune_restores_fields(bfb, oracle):
     rng = np.random.default_rng(31)
     dt, steps = 0.01, 2

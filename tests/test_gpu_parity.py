@@ -134,7 +134,7 @@ def test_config1_full_size_fp64(bfb, oracle):
 
 SHAPES = [((1, 1, 1), 1), ((1, 4, 6), 2), ((2, 3, 1), 3), ((3, 2, 2), 1), ((5, 17, 3), 4), ((17, 5, 2), 6),
           ((8, 8, 8), 4), ((8, 8, 8), 8), ((7, 5, 9), 3), ((33, 31, 35), 5), ((64, 2, 3), 2), ((2, 64, 40), 1),
-          ((40, 3, 64), 7)]
+          ((40, 3, 64), 7), ((6, 5, 7), 40), ((3, 9, 4), 33)]  # S > 32: lanes solve several z lines each
 
 
 @pytest.mark.parametrize("tma", [1, 0], ids=["tma", "cpasync"])
