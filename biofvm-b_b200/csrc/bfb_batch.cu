@@ -1,24 +1,36 @@
-// bfb_batch.cu -- many independent microenvironments in one persistent launch.
+// bfb_batch.cu -- many independent microenvironments stepped together.
 //
 // A batch references N envs of uneven shapes and substrate counts (same
-// device and precision). One LOD step of all of them is one launch of
-// batch_step_kernel: a grid of resident CTAs whose warps pull work items from
-// a device queue (one atomic counter). An item is `tiles_per_item` adjacent
-// warp tiles of one env and one stage; the items of one step are ordered
+// device and precision). Every tile runs the single-env kernels' warp-tile
+// code: the TMA tiles (bfb_tma_tiles.cuh; the env's own tensor maps, read from
+// global memory) where the env's grid and launch shape allow them, else the
+// cp.async tiles (bfb_tiles.cuh). One step is captured once in a CUDA graph and
+// replayed, in one of two modes:
+//
+// Staged (default): one launch per stage over a flat grid of tiles, one warp
+// per tile (batch_stage_kernel). Per stage, the envs are listed by group, tile
+// path and tile size (d_perm) with the prefix of their tile counts (d_tpre);
+// a launch covers one class -- one group, one path, tiles within a factor 2 of
+// each other -- so that its kernel compiles one path and its shared memory per
+// warp fits the class. Each group of envs (about equal work) runs its chain of
+// stage launches on its own stream, forked from and joined to the batch stream
+// inside the graph; stream order alone orders the stages, so no warp waits.
+//
+// Persistent: one launch of batch_step_kernel per step, a grid of resident
+// CTAs whose warps pull work items from a device queue (one atomic counter).
+// An item is `tiles_per_item` adjacent warp tiles of one env and one stage;
+// the items of one step are ordered
 //     [x items of env 0..N-1][y items ...][z items ...][cell chunks ...]
 // and an item of env k waits (bounded) until env k has finished every item of
 // the previous stage. It only ever waits for items that running warps took
 // earlier, so the launch cannot deadlock, whether or not the whole grid is
-// resident. Each tile runs the single-env kernels' warp-tile code: the TMA
-// tiles (bfb_tma_tiles.cuh; the env's own tensor maps, read from global
-// memory) where the env's grid and launch shape allow them, else the
-// cp.async tiles (bfb_tiles.cuh). A finished item is published with its bulk
-// stores complete (cp.async.bulk.wait_group 0), a proxy fence and a release;
-// a consumer acquires, then fences before its own tensor loads. The step
-// (counter resets + launch) is captured once in a CUDA graph and replayed.
-// bfb_batch_simulate_loop runs the same envs one bfb_simulate call at a time,
-// the per-instance launch loop the persistent launch is compared with;
-// bfb_batch_autotune picks warps per CTA and tiles per item.
+// resident. A finished item is published with its bulk stores complete
+// (cp.async.bulk.wait_group), a proxy fence and a release; a consumer
+// acquires, then fences before its own tensor loads.
+//
+// bfb_batch_simulate_loop runs the same envs one bfb_simulate call at a time
+// (the per-instance launch loop); bfb_batch_autotune picks the mode, warps per
+// CTA and tiles per item.
 #include <algorithm>
 #include <vector>
 
