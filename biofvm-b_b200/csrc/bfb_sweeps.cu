@@ -369,6 +369,9 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, co
     }
     g.ncb = (int)((g.P + 31) / 32);
     warps = std::max(1, std::min(warps, 4));
+    // the x sweep's load-time Dirichlet and bulk update: without either, the
+    // plain kernel computes the same
+    fuse_pre = fuse_pre && (a.dir.any || a.bulk.on);
     if (map && map_out) {
         const int st = launch_strided_tma<T>(a, g, map, map_out, crow, fuse_pre, warps, s);
         if (st != kNotApplicable) return st;
