@@ -214,7 +214,9 @@ BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double
  * at its two ends; 0 on an axis of one voxel. bfb_compute_gradients writes
  * 3*V*S elements of the env's precision to device memory, on the env's
  * stream (returns without waiting); bfb_get_gradients returns host doubles.
- * FP64 is bit-exact with the reference. */
+ * FP64 is bit-exact with the reference. An out_dev on a 16-byte boundary
+ * (any cudaMalloc pointer) lets rows of a whole number of 16-byte vectors run
+ * the faster vectorised kernel; other pointers give the same values. */
 BFB_API int bfb_compute_gradients(bfb_env env, void *out_dev);
 BFB_API int bfb_get_gradients(bfb_env env, double *out_host);
 
