@@ -23,8 +23,8 @@ def lu(rng, lo, hi, size):
     return np.exp(rng.uniform(np.log(lo), np.log(hi), size))
 
 
-def case_config1_small(ref):
-    """Config-1 recipe (1 substrate, D=1e5, lambda=0.1, dt=0.01, Dirichlet 1.0
+def case_lod_15cube_dirichlet(ref):
+    """The 75^3 single-substrate recipe (1 substrate, D=1e5, lambda=0.1, dt=0.01, Dirichlet 1.0
     on all faces, U[0,1) field) on a 15^3 grid, 20 steps, both solvers."""
     rng = np.random.default_rng(1)
     dx, dt, steps = 20.0, 0.01, 20
@@ -112,7 +112,7 @@ def case_agents(ref):
 def main():
     ref = RefLib()
     cases = {
-        "config1_15cube": case_config1_small(ref),
+        "lod_15cube_s1_dirichlet": case_lod_15cube_dirichlet(ref),
         "multi_7x5x9_S3": case_multi(ref, 21, (7, 5, 9), 3, 6),
         "multi_1x4x6_S2": case_multi(ref, 22, (1, 4, 6), 2, 4),
         "multi_2x3x1_S2": case_multi(ref, 23, (2, 3, 1), 2, 4),

@@ -170,8 +170,8 @@ def test_batch_fp32_equals_per_instance_loop(bfb, mode):
         assert np.array_equal(eb.get_field_raw(), el.get_field_raw())
 
 
-def test_config4_batch_vs_loop_and_fp64_check(bfb):
-    """Config 4: 256 envs, edges U{32..160} per axis, 1-6 substrates, 0-20k
+def test_ensemble_256_batch_vs_loop_and_fp64_check(bfb):
+    """Uneven ensemble: 256 envs, edges U{32..160} per axis, 1-6 substrates, 0-20k
     agents each, 200 steps in FP32; FP64 check on 8 sampled envs; the batch
     (staged launches, and one persistent launch per step) against the
     per-instance launch loop."""
@@ -217,7 +217,7 @@ def test_config4_batch_vs_loop_and_fp64_check(bfb):
         e64.synchronize()
         errs.append(envs[q].compare(e64)[0])
         e64.close()
-    print(f"\nconfig 4 (256 envs, {vs / 1e6:.0f} M voxel*substrates, 200 steps): batch, autotuned "
+    print(f"\nuneven ensemble (256 envs, {vs / 1e6:.0f} M voxel*substrates, 200 steps): batch, autotuned "
           f"({mode}, warps, tiles per item = {tuned}) {t_batch * 1e3:.3f} ms/step ({vs / t_batch:.3e} vox*sub/s); "
           f"staged (1 warp) {t_staged * 1e3:.3f}, persistent (1 warp, 4 tiles) {t_pers * 1e3:.3f}; "
           f"per-instance loop {t_loop * 1e3:.3f} ms/step ({vs / t_loop:.3e}); "

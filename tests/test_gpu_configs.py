@@ -24,7 +24,7 @@ def agents_in_ball(rng, n, centre, radius):
     return np.asarray(centre) + u * (radius * rng.random((n, 1)) ** (1.0 / 3.0))
 
 
-def config2_inputs(rng, n_vox, n_agents, radius):
+def agents_xface_inputs(rng, n_vox, n_agents, radius):
     S = 8
     D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
     rho0 = rng.random((n_vox, n_vox, n_vox, S))
@@ -52,11 +52,11 @@ def build_env(bfb, prec, rho0, D, lam, agents, dt, dirichlet):
     return env
 
 
-def test_config2_reduced_fp64_bitexact(bfb, oracle):
-    """Config 2's recipe (x-face Dirichlet 38 on substrate 0, agents in a
+def test_agents_xface_reduced_fp64_bitexact(bfb, oracle):
+    """The 200^3 x 8 agents workload's recipe (x-face Dirichlet 38 on substrate 0, agents in a
     central ball, diffusion then cells) on 40^3 x 8 for 20 steps."""
     rng = np.random.default_rng(202)
-    D, lam, rho0, pos, vol, sec, upt, sat, fm, act, vals = config2_inputs(rng, 40, 4000, 100.0)
+    D, lam, rho0, pos, vol, sec, upt, sat, fm, act, vals = agents_xface_inputs(rng, 40, 4000, 100.0)
     dt = 0.01
     env = build_env(bfb, bfb.FP64, rho0, D, lam, (pos, vol, sec, upt, sat), dt, (fm, act, vals))
     env.simulate(dt, 20, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
@@ -73,10 +73,10 @@ def test_config2_reduced_fp64_bitexact(bfb, oracle):
     assert np.array_equal(got, want)
 
 
-def test_config2_full_fp32_vs_fp64(bfb):
-    """Config 2: 200^3 x 8, 100k agents in a 500 um ball, 500 steps."""
+def test_agents_200cube_s8_fp32_vs_fp64(bfb):
+    """The agents workload: 200^3 x 8, 100k agents in a 500 um ball, 500 steps."""
     rng = np.random.default_rng(2)
-    D, lam, rho0, pos, vol, sec, upt, sat, fm, act, vals = config2_inputs(rng, 200, 100_000, 500.0)
+    D, lam, rho0, pos, vol, sec, upt, sat, fm, act, vals = agents_xface_inputs(rng, 200, 100_000, 500.0)
     dt = 0.01
     envs = {}
     for prec in (bfb.FP64, bfb.FP32):
@@ -87,7 +87,7 @@ def test_config2_full_fp32_vs_fp64(bfb):
     linf, l2 = envs[bfb.FP32].compare(envs[bfb.FP64])
     f32, f64 = envs[bfb.FP32].get_field(), envs[bfb.FP64].get_field()
     per = [float(np.abs(f32[..., d] - f64[..., d]).max() / np.abs(f64[..., d]).max()) for d in range(8)]
-    print(f"\nconfig 2 (200^3 x 8, 100k agents, 500 steps): FP32 vs FP64 rel Linf {linf:.3e}, rel L2 {l2:.3e}; "
+    print(f"\nagents workload (200^3 x 8, 100k agents, 500 steps): FP32 vs FP64 rel Linf {linf:.3e}, rel L2 {l2:.3e}; "
           f"per substrate rel Linf {['%.1e' % v for v in per]}")
     assert linf <= FP32_TOL
 
@@ -111,8 +111,8 @@ def blobs_field(torch, n, S, seed):
     return f
 
 
-def test_config3_full_fp32_vs_fp64_and_mass(bfb):
-    """Config 3: 512^3 x 4 (4.3 GB FP64), D {1e3,1e4,1e5,1e5}, lambda
+def test_blobs_512cube_s4_fp32_vs_fp64_and_mass(bfb):
+    """Gaussian blobs: 512^3 x 4 (4.3 GB FP64), D {1e3,1e4,1e5,1e5}, lambda
     {0.01,0.1,1,0.001}, 1000 steps, blobs + noise, no Dirichlet."""
     import torch
 
@@ -138,7 +138,7 @@ def test_config3_full_fp32_vs_fp64_and_mass(bfb):
     exact = m0 * (1.0 + dt * lam / 3.0) ** (-3 * steps)  # no Dirichlet: 1^T A = (1 + c2) 1^T per sweep
     drift64 = np.abs(envs[bfb.FP64].checksum() / exact - 1.0)
     drift32 = np.abs(envs[bfb.FP32].checksum() / exact - 1.0)
-    print(f"\nconfig 3 (512^3 x 4, 1000 steps): FP32 vs FP64 rel Linf {linf:.3e}, rel L2 {l2:.3e}; "
+    print(f"\nGaussian blobs (512^3 x 4, 1000 steps): FP32 vs FP64 rel Linf {linf:.3e}, rel L2 {l2:.3e}; "
           f"mass drift vs exact decay FP64 {['%.1e' % v for v in drift64]}, FP32 {['%.1e' % v for v in drift32]} "
           f"(remaining mass fraction {['%.1e' % v for v in exact / m0]})")
     assert linf <= FP32_TOL

@@ -42,8 +42,8 @@ def make_env(bfb, rho, D, lam, prec, dx=20.0, tma=1):
 # golden fixtures made by the reference
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("via", ["diffusion_step", "simulate"])
-def test_config1_golden(bfb, via):
-    g = golden("config1_15cube")
+def test_lod_15cube_golden(bfb, via):
+    g = golden("lod_15cube_s1_dirichlet")
     env = make_env(bfb, g["rho0"], g["D"], g["lam"], bfb.FP64, float(g["dx"]))
     env.set_dirichlet_uniform([1], g["dir_value"])
     steps, dt = int(g["steps"]), float(g["dt"])
@@ -118,8 +118,8 @@ def test_agents_golden(bfb):
 # ---------------------------------------------------------------------------
 # against the oracle restatement
 # ---------------------------------------------------------------------------
-def test_config1_full_size_fp64(bfb, oracle):
-    """Config 1 exactly: 75^3 x 1, D=1e5, lambda=0.1, dt=0.01, 100 steps,
+def test_cube75_s1_full_size_fp64(bfb, oracle):
+    """The 75^3 single-substrate workload exactly: 75^3 x 1, D=1e5, lambda=0.1, dt=0.01, 100 steps,
     Dirichlet 1.0 on all faces, U[0,1) field from a seed."""
     rng = np.random.default_rng(2024)
     rho0 = rng.random((75, 75, 75, 1))
@@ -310,9 +310,9 @@ def test_mass_balance_full_size(bfb, rng):
 
 
 def test_fp32_vs_fp64_full_size_1000_steps(bfb, rng):
-    """The north-star precision target: FP32 within 1e-5 relative L-inf of
+    """The FP32 precision target: FP32 within 1e-5 relative L-inf of
     the FP64 path (itself bit-exact with the reference) after 1000 steps at
-    256^3 x 8 (D, lambda log-uniform as in config 2, U[0,1) field)."""
+    256^3 x 8 (D, lambda log-uniform as in the 200^3 x 8 agents workload, U[0,1) field)."""
     S = 8
     D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
     rho0 = rng.random((256, 256, 256, S))

@@ -21,8 +21,8 @@ def golden(name):
     return dict(np.load(GOLD / f"{name}.npz"))
 
 
-def test_config1_golden_bitexact(oracle):
-    g = golden("config1_15cube")
+def test_lod_15cube_golden_bitexact(oracle):
+    g = golden("lod_15cube_s1_dirichlet")
     S = 1
     vals = np.broadcast_to(np.asarray(g["dir_value"], float), g["rho0"].shape)
     out = oracle.lod_steps(g["rho0"], float(g["dt"]), float(g["dx"]), g["D"], g["lam"], int(g["steps"]),

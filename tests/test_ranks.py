@@ -26,7 +26,7 @@ def load_ranks():
     return mod
 
 
-def config4_weights(seed=4, n=256):
+def ensemble_weights(seed=4, n=256):
     """Field bytes of a config-4-like ensemble: edges U{32..160} per axis, 1-6 substrates, FP32."""
     rng = np.random.default_rng(seed)
     ranks = load_ranks()
@@ -35,7 +35,7 @@ def config4_weights(seed=4, n=256):
 
 def test_shard_is_a_balanced_partition():
     ranks = load_ranks()
-    w = config4_weights()
+    w = ensemble_weights()
     for world in (1, 2, 3, 4, 8):
         owner = ranks.shard_instances(w, world)
         assert sorted(set(owner)) == list(range(min(world, len(w))))
@@ -73,7 +73,7 @@ def _rank_main(rank, world, port, q):
         import datetime
         dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
         ranks = load_ranks()
-        w = config4_weights()
+        w = ensemble_weights()
         # every rank derives the same partition without communicating
         owner = ranks.shard_instances(w, world)
         mine = ranks.local_instances(w, rank, world)
