@@ -116,6 +116,65 @@ def test_live_reference_non_multiple_domain_binning(oracle, rng):
     assert np.array_equal(np.where(ov < 0, 0, ov), e.agent_voxels())
 
 
+@needs_ref
+@pytest.mark.parametrize("solver", [0, 1], ids=["LOD_3D", "LOD_3D_AVX256D"])
+@pytest.mark.parametrize("shape,S", [((6, 5, 7), 3), ((4, 9, 3), 5), ((7, 4, 6), 8), ((3, 3, 12), 1)])
+def test_live_reference_both_solvers_bitexact(oracle, rng, solver, shape, S):
+    """Both reference solvers (BioFVM_parallel.cpp:693-1395 and its AVX2 form
+    :1411-2326, whose factor tables are replicated to lcm(S, 4) entries) give
+    the oracle's bits, for S below, above and at a multiple of 4, with
+    per-voxel Dirichlet values on a random subset of substrates."""
+    ref = RefLib()
+    dx, dt = 20.0, 0.01
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    e = RefEnv(ref, (0, 0, 0, *(np.array(shape) * dx)), dx, D, lam)
+    e.set_solver(solver)
+    rho0 = rng.random(e.shape) * 5
+    act = (rng.random(S) < 0.5).astype(np.uint8)
+    vals = rng.random(e.shape) * 10
+    e.set_field(rho0)
+    e.set_dirichlet(act, face_values=vals)
+    e.step(dt, 4)
+    out = oracle.lod_steps(rho0, dt, dx, D, lam, 4, vals, face_mask_all(act))
+    assert np.array_equal(out, e.field())
+
+
+@needs_ref
+def test_live_reference_bulk_diffusion_agents_bitexact(oracle, rng):
+    """A step order of the reference's drivers (examples/3D_tumor_example_X.cpp
+    346-348: bulk sources and sinks, diffusion, then the agents), on random
+    rates with many agents per voxel, so the list-ordered per-voxel update
+    (BioFVM_basic_agent.cpp:279-300) is exercised; bit-exact for 3 steps."""
+    ref = RefLib()
+    shape, S, dx, dt = (8, 7, 6), 3, 20.0, 0.01
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    box = (0.0, 0.0, 0.0, *(np.array(shape) * dx))
+    e = RefEnv(ref, box, dx, D, lam)
+    rho0 = rng.random(e.shape) * 4
+    e.set_field(rho0)
+    e.set_dirichlet([0] * S)
+    S_rate, T_target, U_rate = (log_uniform(rng, 1e-2, 10.0, e.shape) for _ in range(3))
+    e.set_bulk(S_rate, T_target, U_rate)
+    n = 400  # in a 60 um cube: 27 voxels, ~15 agents per voxel
+    pos = rng.uniform(40.0, 100.0, (n, 3))
+    vol = log_uniform(rng, 1e2, 1e3, n)
+    sec, upt, sat = (log_uniform(rng, 1e-2, 10.0, (n, S)) for _ in range(3))
+    e.add_agents(pos, vol, sec, upt, sat, dt)
+    vox = oracle.bin_agents(pos, box, dx, shape)
+    assert (vox >= 0).all() and np.array_equal(vox, e.agent_voxels())
+    assert np.bincount(vox).max() >= 10
+    t1, t2 = oracle.agent_constants(dt, dx, vol, sec, upt, sat)
+    rho = rho0
+    for _ in range(3):
+        e.bulk_step(dt)
+        e.step(dt, 1)
+        e.cells_step(dt)
+        rho = oracle.bulk_step(rho, dt, S_rate, T_target, U_rate)
+        rho = oracle.lod_steps(rho, dt, dx, D, lam, 1, None, np.zeros((6, S), np.uint8))
+        rho = oracle.cells_step(rho, vox, t1, t2)
+    assert np.array_equal(rho, e.field())
+
+
 def test_adjoint_oracle_matches_finite_differences(oracle, rng):
     shape, S = (4, 3, 5), 2
     dx, dt = 20.0, 0.01
