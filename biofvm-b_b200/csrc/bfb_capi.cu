@@ -358,7 +358,7 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
     *out = nullptr;
     if (nx < 1 || ny < 1 || nz < 1 || n_substrates < 1)
         return fail(BFB_ERR_SIZE, "grid sizes and substrate count must be >= 1");
-    if (!(dx > 0)) return fail(BFB_ERR_INVALID_ARG, "dx must be > 0");
+    if (!(dx > 0) || !std::isfinite(dx)) return fail(BFB_ERR_INVALID_ARG, "dx must be finite and > 0");
     if (precision != BFB_FP64 && precision != BFB_FP32) return fail(BFB_ERR_INVALID_ARG, "precision must be BFB_FP64 or BFB_FP32");
     const long long V = (long long)nx * ny * nz;
     if (V > 0x7fffffffLL) return fail(BFB_ERR_SIZE, "more than 2^31-1 voxels");
@@ -429,12 +429,19 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
 
 BFB_API int bfb_create_domain(bfb_env *out, double x0, double x1, double y0, double y1, double z0, double z1,
                               double dx, int n_substrates, int precision, int device) {
-    if (!(dx > 0)) return fail(BFB_ERR_INVALID_ARG, "dx must be > 0");
-    // BioFVM_parallel.cpp:100-102
+    if (!out) return fail(BFB_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (!(dx > 0) || !std::isfinite(dx)) return fail(BFB_ERR_INVALID_ARG, "dx must be finite and > 0");
+    // BioFVM_parallel.cpp:100-102; counts outside int range (or from non-finite
+    // extents) are rejected before the conversion
     const double eps = 1e-16;
-    const int nx = (int)std::ceil(eps + (x1 - x0) / dx);
-    const int ny = (int)std::ceil(eps + (y1 - y0) / dx);
-    const int nz = (int)std::ceil(eps + (z1 - z0) / dx);
+    const double cx = std::ceil(eps + (x1 - x0) / dx), cy = std::ceil(eps + (y1 - y0) / dx),
+                 cz = std::ceil(eps + (z1 - z0) / dx);
+    for (double c : {cx, cy, cz})
+        if (!(c >= 1.0 && c <= 2147483647.0))
+            return fail(BFB_ERR_SIZE, "domain extents must be finite with x1 >= x0, y1 >= y0, z1 >= z0 and give "
+                                      "at most 2^31-1 voxels per axis");
+    const int nx = (int)cx, ny = (int)cy, nz = (int)cz;
     int st = bfb_create(out, nx, ny, nz, n_substrates, dx, precision, device);
     if (st) return st;
     bfb_env_s *env = *out;
