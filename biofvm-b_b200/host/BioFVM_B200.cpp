@@ -156,17 +156,25 @@ int Microenvironment::find_density_index(const std::string &nm) const {
 
 void Microenvironment::resize_space_uniform(double x0, double x1, double y0, double y1, double z0, double z1,
                                             double dx, int *dims, int *coords) {
+    resize_space(x0, x1, y0, y1, z0, z1, dx, dx, dx, dims, coords);
+}
+
+void Microenvironment::resize_space(double x0, double x1, double y0, double y1, double z0, double z1, double dx,
+                                    double dy, double dz, int *dims, int *coords) {
     if (dims && (dims[0] * dims[1] * dims[2] != 1))
         std::cout << "BioFVM-B200: one device-resident grid per process; dims are ignored" << std::endl;
     (void)coords;
     // Cartesian_Mesh::resize (BioFVM_parallel.cpp:71-160) at one rank
     const double eps = 1e-16;
     mesh.x_size = (int)std::ceil(eps + (x1 - x0) / dx);
-    mesh.y_size = (int)std::ceil(eps + (y1 - y0) / dx);
-    mesh.z_size = (int)std::ceil(eps + (z1 - z0) / dx);
-    mesh.dx = mesh.dy = mesh.dz = dx;
-    mesh.dV = dx * dx * dx;
-    mesh.uniform_mesh = true;
+    mesh.y_size = (int)std::ceil(eps + (y1 - y0) / dy);
+    mesh.z_size = (int)std::ceil(eps + (z1 - z0) / dz);
+    mesh.dx = dx;
+    mesh.dy = dy;
+    mesh.dz = dz;
+    mesh.dV = dx * dy * dz;
+    const double tol = 1e-16;  // BioFVM_parallel.cpp:124-127
+    mesh.uniform_mesh = !(std::fabs(dx - dy) > tol || std::fabs(dy - dz) > tol || std::fabs(dx - dz) > tol);
     mesh.bounding_box[0] = x0;
     mesh.bounding_box[1] = y0;
     mesh.bounding_box[2] = z0;
@@ -177,8 +185,8 @@ void Microenvironment::resize_space_uniform(double x0, double x1, double y0, dou
     mesh.y_coordinates.resize(mesh.y_size);
     mesh.z_coordinates.resize(mesh.z_size);
     for (int i = 0; i < mesh.x_size; ++i) mesh.x_coordinates[i] = x0 + (i + 0.5) * dx;
-    for (int i = 0; i < mesh.y_size; ++i) mesh.y_coordinates[i] = y0 + (i + 0.5) * dx;
-    for (int i = 0; i < mesh.z_size; ++i) mesh.z_coordinates[i] = z0 + (i + 0.5) * dx;
+    for (int i = 0; i < mesh.y_size; ++i) mesh.y_coordinates[i] = y0 + (i + 0.5) * dy;
+    for (int i = 0; i < mesh.z_size; ++i) mesh.z_coordinates[i] = z0 + (i + 0.5) * dz;
     const size_t N = (size_t)number_of_voxels() * number_of_densities();
     field_.assign(N, 0.0);
     dirichlet_value_vectors.assign(N, 100.0);  // BioFVM_parallel.cpp:56
@@ -264,6 +272,10 @@ void Microenvironment::set_precision(Precision p) {
 
 int Microenvironment::ensure_device() {
     if (env_) return BFB_OK;
+    if (!mesh.uniform_mesh) {
+        std::cout << "BioFVM-B200: the device grid needs a uniform mesh (dx = dy = dz)" << std::endl;
+        return BFB_ERR_UNSUPPORTED;
+    }
     const double *bb = mesh.bounding_box;
     int st = bfb_create_domain(&env_, bb[0], bb[3], bb[1], bb[4], bb[2], bb[5], mesh.dx, number_of_densities(),
                                (int)precision_, 0);
@@ -373,6 +385,19 @@ std::vector<double> Microenvironment::checksum() {
     if (!st) st = bfb_checksum(env_, out.data());
     report(st, "checksum");
     return out;
+}
+
+bool Microenvironment::compare_microenvironment(Microenvironment &reference) {
+    if (mesh.x_coordinates.size() != reference.mesh.x_coordinates.size() ||
+        mesh.y_coordinates.size() != reference.mesh.y_coordinates.size() ||
+        mesh.z_coordinates.size() != reference.mesh.z_coordinates.size())
+        return false;
+    if (number_of_densities() != reference.number_of_densities()) return false;
+    sync_to_host();
+    reference.sync_to_host();
+    for (size_t n = 0; n < field_.size(); ++n)
+        if (field_[n] != reference.field_[n]) return false;
+    return true;
 }
 
 void Microenvironment::apply_dirichlet_conditions(int rank, int size) {

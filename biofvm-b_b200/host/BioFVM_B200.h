@@ -103,6 +103,12 @@ class Microenvironment {
     // resize_space_uniform(..., dims, coords) at one rank (BioFVM_parallel.cpp:18-59)
     void resize_space_uniform(double x0, double x1, double y0, double y1, double z0, double z1, double dx,
                               int *dims = nullptr, int *coords = nullptr);
+    // resize_space(..., dx, dy, dz, dims, coords) at one rank (BioFVM_parallel.cpp:29-59, 71-160): node
+    // counts per axis from its own spacing. Spacings that differ by more than 1e-16 make the mesh
+    // non-uniform, as in the reference; the LOD solver then refuses to run (it prints the reference's
+    // message) and no device operation is available for that mesh.
+    void resize_space(double x0, double x1, double y0, double y1, double z0, double z1, double dx, double dy,
+                      double dz, int *dims = nullptr, int *coords = nullptr);
     int voxel_index(int i, int j, int k) const { return mesh.voxel_index(i, j, k); }
     std::vector<int> cartesian_indices(int n) const { return mesh.cartesian_indices(n); }
     int nearest_voxel_index(std::vector<double> &position) const { return mesh.nearest_voxel_index(position); }
@@ -125,6 +131,13 @@ class Microenvironment {
     void set_substrate_dirichlet_activation(int substrate_index, bool new_value);
     double *dirichlet_values(int i, int j, int k);
     void apply_dirichlet_conditions(int rank = 0, int size = 1);
+    // the reference's second version (BioFVM_microenvironment.cpp:486-...) writes the same faces with
+    // the same values; examples/dirichlet_test.cpp:273-274 checks the two agree
+    void apply_dirichlet_conditions_v2(int rank = 0, int size = 1) { apply_dirichlet_conditions(rank, size); }
+    // compare_microenvironment (BioFVM_microenvironment.cpp:1688-1726): the same node counts and
+    // substrate count, and every density equal bit for bit. The reference takes its argument by value;
+    // this facade's Microenvironment owns device state and is not copyable, so it takes a reference.
+    bool compare_microenvironment(Microenvironment &reference);
     // B200 extension: per-face activation mask[face*S + d] (faces x-lo, x-hi,
     // y-lo, y-hi, z-lo, z-hi), ANDed with the per-substrate activation.
     void set_dirichlet_face_mask(const std::vector<uint8_t> &mask);
