@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <fstream>
 #include <iostream>
 
 namespace BioFVM_B200 {
@@ -82,6 +83,7 @@ Microenvironment::Microenvironment() {
     dirichlet_value_vectors.assign(1, 1.0);
     dirichlet_activation_vector.assign(1, true);
     diffusion_decay_solver = diffusion_decay_solver__constant_coefficients_LOD_3D_B200;
+    print_voxels_densities = &BioFVM_B200::print_voxels_densities;
     bulk_supply_rate_function = zero_function;
     bulk_supply_target_densities_function = zero_function;
     bulk_uptake_rate_function = zero_function;
@@ -385,6 +387,33 @@ std::vector<double> Microenvironment::checksum() {
     if (!st) st = bfb_checksum(env_, out.data());
     report(st, "checksum");
     return out;
+}
+
+void Microenvironment::print_result(double dt, int mpi_Size, int mpi_Rank, int *mpi_Coords, std::string *file_name,
+                                    int *mpi_Dims, MPI_Comm comm) {
+    if (print_voxels_densities) print_voxels_densities(*this, dt, mpi_Size, mpi_Rank, mpi_Coords, file_name, mpi_Dims, comm);
+}
+
+void print_voxels_densities(Microenvironment &M, double dt, int size, int rank, int *coords, std::string *file_name,
+                            int *dims, MPI_Comm comm) {
+    (void)dt;
+    (void)coords;
+    (void)dims;
+    (void)comm;
+    if (size != 1) std::cout << "BioFVM-B200: one grid per process; the densities are written once" << std::endl;
+    M.sync_to_host();
+    const std::vector<double> &f = *M.p_density_vectors;
+    const int S = M.number_of_densities();
+    std::ofstream out(*file_name, std::ios::app);
+    size_t index = 0;
+    for (int i = 0; i < M.mesh.x_size; i++)
+        for (int j = 0; j < M.mesh.y_size; j++)
+            for (int k = 0; k < M.mesh.z_size; k++) {
+                out << (M.mesh.x_coordinates.size() * rank) + i << " " << j << " " << k << " : ";
+                for (int d = 0; d < S; ++d) out << f[index++] << " ";
+                out << std::endl;
+            }
+    out << std::flush;
 }
 
 bool Microenvironment::compare_microenvironment(Microenvironment &reference) {

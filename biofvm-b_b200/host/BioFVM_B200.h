@@ -165,6 +165,11 @@ class Microenvironment {
     void display_information(std::ostream &os);
     // MATLAB v4 snapshot (BioFVM_microenvironment.cpp:1079-1107), packed on the device
     void write_to_matlab(std::string filename);
+    // print_result (BioFVM_microenvironment.cpp:375-379) calls the print_voxels_densities hook, which
+    // drivers set to the free function below (examples/test_VS.cpp:241); here it is set by default.
+    void (*print_voxels_densities)(Microenvironment &, double, int, int, int *, std::string *, int *, MPI_Comm);
+    void print_result(double dt, int mpi_Size, int mpi_Rank, int *mpi_Coords, std::string *file_name,
+                      int *mpi_Dims, MPI_Comm comm);
     void write_to_matlab(std::string filename, int rank, int size, MPI_Comm comm) {
         (void)rank;
         (void)size;
@@ -268,6 +273,11 @@ void delete_basic_agent(Basic_Agent *p);
 
 Microenvironment *get_default_microenvironment();
 void set_default_microenvironment(Microenvironment *M);
+
+// print_voxels_densities (BioFVM_parallel.cpp:2334-2366) at one rank: appends one line per voxel,
+// "i j k : d0 d1 ... ", in (i, j, k) order with default stream formatting, to *file_name.
+void print_voxels_densities(Microenvironment &M, double dt, int size, int rank, int *coords, std::string *file_name,
+                            int *dims, MPI_Comm comm);
 
 }  // namespace BioFVM_B200
 

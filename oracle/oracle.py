@@ -212,6 +212,7 @@ class RefLib:
         L.ref_cells_step.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.ref_gradients.argtypes = [ctypes.c_void_p, _dp]
         L.ref_write_matlab.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.ref_print_densities.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.ref_gradients_per_voxel.argtypes = [ctypes.c_void_p, _dp]
 
 
@@ -290,6 +291,10 @@ class RefEnv:
 
     def write_matlab(self, filename):
         self.ref.lib.ref_write_matlab(self.h, str(filename).encode())
+
+    def print_densities(self, filename):
+        """The text dump of print_result / print_voxels_densities (appends)."""
+        self.ref.lib.ref_print_densities(self.h, str(filename).encode())
 
     def gradients(self, per_voxel=False):
         """(nx, ny, nz, S, 3) gradient vectors from compute_all_gradient_vectors,

@@ -229,6 +229,17 @@ void ref_write_matlab(void *h, const char *filename) {
     M->write_to_matlab(std::string(filename));
 }
 
+// The text dump drivers write through print_result with the
+// print_voxels_densities hook (BioFVM_microenvironment.cpp:375-379,
+// BioFVM_parallel.cpp:2334-2366), at rank 0 of 1; appends to filename.
+void ref_print_densities(void *h, const char *filename) {
+    Microenvironment *M = (Microenvironment *)h;
+    int coords[3] = {0, 0, 0}, dims[3] = {1, 1, 1};
+    std::string name(filename);
+    M->print_voxels_densities = print_voxels_densities;
+    M->print_result(0.0, 1, 0, coords, &name, dims, MPI_COMM_WORLD);
+}
+
 // compute_all_gradient_vectors (BioFVM_microenvironment.cpp:1243-1402), then
 // the public accessor gradient_vector(n) per voxel: out[(n*S + q)*3 + c]. The
 // jumps it uses are set by the first solver call, so call ref_step first.

@@ -1,10 +1,12 @@
 // Host-only checks of the C++ facade; no device call is made, so it runs
 // without a GPU. Covers the mesh resize overloads (node counts, centres,
 // voxel volume, the uniform-mesh test of BioFVM_parallel.cpp:124-127),
-// compare_microenvironment (BioFVM_microenvironment.cpp:1688-1726) and the
-// LOD solver's refusal of a non-uniform mesh. Built and run by
+// compare_microenvironment (BioFVM_microenvironment.cpp:1688-1726), the
+// LOD solver's refusal of a non-uniform mesh and, given a file name, the
+// text dump of print_result (BioFVM_parallel.cpp:2334-2366). Built and run by
 // tests/test_facade_cpu.py; prints "ok" and exits 0 when every check holds.
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "BioFVM_B200.h"
@@ -19,7 +21,7 @@ using namespace BioFVM_B200;
         }                                                                 \
     } while (0)
 
-int main() {
+int main(int argc, char **argv) {
     Microenvironment a, b;
     a.set_density(0, "oxygen", "mmHg", 1e5, 0.1);
     b.set_density(0, "oxygen", "mmHg", 1e5, 0.1);
@@ -58,6 +60,20 @@ int main() {
     e.simulate_diffusion_decay(0.01);  // prints the reference's message, computes nothing
     CHECK(e.density_vector(0)[0] == 2.0);
     CHECK(e.last_status() == 0);
+
+    // print_result's text dump of a 3 x 4 x 5 x 2 field v[n][d] = n * 0.1 + d / 7.0, appended to argv[1]
+    if (argc > 1) {
+        Microenvironment f;
+        f.set_density(0, "a", "u", 1e3, 0.1);
+        f.add_density("b", "u", 1e4, 0.2);
+        f.resize_space_uniform(0.0, 60.0, 0.0, 80.0, 0.0, 100.0, 20.0);
+        CHECK(f.number_of_voxels() == 60 && f.number_of_densities() == 2);
+        for (int n = 0; n < 60; ++n)
+            for (int d = 0; d < 2; ++d) f.density_vector(n)[d] = n * 0.1 + d / 7.0;
+        std::string name(argv[1]);
+        int coords[3] = {0, 0, 0}, dims[3] = {1, 1, 1};
+        f.print_result(0.01, 1, 0, coords, &name, dims, 0);
+    }
 
     std::printf("ok\n");
     return 0;
