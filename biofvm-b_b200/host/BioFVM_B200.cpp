@@ -634,6 +634,18 @@ void Basic_Agent::set_internal_uptake_constants(double dt) {
     volume_is_changed = false;
 }
 
+double *Basic_Agent::nearest_density_vector() {
+    return microenvironment ? microenvironment->nearest_density_vector(current_voxel_index) : nullptr;
+}
+
+std::vector<double> &Basic_Agent::nearest_gradient(int substrate_index) {
+    return microenvironment->gradient_vector(current_voxel_index)[substrate_index];
+}
+
+std::vector<std::vector<double>> &Basic_Agent::nearest_gradient_vector() {
+    return microenvironment->gradient_vector(current_voxel_index);
+}
+
 void Basic_Agent::simulate_secretion_and_uptake(Microenvironment *M, double dt) {
     if (!is_active) return;
     if (volume_is_changed) set_internal_uptake_constants(dt);

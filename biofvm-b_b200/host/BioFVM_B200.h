@@ -255,6 +255,13 @@ class Basic_Agent {
     void simulate_secretion_and_uptake(Microenvironment *M, double dt);
     int get_current_voxel_index() const { return current_voxel_index; }
     bool active() const { return is_active; }
+    // BioFVM_basic_agent.cpp:250-266: the densities / gradients at the agent's voxel of its
+    // microenvironment (gradients as Microenvironment::gradient_vector gives them)
+    double *nearest_density_vector();
+    std::vector<double> &nearest_gradient(int substrate_index);
+    std::vector<std::vector<double>> &nearest_gradient_vector();
+    std::vector<double> velocity;
+    void update_position(double dt) { (void)dt; }  // a stub in the reference too (BioFVM_basic_agent.cpp:92-94)
 
    private:
     Microenvironment *microenvironment = nullptr;

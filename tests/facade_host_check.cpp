@@ -61,6 +61,16 @@ int main(int argc, char **argv) {
     CHECK(e.density_vector(0)[0] == 2.0);
     CHECK(e.last_status() == 0);
 
+    // an agent's nearest densities are its voxel's (BioFVM_basic_agent.cpp:250-253)
+    {
+        Basic_Agent *ag = create_basic_agent();
+        ag->register_microenvironment(&a);
+        ag->assign_position(45.0, 30.0, 5.0);  // voxel (2, 1, 1) of a's 5 x 4 x 3 grid
+        CHECK(ag->get_current_voxel_index() == a.voxel_index(2, 1, 1));
+        CHECK(ag->nearest_density_vector() == a.density_vector(a.voxel_index(2, 1, 1)));
+        delete_basic_agent(ag);
+    }
+
     // print_result's text dump of a 3 x 4 x 5 x 2 field v[n][d] = n * 0.1 + d / 7.0, appended to argv[1]
     if (argc > 1) {
         Microenvironment f;
