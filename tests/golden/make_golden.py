@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory by running the REFERENCE
 BioFVM-B library, compiled from its own sources (oracle/Makefile `ref`).
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [out_dir]
 
 Every case uses seeded inputs; the outputs are what the reference computes.
 The committed .npz files let the oracle restatement and the GPU path be
@@ -109,9 +109,9 @@ def case_agents(ref):
                 voxels=vox, bbox=np.array(box, dtype=float))
 
 
-def main():
-    ref = RefLib()
-    cases = {
+def make_cases(ref):
+    """Every fixture's arrays, computed by the reference library `ref`."""
+    return {
         "lod_15cube_s1_dirichlet": case_lod_15cube_dirichlet(ref),
         "multi_7x5x9_S3": case_multi(ref, 21, (7, 5, 9), 3, 6),
         "multi_1x4x6_S2": case_multi(ref, 22, (1, 4, 6), 2, 4),
@@ -120,10 +120,13 @@ def main():
         "bulk_9x8x7_S3": case_bulk(ref),
         "agents_12x10x9_S2": case_agents(ref),
     }
-    for name, data in cases.items():
-        np.savez_compressed(HERE / f"{name}.npz", **{k: np.asarray(v) for k, v in data.items()})
+
+
+def main(out_dir: Path = HERE):
+    for name, data in make_cases(RefLib()).items():
+        np.savez_compressed(Path(out_dir) / f"{name}.npz", **{k: np.asarray(v) for k, v in data.items()})
         print("wrote", name)
 
 
 if __name__ == "__main__":
-    main()
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else HERE)

@@ -89,6 +89,24 @@ def test_live_reference_bitexact(oracle, rng, shape, S):
 
 
 @needs_ref
+def test_golden_fixtures_reproduce_from_the_reference():
+    """The committed fixtures are what the reference library computes today:
+    tests/golden/make_golden.py's cases, rerun, give the same arrays."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_golden", GOLD / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    cases = mg.make_cases(RefLib())
+    assert sorted(cases) == sorted(p.stem for p in GOLD.glob("*.npz"))
+    for name, data in cases.items():
+        g = golden(name)
+        assert sorted(g) == sorted(data), name
+        for k, v in data.items():
+            assert np.array_equal(np.asarray(v), g[k]), (name, k)
+
+
+@needs_ref
 def test_live_reference_default_dirichlet_is_100(oracle):
     """dirichlet_test's 'should be 100' (examples/dirichlet_test.cpp:277): after
     resize the reference's Dirichlet value is 100.0 with activation true."""
