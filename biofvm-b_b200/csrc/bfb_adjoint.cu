@@ -1244,6 +1244,7 @@ extern "C" BFB_API int bfb_adjoint_run(bfb_env env, double dt, int n_steps, int 
                                        double *dL_dsaturation) {
     if (!env) return fail(BFB_ERR_INVALID_ARG, "null bfb_env");
     if (n_steps < 1 || checkpoint_every < 1 || !(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "bad dt, n_steps or K");
+    NvtxRange range("bfb_adjoint_run");
     if (!dL_dfinal) return fail(BFB_ERR_INVALID_ARG, "dL_dfinal is NULL");
     if (!(flags & BFB_STEP_DIFFUSION) || (flags & ~(BFB_STEP_DIFFUSION | BFB_STEP_CELLS)))
         return fail(BFB_ERR_UNSUPPORTED, "adjoint: flags must be BFB_STEP_DIFFUSION [| BFB_STEP_CELLS]");

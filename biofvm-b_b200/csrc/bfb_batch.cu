@@ -720,6 +720,7 @@ BFB_API int bfb_batch_simulate(bfb_batch b, double dt, int n_steps, int flags) {
     if (!(flags & BFB_STEP_DIFFUSION) || (flags & ~(BFB_STEP_DIFFUSION | BFB_STEP_CELLS)))
         return fail(BFB_ERR_UNSUPPORTED, "batch: flags must be BFB_STEP_DIFFUSION [| BFB_STEP_CELLS]");
     BFB_CUDA(cudaSetDevice(b->device));
+    NvtxRange range("bfb_batch_simulate");
     // every env's factors, Dirichlet faces and agents as bfb_simulate would use them
     bool changed = b->graph_flags != flags || b->graph_dt != dt || b->graph_epochs.size() != b->envs.size();
     for (int k = 0; k < b->n; ++k) {

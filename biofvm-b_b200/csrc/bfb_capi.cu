@@ -827,6 +827,7 @@ BFB_API int bfb_simulate(bfb_env env, double dt, int n_steps, int flags) {
     if (flags & BFB_STEP_DIFFUSION)
         if ((st = ensure_factors(env, dt))) return st;
     if (n_steps == 0) return BFB_OK;
+    NvtxRange range("bfb_simulate");
     if (!env->use_graphs || env->stream == nullptr) return run_steps_any(env, dt, n_steps, flags, env->stream);
     // One step captured as a graph, replayed n_steps times.
     if (!env->graph_exec || env->graph_flags != flags || env->graph_dt != dt || env->graph_epoch != env->epoch) {
@@ -859,6 +860,7 @@ BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_step
     if (st) return st;
     if (!host_field) return fail(BFB_ERR_INVALID_ARG, "host_field is NULL");
     if ((st = ensure_factors(env, dt))) return st;
+    NvtxRange range("bfb_step_host");
     cudaStream_t s = env->stream;
     if (env->precision == BFB_FP64) {
         BFB_CUDA(cudaMemcpyAsync(env->field, host_field, sizeof(double) * env->N, cudaMemcpyHostToDevice, s));
@@ -1018,7 +1020,9 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
     cudaStream_t s = env->stream;
     cudaEvent_t ev[BFB_PROFILE_PHASES + 1];
     for (auto &e : ev) BFB_CUDA(cudaEventCreate(&e));
+    static const char *const kPhaseNames[BFB_PROFILE_PHASES] = {"sweep_x", "sweep_y", "sweep_z", "bulk", "cells"};
     auto phase_ms = [&](int ph, auto &&launch) -> int {
+        NvtxRange range(kPhaseNames[ph]);
         BFB_CUDA(cudaEventRecord(ev[0], s));
         int r = launch();
         if (r) return r;

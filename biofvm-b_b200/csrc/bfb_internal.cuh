@@ -7,9 +7,22 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "biofvm_b200.h"
 
 namespace bfb {
+
+// An NVTX range over a host scope: one per entry point that launches work and
+// one per phase in bfb_profile_steps, so that profilers recording NVTX (ncu's
+// --nvtx filters) can select them. Without a profiler attached the calls do
+// nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ---------------------------------------------------------------------------
 // Error plumbing: every C entry point returns a status and records a message.
