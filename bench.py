@@ -188,6 +188,17 @@ def cpu_reference_run(max_seconds, min_steps=1, steps=None, warmup=1):
     return best
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), for the baseline's record."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_port_run(max_seconds):
     """Fallback when the reference is not built: our oracle port, 1 thread,
     on a 64^3 x 8 sample of the workload."""
@@ -233,7 +244,7 @@ def run_reference_arm(args):
         "warmup": warm, "ms_per_step": el / n * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded U[0,1) field, log-uniform D/lambda)",
         "config": config({"solver": name, "threads": threads, "ranks": "1 rank x N threads (MPI unavailable)"}),
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "cpu": cpu_model(),
                          "sample": f"{n} of the {args.steps} requested full {NX}^3x{S} FP64 steps (capped at "
                                    f"{args.ref_seconds:.0f} s) after {warm} untimed steps (the first sets up the factors), "
                                    "best of LOD_3D / AVX256D"},
@@ -356,12 +367,12 @@ def run_our_arm(args):
         r = cpu_reference_run(args.cpu_seconds, min_steps=1)
         if r is not None:
             rate, n, threads, sname, el = r
-            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "cpu": cpu_model(),
                    "sample": f"{n} full {NX}^3x{S} FP64 steps ({el:.1f} s) of the reference {sname} "
                              "(faster of LOD_3D / AVX256D), after one factor-setup step"}
         else:
             rate, n = cpu_port_run(args.cpu_seconds)
-            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "cpu": cpu_model(),
                    "sample": f"{n} steps of a 64^3x8 sample with the oracle port (reference not built)"}
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warm,
