@@ -405,3 +405,129 @@ void orc_gradients(const double *rho, int nx, int ny, int nz, int S, double dx, 
                 }
             }
 }
+
+/* ---------------------------------------------------------------------------
+ * The product's FP32 path (orc_lod_steps_f32). Not a reference function: the
+ * reference has no FP32 solver. Restated from the CUDA line solver so that its
+ * results can be checked bit for bit and its error against FP64 predicted on
+ * the CPU. Every operation is a single IEEE binary32 operation: the file is
+ * compiled with -ffp-contract=off and fused steps call fmaf.
+ * ------------------------------------------------------------------------- */
+
+/* The tables of one axis as the host rounds them for the FP32 kernels:
+ * rh = RN32(r), rl = RN32(r - rh) with r = 1/den in FP64, a = RN32(c1/den),
+ * cb = RN32(c). */
+static void f32_tables(int n, int S, const double *den, const double *c, const double *c1, float *rh, float *rl,
+                       float *a, float *cb)
+{
+    for (int m = 0; m < n; ++m)
+        for (int d = 0; d < S; ++d) {
+            size_t q = (size_t)m * S + d;
+            double r = 1.0 / den[q];
+            rh[q] = (float)r;
+            rl[q] = (float)(r - (double)rh[q]);
+            a[q] = (float)(c1[d] / den[q]);
+            cb[q] = (float)c[q];
+        }
+}
+
+/* One line in the deviation form, xb = the line's row 1 (row 0 when n == 1):
+ *   p_0 = fma(d_0, rh_0, d_0*rl_0),  p_m = fma(a_m, p_(m-1), fma(d_m, rh_m, d_m*rl_m)),  d_m = x_m - xb
+ *   z_(n-1) = p_(n-1),  z_m = fma(-cb_m, z_(m+1), p_m)
+ *   out_m = fma(xb, gh, fma(xb, gl, z_m))        (xb*g + z with g = 1/(1+c2) as hi + lo) */
+static void thomas_line_f32(float *u, size_t start, size_t stride, int n, int S, int d, const float *rh,
+                            const float *rl, const float *a, const float *cb, float gh, float gl, float *p)
+{
+    const float xb = u[start + (size_t)(n > 1 ? 1 : 0) * stride];
+    for (int m = 0; m < n; ++m) {
+        const size_t q = (size_t)m * S + d;
+        const float dl = u[start + (size_t)m * stride] - xb;
+        const float w = fmaf(dl, rh[q], dl * rl[q]);
+        p[m] = m == 0 ? w : fmaf(a[q], p[m - 1], w);
+    }
+    float next = p[n - 1];
+    u[start + (size_t)(n - 1) * stride] = fmaf(xb, gh, fmaf(xb, gl, next));
+    for (int m = n - 2; m >= 0; --m) {
+        next = fmaf(-cb[(size_t)m * S + d], next, p[m]);
+        u[start + (size_t)m * stride] = fmaf(xb, gh, fmaf(xb, gl, next));
+    }
+}
+
+static void dirichlet_f32(float *rho, int nx, int ny, int nz, int S, const float *values, const uint8_t *face_mask)
+{
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int face = i == 0 || i == nx - 1 || j == 0 || j == ny - 1 || k == 0 || k == nz - 1;
+                if (!face) continue;
+                size_t base = (((size_t)i * ny + j) * nz + k) * S;
+                for (int d = 0; d < S; ++d) {
+                    int act = 0;
+                    for (int f = 0; f < 6 && !act; ++f)
+                        act = face_mask[f * S + d] && on_face(f, i, j, k, nx, ny, nz);
+                    if (act) rho[base + d] = values[base + d];
+                }
+            }
+}
+
+void orc_lod_steps_f32(float *rho, int nx, int ny, int nz, int S, double dt, double dx, const double *D,
+                       const double *lambda, int n_steps, const double *dir_values, const uint8_t *face_mask)
+{
+    const int ns[3] = {nx, ny, nz};
+    const size_t V = (size_t)nx * ny * nz;
+    int nmax = nx > ny ? nx : ny;
+    if (nz > nmax) nmax = nz;
+    double *den = malloc(sizeof(double) * (size_t)nmax * S), *c = malloc(sizeof(double) * (size_t)nmax * S);
+    double *c1 = malloc(sizeof(double) * S);
+    float *tab[3][4];
+    float *gh = malloc(sizeof(float) * S), *gl = malloc(sizeof(float) * S), *p = malloc(sizeof(float) * nmax);
+    float *vals = NULL;
+    orc_constant1(S, dt, dx, D, c1);
+    for (int ax = 0; ax < 3; ++ax) {
+        for (int t = 0; t < 4; ++t) tab[ax][t] = malloc(sizeof(float) * (size_t)ns[ax] * S);
+        orc_factors(ns[ax], S, dt, dx, D, lambda, den, c);
+        f32_tables(ns[ax], S, den, c, c1, tab[ax][0], tab[ax][1], tab[ax][2], tab[ax][3]);
+    }
+    for (int d = 0; d < S; ++d) {  /* g = 1/(1 + c2), c2 = dt*lambda/3, as hi + lo */
+        double c2 = lambda[d] * dt;
+        c2 /= 3.0;
+        const double g = 1.0 / (1.0 + c2);
+        gh[d] = (float)g;
+        gl[d] = (float)(g - (double)gh[d]);
+    }
+    if (dir_values && face_mask) {
+        vals = malloc(sizeof(float) * V * S);
+        for (size_t q = 0; q < V * S; ++q) vals[q] = (float)dir_values[q];
+    }
+    const size_t ij = (size_t)ny * nz * S, jj = (size_t)nz * S, kj = (size_t)S;
+    for (int step = 0; step < n_steps; ++step) {
+        if (vals) dirichlet_f32(rho, nx, ny, nz, S, vals, face_mask);
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k)
+                for (int d = 0; d < S; ++d)
+                    thomas_line_f32(rho, j * jj + k * kj + d, ij, nx, S, d, tab[0][0], tab[0][1], tab[0][2],
+                                    tab[0][3], gh[d], gl[d], p);
+        if (vals) dirichlet_f32(rho, nx, ny, nz, S, vals, face_mask);
+        for (int i = 0; i < nx; ++i)
+            for (int k = 0; k < nz; ++k)
+                for (int d = 0; d < S; ++d)
+                    thomas_line_f32(rho, i * ij + k * kj + d, jj, ny, S, d, tab[1][0], tab[1][1], tab[1][2],
+                                    tab[1][3], gh[d], gl[d], p);
+        if (vals) dirichlet_f32(rho, nx, ny, nz, S, vals, face_mask);
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j)
+                for (int d = 0; d < S; ++d)
+                    thomas_line_f32(rho, i * ij + j * jj + d, kj, nz, S, d, tab[2][0], tab[2][1], tab[2][2],
+                                    tab[2][3], gh[d], gl[d], p);
+        if (vals) dirichlet_f32(rho, nx, ny, nz, S, vals, face_mask);
+    }
+    for (int ax = 0; ax < 3; ++ax)
+        for (int t = 0; t < 4; ++t) free(tab[ax][t]);
+    free(den);
+    free(c);
+    free(c1);
+    free(gh);
+    free(gl);
+    free(p);
+    free(vals);
+}

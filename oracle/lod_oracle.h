@@ -5,8 +5,8 @@
  * and bench.py's cpu_baseline leg as the checker; the product library never
  * links or calls it.
  *
- * Parity is pinned: tests/test_oracle.py checks every function here bit-for-bit
- * against the reference library compiled from its own sources
+ * Parity is pinned: tests/test_oracle.py checks every restated reference
+ * function here bit-for-bit against the reference library compiled from its own sources
  * (oracle/_ref, see oracle/Makefile) and against the committed golden fixtures
  * in tests/golden/ that were produced by that library.
  *
@@ -79,6 +79,16 @@ void orc_lod_step_adjoint(const double *rho_in, double *lam, int nx, int ny, int
                           double dt, double dx, const double *D, const double *lambda,
                           const double *dir_values, const uint8_t *face_mask,
                           double *gD, double *gL);
+
+/* The product's FP32 path restated (not a reference function): n_steps LOD
+ * steps Dir, X, Dir, Y, Dir, Z, Dir on an FP32 field, with the reference's
+ * FP64 factors (orc_factors) rounded once into FP32 tables, and each line
+ * solved in the deviation form u - u_ref with the reciprocal 1/den carried as
+ * a hi + lo pair, in exactly the FP32 operations of the CUDA line solver.
+ * dir_values (V*S FP64, rounded to FP32 like the device face values) and
+ * face_mask (6*S) may both be NULL for no Dirichlet faces. */
+void orc_lod_steps_f32(float *rho, int nx, int ny, int nz, int S, double dt, double dx, const double *D,
+                       const double *lambda, int n_steps, const double *dir_values, const uint8_t *face_mask);
 
 #ifdef __cplusplus
 }

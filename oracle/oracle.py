@@ -73,6 +73,9 @@ class Oracle:
         L.orc_gradients.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]
         L.orc_lod_step_adjoint.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _up, _dp, _dp]
+        L.orc_lod_steps_f32.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp, ctypes.c_int,
+                                        _dp, _up]
 
     def factors(self, n, dt, dx, D, lam):
         D, lam = f64(D), f64(lam)
@@ -113,6 +116,22 @@ class Oracle:
         for _ in range(n_steps):
             self.lib.orc_lod_step(_d(rho), nx, ny, nz, S, _d(fx[0]), _d(fx[1]), _d(fy[0]), _d(fy[1]),
                                   _d(fz[0]), _d(fz[1]), _d(c1), _d(dv), _u(fm))
+        return rho
+
+    def lod_steps_f32(self, rho, dt, dx, D, lam, n_steps=1, dir_values=None, face_mask=None):
+        """The product's FP32 path restated (orc_lod_steps_f32): n LOD steps on
+        an FP32 field; rho (nx, ny, nz, S) is rounded to FP32 first, as the
+        device upload does. Returns float32."""
+        rho = np.ascontiguousarray(rho, dtype=np.float32).copy()
+        nx, ny, nz, S = rho.shape
+        D, lam = f64(D), f64(lam)
+        dv = None if dir_values is None else f64(np.broadcast_to(dir_values, rho.shape))
+        fm = None if face_mask is None else np.ascontiguousarray(face_mask, dtype=np.uint8)
+        if (dv is None) != (fm is None):
+            raise ValueError("dir_values and face_mask go together")
+        self.lib.orc_lod_steps_f32(rho.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nx, ny, nz, S, dt, dx,
+                                   _d(D), _d(lam), n_steps, None if dv is None else _d(dv),
+                                   None if fm is None else _u(fm))
         return rho
 
     def bulk_step(self, rho, dt, S_rate, T_target, U_rate):

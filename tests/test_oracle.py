@@ -308,3 +308,26 @@ def test_gradients_oracle_bitexact_with_reference(oracle, rng, shape, S):
         assert np.all(got[..., 2] == 0.0)
     assert np.array_equal(got, want)
     assert np.array_equal(e.gradients(per_voxel=True), want)
+
+
+@pytest.mark.parametrize("shape,S,steps", [((9, 7, 8), 3, 40), ((1, 5, 6), 2, 20), ((12, 1, 3), 1, 20),
+                                           ((2, 2, 9), 4, 30), ((16, 16, 16), 8, 100)])
+def test_fp32_restatement_tracks_the_fp64_oracle(oracle, rng, shape, S, steps):
+    """The FP32 path's C restatement (orc_lod_steps_f32: FP32 tables rounded
+    once from the reference's factors, deviation form, hi + lo reciprocal)
+    stays within 1e-5 relative L-inf of the FP64 oracle, the FP32 target, on
+    grids with one- and two-voxel axes and Dirichlet faces."""
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    rho0 = rng.random((*shape, S)) * 3
+    act = (rng.random(S) < 0.6).astype(np.uint8)
+    vals = rng.random((*shape, S)) * 5
+    r64 = oracle.lod_steps(rho0, 0.01, 20.0, D, lam, steps, vals, face_mask_all(act))
+    r32 = oracle.lod_steps_f32(rho0, 0.01, 20.0, D, lam, steps, vals, face_mask_all(act))
+    assert r32.dtype == np.float32
+    err = np.abs(r32.astype(np.float64) - r64).max() / np.abs(r64).max()
+    assert err <= 1e-5, err
+    # deterministic, and the Dirichlet faces carry the FP32-rounded values exactly
+    assert np.array_equal(r32, oracle.lod_steps_f32(rho0, 0.01, 20.0, D, lam, steps, vals, face_mask_all(act)))
+    if act.any():
+        d = int(np.argmax(act))
+        assert np.array_equal(r32[0, ..., d], vals[0, ..., d].astype(np.float32))
