@@ -219,6 +219,62 @@ def cpu_port_run(max_seconds):
 
 
 # ---------------------------------------------------------------------------
+# collectives between ranks: torch.distributed (NCCL on GPUs, gloo in the CPU
+# tests); each is a no-op in one process. The library's own ranks.py holds
+# only the partition of an ensemble's instances.
+# ---------------------------------------------------------------------------
+def _dist():
+    import torch.distributed as dist
+    return dist if dist.is_available() and dist.is_initialized() else None
+
+
+def rank_barrier(device=None):
+    """Barrier across ranks (a no-op in one process), then a device sync."""
+    import torch
+    dist = _dist()
+    if dist is not None:
+        dist.barrier()
+    if device is not None and device.type == "cuda":
+        torch.cuda.synchronize(device)
+
+
+def _all_reduce_scalar(x, op, device):
+    import torch
+    dist = _dist()
+    if dist is None:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def max_over_ranks(x, device=None):
+    """The maximum of x over all ranks: the timed region of a multi-GPU run is the slowest rank's."""
+    import torch.distributed as dist
+    return _all_reduce_scalar(x, dist.ReduceOp.MAX, device)
+
+
+def sum_over_ranks(x, device=None):
+    import torch.distributed as dist
+    return _all_reduce_scalar(x, dist.ReduceOp.SUM, device)
+
+
+def gather_by_instance(local_ids, local_values, n_instances, width, device=None):
+    """Every rank receives the [n_instances, width] array of per-instance
+    values (per-substrate checksums, for example), each row filled by the rank
+    that owns the instance; rows no rank owns stay 0. One all-reduce."""
+    import torch
+    buf = torch.zeros((n_instances, width), dtype=torch.float64, device=device)
+    for i, v in zip(local_ids, local_values):
+        row = torch.as_tensor(np.asarray(v, dtype=np.float64).reshape(-1)[:width], device=device)
+        buf[i, :row.numel()] = row
+    dist = _dist()
+    if dist is not None:
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM)  # every row has exactly one owner
+    return buf.cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
 def dist_setup(args):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -243,8 +299,9 @@ def run_reference_arm(args):
         "impl": "reference", "metric": metric_name(), "value": rate, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": warm, "ms_per_step": el / n * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded U[0,1) field, log-uniform D/lambda)",
-        "config": config({"solver": name, "threads": threads, "ranks": "1 rank x N threads (MPI unavailable)"}),
+        "config": config(),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "cpu": cpu_model(),
+                         "solver": name, "threads": threads, "ranks": "1 rank x N threads (MPI unavailable)",
                          "sample": f"{n} of the {args.steps} requested full {NX}^3x{S} FP64 steps (capped at "
                                    f"{args.ref_seconds:.0f} s) after {warm} untimed steps (the first sets up the factors), "
                                    "best of LOD_3D / AVX256D"},
@@ -270,14 +327,13 @@ def run_our_arm(args):
     D, lam, rng = coefficients()
     rho0 = initial_field(rng)
 
-    ranks = importlib.import_module("biofvm_b_b200.ranks")  # barrier and max over ranks (no-ops in one process)
     dev = torch.device("cuda", local)
 
     def barrier():
-        ranks.barrier(dev)
+        rank_barrier(dev)
 
-    def max_over_ranks(x):
-        return ranks.max_over_ranks(x, dev)
+    def slowest(x):
+        return max_over_ranks(x, dev)
 
     results = {}
     stream = torch.cuda.Stream()
@@ -300,7 +356,7 @@ def run_our_arm(args):
         env.simulate(DT, K, bfb.STEP_DIFFUSION)
         e1.record(stream)
         e1.synchronize()
-        ms = max_over_ranks(e0.elapsed_time(e1))
+        ms = slowest(e0.elapsed_time(e1))
         clk = clocks.stop() if name == "fp32" else None
         barrier()
         # per-kernel device time (events around every launch, same stream)
@@ -326,7 +382,7 @@ def run_our_arm(args):
         env.step_host_ptr(host.data_ptr(), DT, 1)
     e1.record(stream)
     e1.synchronize()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    ms_e2e = slowest(e0.elapsed_time(e1))
 
     # reverse mode on the same FP32 env: n_adj steps, with and without segment recompute
     n_adj = 20
@@ -342,7 +398,7 @@ def run_our_arm(args):
         env.adjoint_run(DT, n_adj, w.data_ptr(), checkpoint_every=Kc)
         e1.record(stream)
         e1.synchronize()
-        adj_ms[Kc] = max_over_ranks(e0.elapsed_time(e1))
+        adj_ms[Kc] = slowest(e0.elapsed_time(e1))
     env.close()
 
     if dist is not None:

@@ -58,7 +58,7 @@ EXPORTS = [
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
     "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_write_matlab", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_get_option", "bfb_batch_simulate",
     "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_batch_autotune", "bfb_adjoint_run",
-    "bfb_checksum_noalloc",
+    "bfb_checksum_noalloc", "bfb_watchdog_selftest", "bfb_host_register", "bfb_host_unregister",
 ]
 
 
@@ -93,6 +93,9 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_set_stream": [_vp, _vp],
         "bfb_set_option": [_vp, ctypes.c_int, ctypes.c_int],
         "bfb_synchronize": [_vp],
+        "bfb_watchdog_selftest": [_vp, ctypes.c_int],
+        "bfb_host_register": [_vp, ctypes.c_size_t],
+        "bfb_host_unregister": [_vp],
         "bfb_set_coefficients": [_vp, _dp, _dp],
         "bfb_set_field": [_vp, _vp],
         "bfb_get_field": [_vp, _vp],
@@ -157,6 +160,19 @@ def _f64(a):
 
 def _u8(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def host_register(a: np.ndarray):
+    """Page-lock a host array (bfb_host_register) so that field copies from and
+    to it run at pinned-memory speed; undo with host_unregister before the
+    array is freed."""
+    L = load_library()
+    _check(L.bfb_host_register(ctypes.c_void_p(a.ctypes.data), a.nbytes))
+
+
+def host_unregister(a: np.ndarray):
+    L = load_library()
+    _check(L.bfb_host_unregister(ctypes.c_void_p(a.ctypes.data)))
 
 
 class Env:
@@ -310,6 +326,11 @@ class Env:
 
     def synchronize(self):
         _check(self.L.bfb_synchronize(self.h))
+
+    def watchdog_selftest(self, polls=64):
+        """Queue one bounded wait that runs out (bfb_watchdog_selftest): the
+        env's error flag is set as a stalled copy would set it."""
+        _check(self.L.bfb_watchdog_selftest(self.h, polls))
 
     def profile_steps(self, dt, n, flags=STEP_DIFFUSION):
         """Milliseconds per phase over n steps: x, y, z, bulk, cells."""

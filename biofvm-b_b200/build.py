@@ -12,6 +12,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -40,12 +41,12 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     newest = max(p.stat().st_mtime for p in deps)
     if LIB.exists() and LIB.stat().st_mtime >= newest and not force:
         return LIB
-    objs = []
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-    for s in SOURCES:
-        o = obj_dir / (Path(s).stem + ".o")
-        _run([NVCC, *ARCH, *FLAGS, *extra, "-c", CSRC / s, "-o", o])
-        objs.append(o)
+    objs = [obj_dir / (Path(s).stem + ".o") for s in SOURCES]
+    # one nvcc per translation unit, in parallel
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as pool:
+        list(pool.map(lambda so: _run([NVCC, *ARCH, *FLAGS, *extra, "-c", CSRC / so[0], "-o", so[1]]),
+                      zip(SOURCES, objs)))
     _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs])
     build_host()
     return LIB

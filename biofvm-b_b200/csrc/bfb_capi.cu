@@ -338,7 +338,7 @@ using namespace bfb;
 
 // The device error flag is sticky: once a kernel's bounded wait ran out, the
 // env's field is not trustworthy and every later synchronize reports it.
-static int check_device_error(bfb_env_s *env) {
+int bfb::env_check_device_error(bfb_env_s *env) {
     int flag = 0;
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     BFB_CUDA(cudaMemcpy(&flag, env->d_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -523,7 +523,14 @@ BFB_API int bfb_set_option(bfb_env env, int option, int value) {
 BFB_API int bfb_synchronize(bfb_env env) {
     int st = check_env(env);
     if (st) return st;
-    return check_device_error(env);
+    return env_check_device_error(env);
+}
+
+BFB_API int bfb_watchdog_selftest(bfb_env env, int polls) {
+    int st = check_env(env);
+    if (st) return st;
+    if (polls < 1 || polls > (1 << 20)) return fail(BFB_ERR_INVALID_ARG, "polls must be in [1, 2^20]");
+    return launch_watchdog_probe(polls, env->d_err, env->stream);
 }
 
 BFB_API int bfb_set_coefficients(bfb_env env, const double *D, const double *lambda) {
@@ -568,7 +575,7 @@ BFB_API int bfb_get_field(bfb_env env, double *host) {
         if ((st = launch_convert_f2d((const float *)env->field, (double *)env->staging, env->N, env->stream))) return st;
         BFB_CUDA(cudaMemcpyAsync(host, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, env->stream));
     }
-    return check_device_error(env);
+    return env_check_device_error(env);
 }
 
 BFB_API int bfb_set_field_raw(bfb_env env, const void *host) {
@@ -585,8 +592,7 @@ BFB_API int bfb_get_field_raw(bfb_env env, void *host) {
     if (st) return st;
     if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
     BFB_CUDA(cudaMemcpyAsync(host, env->field, env->elem * env->N, cudaMemcpyDeviceToHost, env->stream));
-    BFB_CUDA(cudaStreamSynchronize(env->stream));
-    return BFB_OK;
+    return env_check_device_error(env);
 }
 
 // Device-to-device field transfer with precision conversion.
@@ -618,7 +624,7 @@ BFB_API int bfb_get_field_device(bfb_env env, void *dst, int dst_precision) {
     } else {
         if ((st = launch_convert_d2f((const double *)env->field, (float *)dst, env->N, env->stream))) return st;
     }
-    return check_device_error(env);
+    return env_check_device_error(env);
 }
 
 BFB_API int bfb_compare_fields(bfb_env test, bfb_env ref, double *out4) {
@@ -870,6 +876,9 @@ BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_step
         if ((st = launch_convert_d2f((const double *)env->staging, (float *)env->field, env->N, s))) return st;
     }
     if ((st = run_steps_any(env, dt, n_steps, BFB_STEP_DIFFUSION, s))) return st;
+    // a wait that ran out leaves the device field untrustworthy: report it and
+    // leave the caller's host field as it was
+    if ((st = env_check_device_error(env))) return st;
     if (env->precision == BFB_FP64) {
         BFB_CUDA(cudaMemcpyAsync(host_field, env->field, sizeof(double) * env->N, cudaMemcpyDeviceToHost, s));
     } else {
@@ -877,6 +886,18 @@ BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_step
         BFB_CUDA(cudaMemcpyAsync(host_field, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, s));
     }
     BFB_CUDA(cudaStreamSynchronize(s));
+    return BFB_OK;
+}
+
+BFB_API int bfb_host_register(void *host, size_t bytes) {
+    if (!host || bytes == 0) return fail(BFB_ERR_INVALID_ARG, "host is NULL or bytes is 0");
+    BFB_CUDA(cudaHostRegister(host, bytes, cudaHostRegisterDefault));
+    return BFB_OK;
+}
+
+BFB_API int bfb_host_unregister(void *host) {
+    if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
+    BFB_CUDA(cudaHostUnregister(host));
     return BFB_OK;
 }
 
@@ -1002,7 +1023,7 @@ BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double
                                     : time_candidates<float>(env, dt, trials, scratch, best, ms);
     cudaFree(scratch);
     if (st) return st;
-    if ((st = check_device_error(env))) return st;
+    if ((st = env_check_device_error(env))) return st;
     apply_tuning(env, best);
     if (chosen) std::copy(best, best + 9, chosen);
     if (best_ms) std::copy(ms, ms + 3, best_ms);
@@ -1080,8 +1101,7 @@ BFB_API int bfb_checksum(bfb_env env, double *out) {
     double *dout = env->partials + (size_t)env->partial_blocks * env->S;
     if ((st = launch_checksum(env, dout, env->stream))) return st;
     BFB_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * env->S, cudaMemcpyDeviceToHost, env->stream));
-    BFB_CUDA(cudaStreamSynchronize(env->stream));
-    return BFB_OK;
+    return env_check_device_error(env);
 }
 
 }  // extern "C"

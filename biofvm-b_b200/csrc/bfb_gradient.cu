@@ -276,7 +276,7 @@ BFB_API int bfb_get_gradients(bfb_env env, double *out_host) {
     cudaFree(buf);
     if (st) return st;
     if (e != cudaSuccess) return cuda_fail(e, "bfb_get_gradients");
-    return BFB_OK;
+    return env_check_device_error(env);
 }
 
 }  // extern "C"

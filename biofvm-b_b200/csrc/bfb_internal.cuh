@@ -31,6 +31,11 @@ void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 
+// Waits for the env's stream, then reads its sticky device error flag:
+// BFB_ERR_WATCHDOG once a kernel's bounded wait has run out (the field is then
+// not trustworthy), BFB_OK otherwise.
+int env_check_device_error(::bfb_env_s *env);
+
 #define BFB_CUDA(call)                                        \
     do {                                                      \
         cudaError_t _e = (call);                              \

@@ -79,6 +79,10 @@ extern "C" BFB_API int bfb_write_matlab(bfb_env env, const char *filename) {
         cudaFreeHost(hbuf);
         return cuda_fail(e, "bfb_write_matlab");
     }
+    if (int es = env_check_device_error(env)) {  // no file from an untrustworthy field
+        cudaFreeHost(hbuf);
+        return es;
+    }
     static const char name[] = "multiscale_microenvironment";
     const unsigned header[5] = {0u, (unsigned)(4 + S), (unsigned)V, 0u, (unsigned)(sizeof(name) - 1)};
     std::FILE *fp = std::fopen(filename, "wb");

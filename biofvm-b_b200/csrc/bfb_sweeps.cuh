@@ -117,6 +117,9 @@ int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cud
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
                            int S, int chunks = kChunks);
 void tma_prepare_device();
+// One bounded mbarrier wait that nothing completes, `polls` polls long; sets
+// *err like a stalled copy would (bfb_watchdog_selftest).
+int launch_watchdog_probe(int polls, int *err, cudaStream_t s);
 template <typename T>
 int launch_dirichlet(const SweepArgs<T> &a, cudaStream_t s);
 template <typename T>

@@ -151,6 +151,31 @@ __global__ void __launch_bounds__(128, 1) sweep_contig_pipe_kernel(SweepArgs<T> 
 }
 
 // ---------------------------------------------------------------------------
+// Watchdog self-test: one bounded wait on an mbarrier that nothing completes
+// (no thread arrives on it and no copy targets it), so nothing is in flight
+// when the wait gives up. It sets the error flag exactly as a stalled copy in
+// a sweep would.
+// ---------------------------------------------------------------------------
+__global__ void watchdog_probe_kernel(int polls, int *err) {
+    __shared__ __align__(8) unsigned long long bar;
+    const unsigned b = smem_u32(&bar);
+    if (threadIdx.x == 0) {
+        mbar_init(b, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    bool done = false;
+    for (int i = 0; i < polls && !done; ++i) done = mbar_try_wait(b, 0);
+    if (!done && threadIdx.x == 0) atomicOr(err, 1);
+}
+
+int launch_watchdog_probe(int polls, int *err, cudaStream_t s) {
+    watchdog_probe_kernel<<<1, 32, 0, s>>>(polls, err);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 template <typename T>

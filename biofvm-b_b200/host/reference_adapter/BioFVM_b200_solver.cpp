@@ -14,11 +14,22 @@
 // The field stays in the Microenvironment's own std::vector<double>. Each call
 // copies it to the device, runs one FP64 LOD step there (bit-exact with the
 // reference's LOD_3D) and copies it back, so host code sees what the CPU
-// solver would have produced. The device grid is created on the first call,
-// where the reference computes its Thomas factors (BioFVM_parallel.cpp:714),
-// and kept per Microenvironment; the factors stay at the first call's dt, D
-// and lambda, as the reference's do. Errors are printed, as the reference
-// prints its own (BioFVM_parallel.cpp:705-710), and leave the field unchanged.
+// solver would have produced. The vector's storage is page-locked
+// (bfb_host_register) on the first call, so both copies run at the host
+// link's pinned-memory speed.
+//
+// State per Microenvironment:
+//   * the device grid, created on the first call, where the reference computes
+//     its Thomas factors (BioFVM_parallel.cpp:714); the factors stay at the
+//     first call's dt, D and lambda, as the reference's do (:714, 913). A grid
+//     whose mesh size or substrate count no longer matches the
+//     Microenvironment (after resize_space or add_density) is replaced;
+//   * the Dirichlet state last sent to the device. The reference applies the
+//     activation flags and the outer-face entries of dirichlet_value_vectors on
+//     every call (BioFVM_microenvironment.cpp:381-484); they are compared with
+//     what the device holds and sent again only when one has changed.
+// Errors are printed, as the reference prints its own (BioFVM_parallel.cpp:
+// 705-710), and leave the field unchanged.
 #include <cstdint>
 #include <iostream>
 #include <map>
@@ -30,9 +41,44 @@
 namespace BioFVM {
 
 namespace {
-std::map<Microenvironment *, bfb_env> g_b200_envs;
+
+struct B200State {
+    bfb_env env = nullptr;
+    void *pinned = nullptr;            // the field storage page-locked for this Microenvironment
+    std::vector<uint8_t> activation;   // Dirichlet activation last sent to the device
+    std::vector<double> face_values;   // outer-face entries of dirichlet_value_vectors last sent
+    bool dirichlet_sent = false;
+};
+
+std::map<Microenvironment *, B200State> g_b200;
 
 void b200_report(const char *what) { std::cout << "B200 solver: " << what << ": " << bfb_last_error() << std::endl; }
+
+void release_state(B200State &st) {
+    if (st.pinned) bfb_host_unregister(st.pinned);
+    if (st.env) bfb_destroy(st.env);
+    st = B200State();
+}
+
+// The outer-face entries of the per-voxel Dirichlet values, in a fixed order
+// (the faces x = 0, x = nx-1, y = 0, y = ny-1, z = 0, z = nz-1; edges repeat).
+void face_entries(const std::vector<double> &v, int nx, int ny, int nz, int S, std::vector<double> &out) {
+    out.clear();
+    auto put = [&](int i, int j, int k) {
+        const size_t b = (((size_t)i * ny + j) * nz + k) * S;
+        out.insert(out.end(), v.begin() + b, v.begin() + b + S);
+    };
+    for (int i : {0, nx - 1})
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) put(i, j, k);
+    for (int j : {0, ny - 1})
+        for (int i = 0; i < nx; ++i)
+            for (int k = 0; k < nz; ++k) put(i, j, k);
+    for (int k : {0, nz - 1})
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) put(i, j, k);
+}
+
 }  // namespace
 
 void diffusion_decay_solver__constant_coefficients_LOD_3D_B200(Microenvironment &M, double dt, int mpi_Size,
@@ -52,37 +98,70 @@ void diffusion_decay_solver__constant_coefficients_LOD_3D_B200(Microenvironment 
         return;
     }
     const int S = M.number_of_densities();
-    auto it = g_b200_envs.find(&M);
-    if (it == g_b200_envs.end()) {
-        bfb_env env = nullptr;
-        if (bfb_create(&env, M.mesh.x_size, M.mesh.y_size, M.mesh.z_size, S, M.mesh.dx, BFB_FP64, 0) != BFB_OK) {
-            b200_report("bfb_create");
-            return;
-        }
-        if (bfb_set_coefficients(env, M.diffusion_coefficients.data(), M.decay_rates.data()) != BFB_OK) {
-            b200_report("bfb_set_coefficients");
-            bfb_destroy(env);
-            return;
-        }
-        it = g_b200_envs.emplace(&M, env).first;
-    }
-    std::vector<uint8_t> activation(S);
-    for (int d = 0; d < S; ++d) activation[d] = M.dirichlet_activation_vector[d] ? 1 : 0;
-    // all six faces follow the activation, the reference's rule (BioFVM_microenvironment.cpp:381-484)
-    if (bfb_set_dirichlet(it->second, M.dirichlet_value_vectors.data(), activation.data(), nullptr) != BFB_OK) {
-        b200_report("bfb_set_dirichlet");
+    const int nx = M.mesh.x_size, ny = M.mesh.y_size, nz = M.mesh.z_size;
+    std::vector<double> &field = *M.p_density_vectors;
+    if (field.size() != (size_t)nx * ny * nz * S) {
+        std::cout << "B200 solver: the density vector does not hold mesh voxels x substrates values" << std::endl;
         return;
     }
-    if (bfb_step_host(it->second, M.p_density_vectors->data(), dt, 1) != BFB_OK) b200_report("bfb_step_host");
+    B200State &st = g_b200[&M];
+    if (st.env) {  // a grid of another size or substrate count is replaced
+        int gx = 0, gy = 0, gz = 0, gs = 0;
+        bfb_get_shape(st.env, &gx, &gy, &gz, &gs);
+        if (gx != nx || gy != ny || gz != nz || gs != S) release_state(st);
+    }
+    if (!st.env) {
+        if (bfb_create(&st.env, nx, ny, nz, S, M.mesh.dx, BFB_FP64, 0) != BFB_OK) {
+            b200_report("bfb_create");
+            st.env = nullptr;
+            return;
+        }
+        if (bfb_set_coefficients(st.env, M.diffusion_coefficients.data(), M.decay_rates.data()) != BFB_OK) {
+            b200_report("bfb_set_coefficients");
+            release_state(st);
+            return;
+        }
+    }
+    if (st.pinned != field.data()) {  // the vector's storage moved: page-lock the new one
+        if (st.pinned) bfb_host_unregister(st.pinned);
+        st.pinned = nullptr;
+        if (bfb_host_register(field.data(), field.size() * sizeof(double)) == BFB_OK) st.pinned = field.data();
+        // not fatal: unregistered memory is copied at pageable speed
+    }
+    std::vector<uint8_t> activation(S);
+    bool any = false;
+    for (int d = 0; d < S; ++d) {
+        activation[d] = M.dirichlet_activation_vector[d] ? 1 : 0;
+        any = any || activation[d];
+    }
+    // the face values matter only where a substrate is active
+    std::vector<double> faces;
+    if (any) face_entries(M.dirichlet_value_vectors, nx, ny, nz, S, faces);
+    if (!st.dirichlet_sent || activation != st.activation || faces != st.face_values) {
+        // all six faces follow the activation, the reference's rule (BioFVM_microenvironment.cpp:381-484)
+        if (bfb_set_dirichlet(st.env, any ? M.dirichlet_value_vectors.data() : nullptr, activation.data(), nullptr) !=
+            BFB_OK) {
+            b200_report("bfb_set_dirichlet");
+            st.dirichlet_sent = false;
+            return;
+        }
+        st.activation = activation;
+        st.face_values.swap(faces);
+        st.dirichlet_sent = true;
+    }
+    if (bfb_step_host(st.env, field.data(), dt, 1) != BFB_OK) b200_report("bfb_step_host");
 }
 
-// Frees the device grid held for M; call it before M is destroyed if M's
-// address may be reused by another Microenvironment.
+// Frees the device grid held for M and unpins its field storage; call it
+// before M is destroyed if M's address may be reused by another
+// Microenvironment, and before M's density vectors are reallocated by a call
+// that does not step (the solver itself notices a reallocation on its next
+// call).
 void release_b200_solver(Microenvironment &M) {
-    auto it = g_b200_envs.find(&M);
-    if (it == g_b200_envs.end()) return;
-    bfb_destroy(it->second);
-    g_b200_envs.erase(it);
+    auto it = g_b200.find(&M);
+    if (it == g_b200.end()) return;
+    release_state(it->second);
+    g_b200.erase(it);
 }
 
 }  // namespace BioFVM

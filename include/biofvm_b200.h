@@ -96,6 +96,15 @@ BFB_API int bfb_get_shape(bfb_env env, int *nx, int *ny, int *nz, int *n_substra
 BFB_API int bfb_set_stream(bfb_env env, void *cuda_stream);
 BFB_API int bfb_set_option(bfb_env env, int option, int value);
 BFB_API int bfb_synchronize(bfb_env env);
+/* No counterpart in the reference (which has no device waits). Every wait of
+ * the TMA kernels on a copy is bounded; one that runs out sets the env's
+ * sticky error flag, after which bfb_synchronize, bfb_get_field[_raw],
+ * bfb_step_host (which then leaves the host field unchanged), bfb_checksum,
+ * bfb_get_gradients and bfb_write_matlab return BFB_ERR_WATCHDOG for this env.
+ * bfb_watchdog_selftest queues, on the env's stream, one such wait (`polls`
+ * polls, 1..2^20) on a barrier that nothing completes, so the error path can
+ * be tested without stalling any copy; the flag stays set for the env's life. */
+BFB_API int bfb_watchdog_selftest(bfb_env env, int polls);
 
 /* Per-substrate diffusion coefficients and decay rates (the public vectors
  * diffusion_coefficients / decay_rates, BioFVM_microenvironment.h:151-152).
@@ -179,6 +188,15 @@ BFB_API int bfb_simulate(bfb_env env, double dt, int n_steps, int flags);
 /* Host-buffer step for reference-facing callers: copies host (V*S doubles)
  * to the device, runs n_steps diffusion steps, copies the result back. */
 BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_steps);
+
+/* No counterpart in the reference. Page-locks (cudaHostRegister) `bytes` of
+ * caller-owned host memory at `host`, such as a Microenvironment's field
+ * vector, so that bfb_step_host / bfb_set_field / bfb_get_field copy it at
+ * pinned-memory speed instead of through the driver's staging buffers.
+ * bfb_host_unregister undoes it; call it before the memory is freed or
+ * reallocated (for a std::vector: before it grows or is destroyed). */
+BFB_API int bfb_host_register(void *host, size_t bytes);
+BFB_API int bfb_host_unregister(void *host);
 
 /* Device time per phase, the counterpart of the reference's -DTIMING per-sweep
  * CSV (BioFVM_parallel.cpp:695-697, 1259-1392): runs n_steps steps like
@@ -308,8 +326,11 @@ BFB_API int bfb_adjoint_run(bfb_env env, double dt, int n_steps, int flags, int 
  * the library, so at most BFB_NOALLOC_MAX_SUBSTRATES substrates (larger counts
  * return BFB_ERR_SIZE), and calls that overlap on the GPU share that array and
  * race: order them on one stream. The first call on each device looks the
- * array's device address up (cudaGetSymbolAddress); make that first call
- * before capturing a stream. The call allocates nothing. */
+ * array's device address up (cudaGetSymbolAddress) and keeps it for the rest
+ * of the process; make that first call before capturing a stream. The kept
+ * address does not survive a reset of the device's primary context
+ * (cudaDeviceReset): do not call this entry point after one. The call
+ * allocates nothing. */
 #define BFB_NOALLOC_MAX_SUBSTRATES 64
 BFB_API int bfb_checksum_noalloc(const void *field_dev, int precision, long long n_voxels, int n_substrates,
                                  double *out_dev, void *stream);

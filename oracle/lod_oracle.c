@@ -531,3 +531,35 @@ void orc_lod_steps_f32(float *rho, int nx, int ny, int nz, int S, double dt, dou
     free(p);
     free(vals);
 }
+
+/* The FP32 path's bulk update (not a reference function; the reference's
+ * arithmetic is orc_bulk_step's): with A = RN32(T*S) and B = RN32(U + S)
+ * formed in FP64 and rounded once, as the host tabulates them, and
+ * dt32 = RN32(dt):  rho = RN32(fma(dt32, A, rho) / fma(B, dt32, 1)). */
+void orc_bulk_step_f32(float *rho, int64_t V, int S, double dt, const double *S_rate, const double *T_target,
+                       const double *U_rate)
+{
+    const float dt32 = (float)dt;
+    for (int64_t e = 0; e < V * S; ++e) {
+        const float A = (float)(T_target[e] * S_rate[e]);
+        const float B = (float)(U_rate[e] + S_rate[e]);
+        rho[e] = fmaf(dt32, A, rho[e]) / fmaf(B, dt32, 1.0f);
+    }
+}
+
+/* The FP32 path's agent update: simulate_secretion_and_uptake
+ * (BioFVM_basic_agent.cpp:291-296) in FP32 for every active agent in list
+ * order, rho = (rho + RN32(temp1)) / RN32(temp2), with temp1/temp2 the FP64
+ * constants of orc_agent_constants rounded once. */
+void orc_cells_step_f32(float *rho, int S, int n, const int *voxel, const double *temp1, const double *temp2,
+                        const uint8_t *active)
+{
+    for (int a = 0; a < n; ++a) {
+        if (active && !active[a]) continue;
+        for (int d = 0; d < S; ++d) {
+            const size_t e = (size_t)voxel[a] * S + d;
+            rho[e] = (rho[e] + (float)temp1[(size_t)a * S + d]) / (float)temp2[(size_t)a * S + d];
+        }
+    }
+}
+

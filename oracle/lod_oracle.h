@@ -90,6 +90,14 @@ void orc_lod_step_adjoint(const double *rho_in, double *lam, int nx, int ny, int
 void orc_lod_steps_f32(float *rho, int nx, int ny, int nz, int S, double dt, double dx, const double *D,
                        const double *lambda, int n_steps, const double *dir_values, const uint8_t *face_mask);
 
+/* The FP32 path's bulk update and agent update (not reference functions):
+ * the arithmetic of orc_bulk_step / orc_cells_step in IEEE binary32, with the
+ * FP64 inputs rounded once as the product's host code rounds them. */
+void orc_bulk_step_f32(float *rho, int64_t V, int S, double dt, const double *S_rate, const double *T_target,
+                       const double *U_rate);
+void orc_cells_step_f32(float *rho, int S, int n, const int *voxel, const double *temp1, const double *temp2,
+                        const uint8_t *active);
+
 #ifdef __cplusplus
 }
 #endif

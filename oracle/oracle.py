@@ -76,6 +76,9 @@ class Oracle:
         L.orc_lod_steps_f32.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp, ctypes.c_int,
                                         _dp, _up]
+        _fp = ctypes.POINTER(ctypes.c_float)
+        L.orc_bulk_step_f32.argtypes = [_fp, ctypes.c_int64, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.orc_cells_step_f32.argtypes = [_fp, ctypes.c_int, ctypes.c_int, _ip, _dp, _dp, _up]
 
     def factors(self, n, dt, dx, D, lam):
         D, lam = f64(D), f64(lam)
@@ -132,6 +135,25 @@ class Oracle:
         self.lib.orc_lod_steps_f32(rho.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nx, ny, nz, S, dt, dx,
                                    _d(D), _d(lam), n_steps, None if dv is None else _d(dv),
                                    None if fm is None else _u(fm))
+        return rho
+
+    def bulk_step_f32(self, rho, dt, S_rate, T_target, U_rate):
+        """The FP32 path's bulk update (orc_bulk_step_f32) on a float32 field."""
+        rho = np.ascontiguousarray(rho, dtype=np.float32).copy()
+        S = rho.shape[-1]
+        Sr, Tt, Ur = f64(S_rate), f64(T_target), f64(U_rate)
+        self.lib.orc_bulk_step_f32(rho.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), rho.size // S, S, dt,
+                                   _d(Sr), _d(Tt), _d(Ur))
+        return rho
+
+    def cells_step_f32(self, rho, voxel, t1, t2, active=None):
+        """The FP32 path's agent update (orc_cells_step_f32) on a float32 field."""
+        rho = np.ascontiguousarray(rho, dtype=np.float32).copy()
+        S = rho.shape[-1]
+        voxel = np.ascontiguousarray(voxel, dtype=np.int32)
+        act = None if active is None else np.ascontiguousarray(active, dtype=np.uint8)
+        self.lib.orc_cells_step_f32(rho.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), S, voxel.size, _i(voxel),
+                                    _d(f64(t1)), _d(f64(t2)), _u(act) if act is not None else ctypes.cast(None, _up))
         return rho
 
     def bulk_step(self, rho, dt, S_rate, T_target, U_rate):

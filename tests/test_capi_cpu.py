@@ -39,6 +39,9 @@ def test_null_handle_is_rejected_without_gpu(bfb):
     assert L.bfb_destroy(None) == 0
     assert L.bfb_set_option(None, 1, 1) == -1
     assert b"null" in L.bfb_last_error()
+    assert L.bfb_watchdog_selftest(None, 8) == -1
+    assert L.bfb_host_register(None, 8) == -1
+    assert L.bfb_host_unregister(None) == -1
 
 
 def test_create_validates_arguments_before_touching_a_device(bfb):

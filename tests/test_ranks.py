@@ -1,4 +1,5 @@
-"""Multi-rank host logic (biofvm-b_b200/ranks.py) on CPU: two gloo ranks.
+"""Multi-rank host logic on CPU: the partition (biofvm-b_b200/ranks.py) and
+the collectives of the benchmark driver (bench.py), with two gloo ranks.
 
 The multi-GPU runs are replicas of one grid (barrier + max over ranks of the
 timed region) or an ensemble of independent instances sharded across ranks
@@ -21,6 +22,13 @@ ROOT = Path(__file__).resolve().parents[1]
 
 def load_ranks():
     spec = importlib.util.spec_from_file_location("bfb_ranks", ROOT / "biofvm-b_b200" / "ranks.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_bench():
+    spec = importlib.util.spec_from_file_location("bfb_bench", ROOT / "bench.py")
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod
@@ -51,12 +59,12 @@ def test_shard_is_a_balanced_partition():
 
 
 def test_single_process_is_collective_free():
-    ranks = load_ranks()
-    assert ranks.max_over_ranks(3.5) == 3.5
-    assert ranks.sum_over_ranks(2.0) == 2.0
-    g = ranks.gather_by_instance([1], [[7.0, 8.0]], 3, 2)
+    bench = load_bench()
+    assert bench.max_over_ranks(3.5) == 3.5
+    assert bench.sum_over_ranks(2.0) == 2.0
+    g = bench.gather_by_instance([1], [[7.0, 8.0]], 3, 2)
     assert np.array_equal(g, [[0, 0], [7, 8], [0, 0]])
-    ranks.barrier()
+    bench.rank_barrier()
 
 
 def _free_port():
@@ -72,7 +80,7 @@ def _rank_main(rank, world, port, q):
         os.environ["MASTER_PORT"] = str(port)
         import datetime
         dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
-        ranks = load_ranks()
+        ranks, bench = load_ranks(), load_bench()
         w = ensemble_weights()
         # every rank derives the same partition without communicating
         owner = ranks.shard_instances(w, world)
@@ -80,15 +88,15 @@ def _rank_main(rank, world, port, q):
         assert all(owner[i] == rank for i in mine)
         # stand-in per-instance results: a checksum per substrate slot computed from the instance id
         vals = [[float(i), float(i) * 0.5] for i in mine]
-        g = ranks.gather_by_instance(mine, vals, len(w), 2)
+        g = bench.gather_by_instance(mine, vals, len(w), 2)
         expect = np.stack([np.arange(len(w), dtype=float), np.arange(len(w)) * 0.5], axis=1)
         assert np.array_equal(g, expect)
         # timed region of a multi-GPU run: the slowest rank's
         t = 1.25 + rank
-        assert ranks.max_over_ranks(t) == 1.25 + (world - 1)
+        assert bench.max_over_ranks(t) == 1.25 + (world - 1)
         # whole-job throughput: units of all ranks
-        assert ranks.sum_over_ranks(float(len(mine))) == float(len(w))
-        ranks.barrier()
+        assert bench.sum_over_ranks(float(len(mine))) == float(len(w))
+        bench.rank_barrier()
         dist.destroy_process_group()
         q.put((rank, "ok"))
     except Exception as e:  # report to the parent instead of hanging the other rank
