@@ -229,12 +229,16 @@ static void encode_field_maps(bfb_env_s *env) {
 // One LOD diffusion step; `bulk` fuses a preceding bulk source/sink update
 // into the x-sweep load.
 template <typename T>
+static int launch_strided_env(bfb_env_s *env, int axis, bool bulk, double dt, cudaStream_t s) {
+    return launch_strided<T>(make_args<T>(env, axis, bulk, dt), axis, axis == 0, env->tuning.warps[axis],
+                             tma_map(env, axis), tma_map(env, axis), env->tma_crow[axis], s);
+}
+
+template <typename T>
 static int run_diffusion(bfb_env_s *env, double dt, bool bulk, cudaStream_t s) {
-    int st = launch_strided<T>(make_args<T>(env, 0, bulk, dt), 0, true, env->tuning.warps[0], tma_map(env, 0),
-                               tma_map(env, 0), env->tma_crow[0], s);
+    int st = launch_strided_env<T>(env, 0, bulk, dt, s);
     if (st) return st;
-    st = launch_strided<T>(make_args<T>(env, 1, false, dt), 1, false, env->tuning.warps[1], tma_map(env, 1),
-                           tma_map(env, 1), env->tma_crow[1], s);
+    st = launch_strided_env<T>(env, 1, false, dt, s);
     if (st) return st;
     return launch_contig<T>(make_args<T>(env, 2, false, dt), env->tuning.warps[2],
                             env->use_tma != 0 && env->tuning.tma[2] != 0, s, env->tuning.chunks[2]);
@@ -1059,19 +1063,13 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
         if (flags & BFB_STEP_DIFFUSION) {
             const bool bulk = (flags & BFB_STEP_BULK) != 0;
             st = phase_ms(0, [&] {
-                return fp64 ? launch_strided<double>(make_args<double>(env, 0, bulk, dt), 0, true, env->tuning.warps[0],
-                                                     tma_map(env, 0), tma_map(env, 0), env->tma_crow[0], s)
-                            : launch_strided<float>(make_args<float>(env, 0, bulk, dt), 0, true, env->tuning.warps[0],
-                                                    tma_map(env, 0), tma_map(env, 0), env->tma_crow[0], s);
+                return fp64 ? launch_strided_env<double>(env, 0, bulk, dt, s)
+                            : launch_strided_env<float>(env, 0, bulk, dt, s);
             });
             if (!st)
                 st = phase_ms(1, [&] {
-                    return fp64 ? launch_strided<double>(make_args<double>(env, 1, false, dt), 1, false,
-                                                         env->tuning.warps[1], tma_map(env, 1), tma_map(env, 1),
-                                                         env->tma_crow[1], s)
-                                : launch_strided<float>(make_args<float>(env, 1, false, dt), 1, false,
-                                                        env->tuning.warps[1], tma_map(env, 1), tma_map(env, 1),
-                                                        env->tma_crow[1], s);
+                    return fp64 ? launch_strided_env<double>(env, 1, false, dt, s)
+                                : launch_strided_env<float>(env, 1, false, dt, s);
                 });
             if (!st)
                 st = phase_ms(2, [&] {

@@ -166,13 +166,13 @@ __global__ void __launch_bounds__(128, 1) sweep_strided_kernel(SweepArgs<T> a, S
 // ---------------------------------------------------------------------------
 // Contiguous sweep (z). One warp = R consecutive (i,j) rows of nz*S elements.
 // ---------------------------------------------------------------------------
-template <typename T, int VB>
+template <typename T, int VB, int SC>
 __global__ void __launch_bounds__(128, 1) sweep_contig_kernel(SweepArgs<T> a, ContigGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5;
     const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
     if (tile * g.R >= g.nrows) return;
-    contig_tile<T, VB>(a, g, tile, reinterpret_cast<T *>(smem_raw) + (size_t)warp * g.R * g.RS);
+    contig_tile<T, VB, SC>(a, g, tile, reinterpret_cast<T *>(smem_raw) + (size_t)warp * g.R * g.RS);
 }
 // The same for S > 32 (a lane solves several lines of the tile).
 template <typename T, int VB>
@@ -402,10 +402,20 @@ template <typename T, int VB>
 static int go_contig(const SweepArgs<T> &a, const ContigGeom &g, int warps, size_t smem, cudaStream_t s) {
     const long long tiles = (g.nrows + g.R - 1) / g.R;
     const long long blocks = (tiles + warps - 1) / warps;
-    if (a.S > 32)
-        sweep_contig_wide_kernel<T, VB><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
-    else
-        sweep_contig_kernel<T, VB><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
+#define BFB_CONTIG(SC) sweep_contig_kernel<T, VB, SC><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g)
+    switch (a.S) {  // the substrate count as a constant where it is a common one
+    case 1: BFB_CONTIG(1); break;
+    case 2: BFB_CONTIG(2); break;
+    case 3: BFB_CONTIG(3); break;
+    case 4: BFB_CONTIG(4); break;
+    case 5: BFB_CONTIG(5); break;
+    case 6: BFB_CONTIG(6); break;
+    case 8: BFB_CONTIG(8); break;
+    default:
+        if (a.S > 32) sweep_contig_wide_kernel<T, VB><<<(unsigned)blocks, warps * 32, smem, s>>>(a, g);
+        else BFB_CONTIG(0);
+    }
+#undef BFB_CONTIG
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
 }
@@ -463,6 +473,18 @@ static void opt_in(K k) {
     cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
 }
 
+template <typename T, int VB>
+static void opt_in_contig() {
+    opt_in(sweep_contig_kernel<T, VB, 0>);
+    opt_in(sweep_contig_kernel<T, VB, 1>);
+    opt_in(sweep_contig_kernel<T, VB, 2>);
+    opt_in(sweep_contig_kernel<T, VB, 3>);
+    opt_in(sweep_contig_kernel<T, VB, 4>);
+    opt_in(sweep_contig_kernel<T, VB, 5>);
+    opt_in(sweep_contig_kernel<T, VB, 6>);
+    opt_in(sweep_contig_kernel<T, VB, 8>);
+}
+
 void sweeps_prepare_device() {
     static std::mutex mu;
     static unsigned long long done = 0;  // one bit per device
@@ -482,11 +504,11 @@ void sweeps_prepare_device() {
     opt_in(sweep_strided_kernel<float, 4, true, true>);
     opt_in(sweep_strided_kernel<float, 4, true, false>);
     opt_in(sweep_strided_kernel<float, 4, false, false>);
-    opt_in(sweep_contig_kernel<double, 16>);
-    opt_in(sweep_contig_kernel<double, 8>);
-    opt_in(sweep_contig_kernel<float, 16>);
-    opt_in(sweep_contig_kernel<float, 8>);
-    opt_in(sweep_contig_kernel<float, 4>);
+    opt_in_contig<double, 16>();
+    opt_in_contig<double, 8>();
+    opt_in_contig<float, 16>();
+    opt_in_contig<float, 8>();
+    opt_in_contig<float, 4>();
     opt_in(sweep_contig_wide_kernel<double, 16>);
     opt_in(sweep_contig_wide_kernel<double, 8>);
     opt_in(sweep_contig_wide_kernel<float, 16>);

@@ -249,9 +249,9 @@ __device__ __forceinline__ void contig_tile_wide(const SweepArgs<T> &a, const Co
 // while group 1 lands; the back substitution finishes group 1 first and the
 // warp writes it out while it computes group 0. Lane (r, d) solves line
 // (row0 + r, d) with the blocked row loops of bfb_line.cuh.
-template <typename T, int VB>
+template <typename T, int VB, int SC = 0>
 __device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigGeom &g, long long tile, T *sm) {
-    const int S = a.S;
+    const int S = SC > 0 ? SC : a.S;  // SC: the substrate count when it is a compile-time constant
     const int lane = threadIdx.x & 31;
     const long long row0 = tile * g.R;
     const int nr = (int)min((long long)g.R, g.nrows - row0);
@@ -356,11 +356,22 @@ __device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigG
     }
 }
 
-// contig_tile for S <= 32, contig_tile_wide otherwise.
+// contig_tile for S <= 32 (with the substrate count as a constant where it
+// is a common one), contig_tile_wide otherwise.
 template <typename T, int VB>
 __device__ __forceinline__ void contig_tile_any(const SweepArgs<T> &a, const ContigGeom &g, long long tile, T *sm) {
-    if (a.S > 32) contig_tile_wide<T, VB>(a, g, tile, sm);
-    else contig_tile<T, VB>(a, g, tile, sm);
+    switch (a.S) {
+    case 1: contig_tile<T, VB, 1>(a, g, tile, sm); break;
+    case 2: contig_tile<T, VB, 2>(a, g, tile, sm); break;
+    case 3: contig_tile<T, VB, 3>(a, g, tile, sm); break;
+    case 4: contig_tile<T, VB, 4>(a, g, tile, sm); break;
+    case 5: contig_tile<T, VB, 5>(a, g, tile, sm); break;
+    case 6: contig_tile<T, VB, 6>(a, g, tile, sm); break;
+    case 8: contig_tile<T, VB, 8>(a, g, tile, sm); break;
+    default:
+        if (a.S > 32) contig_tile_wide<T, VB>(a, g, tile, sm);
+        else contig_tile<T, VB>(a, g, tile, sm);
+    }
 }
 
 }  // namespace bfb

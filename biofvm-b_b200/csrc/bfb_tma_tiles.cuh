@@ -7,47 +7,35 @@
 
 namespace bfb {
 
-// One warp tile of a strided sweep with TMA: 32 lines of `tile`, in the
-// warp's region `wbase` (128-byte header of row-group mbarriers, then the
-// tile). The mbarriers are initialised by the caller; row group ch waits for
-// parity bit ch of `phase`, and every call completes one phase of each of
-// its row groups. Returns false (error flag set) when a bounded wait ran out.
-template <typename T, bool FUSE_PRE, bool BULK>
-__device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const CUtensorMap *map_out,
-                                                 const SweepArgs<T> &a, const StridedGeom &g, int crow, long long tile,
-                                                 unsigned char *wbase, unsigned phase) {
+// The line solve of one strided warp tile (32 lines of one slab, one lane
+// per line), shared by the TMA tiles of the forward sweeps. Row q of this
+// lane's line is col[q * rs] in shared memory. wait(ch) returns once row
+// group ch (rows [ch*crow, (ch+1)*crow)) has landed, false when its bounded
+// wait ran out; flush(ch) writes row group ch back once its rows are final
+// (the back substitution finishes the groups from the last to the first).
+// Returns false when a wait ran out.
+template <typename T, bool FUSE_PRE, bool BULK, typename WAIT, typename FLUSH>
+__device__ __forceinline__ bool strided_solve(const SweepArgs<T> &a, const StridedGeom &g, int crow, int slab,
+                                              long long col0, T *__restrict__ col, const int rs, WAIT wait,
+                                              FLUSH flush) {
     const int lane = threadIdx.x & 31;
-    const int slab = (int)(tile / g.ncb);
-    const int col0 = (int)((tile % g.ncb) * 32);
     const int n = g.n;
     const long long P = g.P;
     const int nch = (n + crow - 1) / crow;
-    const int rank = g.axis == 0 ? 2 : 3;
-    const unsigned bar0 = smem_u32(wbase);
-    T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
-    const unsigned sm_u32 = smem_u32(sm);
-    const unsigned chunk_bytes = (unsigned)crow * 32u * (unsigned)sizeof(T);
 
-    if (lane == 0) {
-        for (int ch = 0; ch < nch; ++ch) {
-            mbar_expect_tx(bar0 + 8 * ch, chunk_bytes);
-            tma_load(sm_u32 + ch * chunk_bytes, map, col0, ch * crow, slab, rank, bar0 + 8 * ch);
-        }
-    }
-
-    // ---- line coordinates of this lane (lanes past P run along on zeros)
-    const long long col = (long long)col0 + lane;
-    const bool valid = col < P;
+    // ---- line coordinates of this lane (lanes past P run along, unstored)
+    const long long cl = col0 + lane;
+    const bool valid = cl < P;
     const int S = a.S;
-    const int d = (int)(col % S);
+    const int d = (int)(cl % S);
     int ci, cj, ck;
     if (g.axis == 0) {
-        const long long t = col / S;
+        const long long t = cl / S;
         ck = (int)(t % a.nz);
         cj = (int)(t / a.nz);
         ci = 0;
     } else {
-        ck = (int)(col / S);
+        ck = (int)(cl / S);
         ci = slab;
         cj = 0;
     }
@@ -69,20 +57,15 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
     };
     const T *bA = nullptr, *bB = nullptr;
     if constexpr (BULK) {
-        bA = a.bulk.A + (size_t)slab * g.slab_stride + col;
-        bB = a.bulk.B + (size_t)slab * g.slab_stride + col;
+        bA = a.bulk.A + (size_t)slab * g.slab_stride + cl;
+        bB = a.bulk.B + (size_t)slab * g.slab_stride + cl;
     }
     auto load = [&](int r) -> T {
-        T x = sm[r * 32 + lane];
+        T x = col[r * rs];
         if constexpr (BULK) {
             if (valid) x = bulk_update(x, bA[(size_t)r * P], bB[(size_t)r * P], a.bulk.dt);
         }
         return x;
-    };
-    auto wait_group = [&](int ch) -> bool {
-        if (mbar_wait(bar0 + 8 * ch, (phase >> ch) & 1u)) return true;
-        if (lane == 0) atomicOr(a.err, 1);
-        return false;
     };
 
     LineSolver<T> L(a, d);
@@ -99,15 +82,16 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
     const int rref = min(1, n - 1);  // row of the deviation reference
     const int ref_ch = rref / crow;
     for (int ch = 0; ch <= ref_ch; ++ch)
-        if (!wait_group(ch)) return false;
-    sm[lane] = L.first(xin(0), xin(rref));
+        if (!wait(ch)) return false;
+    col[0] = L.first(xin(0), xin(rref));
     int r = 1;
+    auto st_col = [&](int q, T v) { col[q * rs] = v; };
     for (int ch = 0; ch < nch; ++ch) {
-        if (ch > ref_ch && !wait_group(ch)) return false;
+        if (ch > ref_ch && !wait(ch)) return false;
         const int rend = min(n - 1, (ch + 1) * crow);
         const int hend = min(rend, m0);
-        r = head_forward(L, r, hend, load, [&](int q, T v) { sm[q * 32 + lane] = v; });
-        r = tail_forward(L, r, rend, load, [&](int q, T v) { sm[q * 32 + lane] = v; });
+        r = head_forward(L, r, hend, load, st_col);
+        r = tail_forward(L, r, rend, load, st_col);
     }
     if (n > 1) {
         T x = load(n - 1);
@@ -115,41 +99,76 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
         L.template fwd<false>(x, n - 1);
     }
 
-    // ---- back substitution into the tile; each finished row group is stored
+    // ---- back substitution into the tile; each finished row group is flushed
     {
         T y = L.out_last();
         if (hi_dir || (lo_dir && n == 1)) y = vox_dir(n - 1);
-        sm[(n - 1) * 32 + lane] = y;
+        col[(n - 1) * rs] = y;
     }
     const int tl = max(m0, 1);
+    auto ld_col = [&](int q) { return col[q * rs]; };
     r = n - 2;
     for (int ch = nch - 1; ch >= 0; --ch) {
         const int rlo = ch * crow;
         const int tstop = max(rlo, tl);
-        r = tail_backward(L, r, tstop, [&](int q) { return sm[q * 32 + lane]; },
-                          [&](int q, T v) { sm[q * 32 + lane] = v; });
+        r = tail_backward(L, r, tstop, ld_col, st_col);
         const int hstop = max(rlo, 1);
-        r = head_backward(L, r, hstop, [&](int q) { return sm[q * 32 + lane]; },
-                          [&](int q, T v) { sm[q * 32 + lane] = v; });
+        r = head_backward(L, r, hstop, ld_col, st_col);
         if (rlo == 0 && n > 1) {
-            T y = L.template bwd<false>(sm[lane], 0);
+            T y = L.template bwd<false>(col[0], 0);
             if (lo_dir) y = vox_dir(0);
-            sm[lane] = y;
+            col[0] = y;
         }
         if (col_dir)  // the whole column lies on an active face of another axis
-            for (int q = rlo; q < min(n, rlo + crow); ++q) sm[q * 32 + lane] = vox_dir(q);
+            for (int q = rlo; q < min(n, rlo + crow); ++q) col[q * rs] = vox_dir(q);
+        flush(ch);
+    }
+    return true;
+}
+
+// One warp tile of a strided sweep with TMA: 32 lines of `tile`, in the
+// warp's region `wbase` (128-byte header of row-group mbarriers, then the
+// tile). The mbarriers are initialised by the caller; row group ch waits for
+// parity bit ch of `phase`, and every call completes one phase of each of
+// its row groups. Returns false (error flag set) when a bounded wait ran out.
+template <typename T, bool FUSE_PRE, bool BULK>
+__device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const CUtensorMap *map_out,
+                                                 const SweepArgs<T> &a, const StridedGeom &g, int crow, long long tile,
+                                                 unsigned char *wbase, unsigned phase) {
+    const int lane = threadIdx.x & 31;
+    const int slab = (int)(tile / g.ncb);
+    const int col0 = (int)((tile % g.ncb) * 32);
+    const int nch = (g.n + crow - 1) / crow;
+    const int rank = g.axis == 0 ? 2 : 3;
+    const unsigned bar0 = smem_u32(wbase);
+    T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
+    const unsigned sm_u32 = smem_u32(sm);
+    const unsigned chunk_bytes = (unsigned)crow * 32u * (unsigned)sizeof(T);
+
+    if (lane == 0) {
+        for (int ch = 0; ch < nch; ++ch) {
+            mbar_expect_tx(bar0 + 8 * ch, chunk_bytes);
+            tma_load(sm_u32 + ch * chunk_bytes, map, col0, ch * crow, slab, rank, bar0 + 8 * ch);
+        }
+    }
+    auto wait = [&](int ch) -> bool {
+        if (mbar_wait(bar0 + 8 * ch, (phase >> ch) & 1u)) return true;
+        if (lane == 0) atomicOr(a.err, 1);
+        return false;
+    };
+    auto flush = [&](int ch) {
         fence_async_smem();
         __syncwarp();
         if (lane == 0) {
-            tma_store(map_out, col0, rlo, slab, rank, sm_u32 + ch * chunk_bytes);
+            tma_store(map_out, col0, ch * crow, slab, rank, sm_u32 + ch * chunk_bytes);
             bulk_commit();
         }
-    }
+    };
+    if (!strided_solve<T, FUSE_PRE, BULK>(a, g, crow, slab, col0, sm + lane, 32, wait, flush)) return false;
     if (lane == 0) bulk_wait_read_all();  // the tile must outlive the stores' reads
     __syncwarp();
     return true;
 }
-
 
 // One warp tile of the pipelined z sweep (rows row0 .. row0 + R - 1 of
 // `tile`) in the warp's region `wbase`; mbarriers and `phase` as for

@@ -31,6 +31,7 @@
 // Errors are printed, as the reference prints its own (BioFVM_parallel.cpp:
 // 705-710), and leave the field unchanged.
 #include <cstdint>
+#include <cstring>
 #include <iostream>
 #include <map>
 #include <vector>
@@ -77,6 +78,30 @@ void face_entries(const std::vector<double> &v, int nx, int ny, int nz, int S, s
     for (int k : {0, nz - 1})
         for (int i = 0; i < nx; ++i)
             for (int j = 0; j < ny; ++j) put(i, j, k);
+}
+
+// Whether the outer-face entries of v differ, bit for bit, from `cached`
+// (laid out as face_entries lays them out); compared in place, block by block.
+bool faces_changed(const std::vector<double> &v, int nx, int ny, int nz, int S, const std::vector<double> &cached) {
+    const size_t want = 2 * ((size_t)ny * nz + (size_t)nx * nz + (size_t)nx * ny) * S;
+    if (cached.size() != want) return true;
+    const double *c = cached.data();
+    auto differs = [&](size_t at, size_t count) {
+        const bool d = std::memcmp(v.data() + at, c, count * sizeof(double)) != 0;
+        c += count;
+        return d;
+    };
+    const size_t row = (size_t)nz * S;
+    for (int i : {0, nx - 1})
+        if (differs((size_t)i * ny * row, (size_t)ny * row)) return true;
+    for (int j : {0, ny - 1})
+        for (int i = 0; i < nx; ++i)
+            if (differs(((size_t)i * ny + j) * row, row)) return true;
+    for (int k : {0, nz - 1})
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j)
+                if (differs(((size_t)i * ny + j) * row + (size_t)k * S, S)) return true;
+    return false;
 }
 
 }  // namespace
@@ -135,9 +160,11 @@ void diffusion_decay_solver__constant_coefficients_LOD_3D_B200(Microenvironment 
         any = any || activation[d];
     }
     // the face values matter only where a substrate is active
-    std::vector<double> faces;
-    if (any) face_entries(M.dirichlet_value_vectors, nx, ny, nz, S, faces);
-    if (!st.dirichlet_sent || activation != st.activation || faces != st.face_values) {
+    const bool changed = !st.dirichlet_sent || activation != st.activation ||
+                         (any && faces_changed(M.dirichlet_value_vectors, nx, ny, nz, S, st.face_values));
+    if (changed) {
+        std::vector<double> faces;
+        if (any) face_entries(M.dirichlet_value_vectors, nx, ny, nz, S, faces);
         // all six faces follow the activation, the reference's rule (BioFVM_microenvironment.cpp:381-484)
         if (bfb_set_dirichlet(st.env, any ? M.dirichlet_value_vectors.data() : nullptr, activation.data(), nullptr) !=
             BFB_OK) {
