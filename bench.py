@@ -21,6 +21,7 @@ One JSON line is printed by rank 0.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import importlib.util
 import json
 import os
@@ -219,6 +220,72 @@ def cpu_port_run(max_seconds):
 
 
 # ---------------------------------------------------------------------------
+# the uneven ensemble: 256 independent microenvironments
+# ---------------------------------------------------------------------------
+ENSEMBLE_N = 256
+ENSEMBLE_SEED = 4
+
+
+def ensemble_specs(n=ENSEMBLE_N, seed=ENSEMBLE_SEED):
+    """Per-instance parameters: grid edges U{32..160} per axis (non-cubic),
+    1-6 substrates with D and lambda log-uniform in [1e2, 1e5] / [1e-3, 1],
+    0-20k agents, Dirichlet 38.0 on the x faces for substrate 0. Each
+    instance's field and agents come from its own seed, so every rank builds
+    any instance identically without communicating."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n):
+        shape = tuple(int(v) for v in rng.integers(32, 161, 3))
+        S_i = int(rng.integers(1, 7))
+        D = np.exp(rng.uniform(np.log(1e2), np.log(1e5), S_i))
+        lam = np.exp(rng.uniform(np.log(1e-3), np.log(1.0), S_i))
+        specs.append({"shape": shape, "S": S_i, "D": D, "lam": lam, "agents": int(rng.integers(0, 20001)),
+                      "seed": seed * 100_000 + i})
+    return specs
+
+
+def build_instance(bfb, spec, precision, device):
+    rng = np.random.default_rng(spec["seed"])
+    shape, S_i = spec["shape"], spec["S"]
+    env = bfb.Env(shape, S_i, dx=DX, precision=precision, device=device)
+    env.set_coefficients(spec["D"], spec["lam"])
+    env.set_field(rng.random((*shape, S_i)))
+    fm = np.zeros((6, S_i), np.uint8)
+    fm[0:2, 0] = 1
+    act = np.zeros(S_i, np.uint8)
+    act[0] = 1
+    env.set_dirichlet_uniform(act, np.full(S_i, 38.0), face_mask=fm)
+    na = spec["agents"]
+    if na:
+        box = np.array(shape) * DX
+        sec, upt, sat = np.exp(rng.uniform(np.log(1e-2), np.log(10.0), (3, na, S_i)))
+        env.set_agents(rng.random((na, 3)) * box, np.full(na, 4.0 / 3.0 * np.pi * 125.0), sec, upt, sat, DT)
+    return env
+
+
+def time_ensemble(bfb, envs, K, stream):
+    """Device time per step of the envs stepped together (bfb_batch_simulate)
+    and one by one (bfb_batch_simulate_loop), CUDA events on one stream."""
+    import torch
+    flags = bfb.STEP_DIFFUSION | bfb.STEP_CELLS
+    batch = bfb.Batch(envs)
+    batch.set_stream(stream.cuda_stream)
+    out = {}
+    for name, run in (("batch", batch.simulate), ("loop", batch.simulate_loop)):
+        run(DT, 3, flags)  # warm-up (graph captures)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run(DT, K, flags)
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = e0.elapsed_time(e1) / K
+    batch.synchronize()
+    batch.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # collectives between ranks: torch.distributed (NCCL on GPUs, gloo in the CPU
 # tests); each is a no-op in one process. The library's own ranks.py holds
 # only the partition of an ensemble's instances.
@@ -401,6 +468,28 @@ def run_our_arm(args):
         adj_ms[Kc] = slowest(e0.elapsed_time(e1))
     env.close()
 
+    # the uneven ensemble at N = 1: batched launches against the per-instance loop
+    ens = None
+    if world == 1 and not args.no_ensemble:
+        specs = ensemble_specs()
+        envs = [build_instance(bfb, sp, bfb.FP32, local) for sp in specs]
+        K_ens = max(1, min(K, 20))
+        t = time_ensemble(bfb, envs, K_ens, stream)
+        vs = sum(int(np.prod(sp["shape"])) * sp["S"] for sp in specs)
+        step_bytes_ens = 6.0 * vs * 4
+        for e in envs:
+            e.close()
+        peak_e, _ = measured_peak()
+        ens = {"workload": f"{len(specs)} independent microenvironments, edges U{{32..160}} per axis, 1-6 "
+                           "substrates, 0-20k agents each, x-face Dirichlet on substrate 0, FP32, diffusion + agents",
+               "voxel_substrates": vs, "steps": K_ens,
+               "batch_ms_per_step": t["batch"], "loop_ms_per_step": t["loop"],
+               "batch_value": vs / (t["batch"] / 1e3), "loop_value": vs / (t["loop"] / 1e3),
+               "batch_over_loop_time": t["batch"] / t["loop"],
+               "step_roofline_frac": {"batch": step_bytes_ens / (t["batch"] / 1e3) / 1e9 / peak_e,
+                                      "loop": step_bytes_ens / (t["loop"] / 1e3) / 1e9 / peak_e},
+               "note": "step roofline counts 6 V*S*4 bytes per step (three sweeps); CUDA events on one stream"}
+
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -466,6 +555,108 @@ def run_our_arm(args):
             "reverse_over_forward": (adj_ms[n_adj] / n_adj - ms_step) / ms_step,
             "run_over_forward": {f"checkpoint_every_{k}": v / n_adj / ms_step for k, v in adj_ms.items()},
         },
+        "ensemble": ens,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ensemble_arm(args):
+    """The uneven ensemble sharded across ranks: each rank steps its share of
+    the instances (greedy bytes balancing, ranks.local_instances) as one
+    batch; no collective touches the fields. value = all ranks' voxel*substrate
+    updates per step / the slowest rank's step time. Per-instance checksums
+    are gathered by instance at the end."""
+    import torch
+    rank, world, local = dist_setup(args)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    bfb = load_bfb()
+    ranks = importlib.import_module("biofvm_b_b200.ranks")
+    specs = ensemble_specs()
+    weights = [ranks.instance_bytes(sp["shape"], sp["S"], 4) for sp in specs]
+    mine = ranks.local_instances(weights, rank, world)
+    envs = [build_instance(bfb, specs[i], bfb.FP32, local) for i in mine]
+    vs_all = sum(int(np.prod(sp["shape"])) * sp["S"] for sp in specs)
+    vs_mine = sum(int(np.prod(specs[i]["shape"])) * specs[i]["S"] for i in mine)
+    flags = bfb.STEP_DIFFUSION | bfb.STEP_CELLS
+    warm, K = max(args.warmup, 3), args.steps
+    stream = torch.cuda.Stream(device=dev)
+    batch = bfb.Batch(envs)
+    batch.set_stream(stream.cuda_stream)
+    batch.simulate(DT, warm, flags)
+    stream.synchronize()
+    rank_barrier(dev)
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.simulate(DT, K, flags)
+    e1.record(stream)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
+    clk = clocks.stop()
+    batch.synchronize()
+    rank_barrier(dev)
+    # end to end: every step uploads each local instance's field from pinned
+    # host memory, steps the batch, and reads every field back
+    for e in envs:
+        e.set_stream(stream.cuda_stream)
+    hosts = [torch.empty(int(np.prod(specs[i]["shape"])) * specs[i]["S"], dtype=torch.float32).pin_memory()
+             for i in mine]
+    def raw(call, e, h):
+        if call(e.h, ctypes.c_void_p(h.data_ptr())) != 0:
+            raise RuntimeError(e.L.bfb_last_error().decode())
+
+    for h, e in zip(hosts, envs):
+        raw(e.L.bfb_get_field_raw, e, h)
+    K_e2e = max(1, min(K, 5))
+    rank_barrier(dev)
+    e0.record(stream)
+    for _ in range(K_e2e):
+        for h, e in zip(hosts, envs):
+            raw(e.L.bfb_set_field_raw, e, h)
+        batch.simulate(DT, 1, flags)
+        for h, e in zip(hosts, envs):
+            raw(e.L.bfb_get_field_raw, e, h)
+    e1.record(stream)
+    e1.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dev)
+    sums = gather_by_instance(mine, [e.checksum() for e in envs], len(specs), 6, dev)
+    batch.close()
+    for e in envs:
+        e.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    peak, _ = measured_peak()
+    step_bytes = 6.0 * vs_all * 4
+    line = {
+        "metric": f"voxel*substrate updates/s per LOD step (uneven ensemble, {len(specs)} instances)",
+        "value": vs_all / (ms / K / 1e3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warm,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded per instance: U[0,1) fields, log-uniform D/lambda and agent rates)",
+        "config": {"workload": f"{len(specs)} independent microenvironments, edges U{{32..160}} per axis, 1-6 "
+                               "substrates, 0-20k agents each, x-face Dirichlet 38 on substrate 0, diffusion + agents",
+                   "voxel_substrates": vs_all, "l2": "inputs larger than L2 (3.2 GB of FP32 fields)",
+                   "parallelism": f"instances sharded over {world} rank(s) by greedy bytes balancing, one batch per rank"},
+        "roofline": {"bound": "hbm", "achieved": step_bytes / (ms / K / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": step_bytes / (ms / K / 1e3) / 1e9 / peak, "traffic": None,
+                     "kernel": "whole step (three sweeps of every instance)"},
+        "clocks": clk,
+        "e2e": {"value": vs_all * K_e2e / (ms_e2e / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": vs_all * 4, "d2h_bytes_per_step": vs_all * 4, "steps": K_e2e,
+                "path": "bfb_set_field_raw per instance (pinned FP32) -> bfb_batch_simulate -> bfb_get_field_raw"},
+        "gpu_launches": None,
+        "checksum_of_checksums": float(sums.sum()),
+        "rank0_share": vs_mine / vs_all,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -484,12 +675,17 @@ def main():
     ap.add_argument("--substrates", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (for profiler runs, whose timing would mislead the tuner)")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the uneven-ensemble block of the default run")
+    ap.add_argument("--workload", default="grid", choices=["grid", "ensemble"],
+                    help="grid: the 256^3 x 8 step (replicas per GPU); ensemble: 256 uneven instances sharded over the GPUs")
     args = ap.parse_args()
     global NX, NY, NZ, S
     NX = NY = NZ = args.grid
     S = args.substrates
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "ensemble":
+        return run_ensemble_arm(args)
     return run_our_arm(args)
 
 

@@ -59,6 +59,7 @@ EXPORTS = [
     "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_write_matlab", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_get_option", "bfb_batch_simulate",
     "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_batch_autotune", "bfb_adjoint_run",
     "bfb_checksum_noalloc", "bfb_watchdog_selftest", "bfb_host_register", "bfb_host_unregister",
+    "bfb_batch_set_stream",
 ]
 
 
@@ -133,6 +134,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_batch_simulate": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_simulate_loop": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "bfb_batch_synchronize": [_vp],
+        "bfb_batch_set_stream": [_vp, _vp],
         "bfb_batch_autotune": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp],
         "bfb_adjoint_run": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _dp, _dp,
                             _dp, _dp, _dp],
@@ -457,3 +459,7 @@ class Batch:
 
     def synchronize(self):
         _check(self.L.bfb_batch_synchronize(self.h))
+
+    def set_stream(self, stream_handle: int):
+        """Issue the batch's steps on a caller's CUDA stream (0: its own)."""
+        _check(self.L.bfb_batch_set_stream(self.h, ctypes.c_void_p(stream_handle or None)))

@@ -291,29 +291,93 @@ int launch_cells(bfb_env_s *env, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------
-// Checksum: fixed partition of voxels per block, block tree sums in FP64,
-// then one block adds the partials in block order -> deterministic.
+// Checksum: fixed partition of voxels per block, one pass over the field,
+// FP64 sums in a fixed order -> deterministic.
+// A block sums voxels [v0, v1) (v0 a multiple of 4, so the block's first
+// element is 16-byte aligned when the field is). The block's elements are cut
+// into rows of W = R*S elements (W a multiple of the 16-byte vector width V);
+// thread t reads vector t of every row, so one warp load covers 512
+// consecutive bytes, every element is read once, and the element at position
+// p = V*t + j of a row always belongs to substrate p mod S: the thread keeps
+// one FP64 accumulator per vector lane j. The block then adds, per substrate
+// d, the accumulators of positions d, d + S, ..., in order, and
+// checksum_final_kernel adds the blocks' partial sums in block order.
 // ---------------------------------------------------------------------------
 constexpr int kSumBlocks = 296;  // 2 x 148 SMs
 constexpr int kSumThreads = 256;
 constexpr int kMaxSumS = 64;
 
 template <typename T>
-__global__ void checksum_partial_kernel(const T *__restrict__ f, long long V, int S, double *__restrict__ partials) {
-    __shared__ double red[kSumThreads];
-    const long long per = (V + gridDim.x - 1) / gridDim.x;
-    const long long v0 = (long long)blockIdx.x * per, v1 = min(V, v0 + per);
-    for (int d = 0; d < S; ++d) {
-        double acc = 0.0;
-        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) acc += (double)f[(size_t)v * S + d];
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
+struct SumVec;
+template <>
+struct SumVec<float> {
+    static constexpr int V = 4;
+    using type = float4;
+    __device__ static void add(const float4 &x, double (&a)[4]) {
+        a[0] += (double)x.x, a[1] += (double)x.y, a[2] += (double)x.z, a[3] += (double)x.w;
+    }
+};
+template <>
+struct SumVec<double> {
+    static constexpr int V = 2;
+    using type = double2;
+    __device__ static void add(const double2 &x, double (&a)[2]) { a[0] += x.x, a[1] += x.y; }
+};
+
+// W = R*S elements per row: the largest multiple of lcm(S, V) not above V*256
+__host__ __device__ inline int sum_row_width(int S, int V) {
+    int l = S;
+    while (l % V) l += S;
+    return (V * kSumThreads) / l * l;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads) checksum_partial_kernel(const T *__restrict__ f, long long V, int S,
+                                                                       double *__restrict__ partials) {
+    constexpr int VW = SumVec<T>::V;
+    using VT = typename SumVec<T>::type;
+    __shared__ double red[VW * kSumThreads];
+    const int W = sum_row_width(S, VW);
+    const int t = threadIdx.x;
+    long long per = (V + gridDim.x - 1) / gridDim.x;
+    per = (per + 3) / 4 * 4;
+    const long long v0 = min(V, (long long)blockIdx.x * per), v1 = min(V, v0 + per);
+    const long long e0 = v0 * S, ne = (v1 - v0) * S;  // the block's elements
+    const T *__restrict__ base = f + e0;
+    double acc[VW];
+#pragma unroll
+    for (int j = 0; j < VW; ++j) acc[j] = 0.0;
+    const bool vec = (reinterpret_cast<uintptr_t>(base) & 15) == 0;
+    const long long rows = ne / W;
+    long long row = 0;
+    if (vec && VW * t < W) {
+        const VT *__restrict__ p = reinterpret_cast<const VT *>(base) + t;
+        const long long stride = W / VW;  // vectors per row
+        constexpr int kRowsInFlight = 8;  // 8 x 16 B per thread in flight
+        for (; row + kRowsInFlight <= rows; row += kRowsInFlight) {
+            VT x[kRowsInFlight];
+#pragma unroll
+            for (int u = 0; u < kRowsInFlight; ++u) x[u] = p[(row + u) * stride];
+#pragma unroll
+            for (int u = 0; u < kRowsInFlight; ++u) SumVec<T>::add(x[u], acc);
         }
-        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * S + d] = red[0];
-        __syncthreads();
+        for (; row < rows; ++row) SumVec<T>::add(p[row * stride], acc);
+    }
+    if (!vec) row = 0;  // an unaligned field is read element by element
+    // the rest (the last partial row, or all rows without 16-byte alignment)
+    // element by element, each element to the accumulator of its row position
+    if (VW * t < W)
+        for (long long e = row * W + VW * t; e < ne; e += W)
+#pragma unroll
+            for (int j = 0; j < VW; ++j)
+                if (e + j < ne) acc[j] += (double)base[e + j];
+#pragma unroll
+    for (int j = 0; j < VW; ++j) red[VW * t + j] = VW * t < W ? acc[j] : 0.0;
+    __syncthreads();
+    if (t < S) {
+        double sum = 0.0;
+        for (int q = t; q < W; q += S) sum += red[q];
+        partials[(size_t)blockIdx.x * S + t] = sum;
     }
 }
 

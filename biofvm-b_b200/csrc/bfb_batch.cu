@@ -842,12 +842,31 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
 
 BFB_API int bfb_batch_simulate_loop(bfb_batch b, double dt, int n_steps, int flags) {
     if (!b) return fail(BFB_ERR_INVALID_ARG, "null bfb_batch");
+    BFB_CUDA(cudaSetDevice(b->device));
+    // every env's stream starts after the work queued on the batch stream, and
+    // the batch stream waits for every env's last step, so events on the batch
+    // stream bracket the whole loop
+    BFB_CUDA(cudaEventRecord(b->fork_ev, b->stream));
+    for (bfb_env e : b->envs) BFB_CUDA(cudaStreamWaitEvent(e->stream, b->fork_ev, 0));
     for (int q = 0; q < n_steps; ++q)
         for (bfb_env e : b->envs) {
             const int st = bfb_simulate(e, dt, 1, flags);
             if (st) return st;
         }
-    for (bfb_env e : b->envs) BFB_CUDA(cudaStreamSynchronize(e->stream));
+    for (bfb_env e : b->envs) {
+        BFB_CUDA(cudaEventRecord(b->join_ev[0], e->stream));
+        BFB_CUDA(cudaStreamWaitEvent(b->stream, b->join_ev[0], 0));
+    }
+    BFB_CUDA(cudaStreamSynchronize(b->stream));
+    return BFB_OK;
+}
+
+BFB_API int bfb_batch_set_stream(bfb_batch b, void *stream) {
+    if (!b) return fail(BFB_ERR_INVALID_ARG, "null bfb_batch");
+    BFB_CUDA(cudaSetDevice(b->device));
+    cudaStream_t want = stream ? (cudaStream_t)stream : b->own_stream;
+    if (want != b->stream) BFB_CUDA(cudaStreamSynchronize(b->stream));
+    b->stream = want;  // the captured step graph is launched into whichever stream is current
     return BFB_OK;
 }
 

@@ -276,6 +276,10 @@ BFB_API int bfb_batch_set_option(bfb_batch batch, int option, int value);
 BFB_API int bfb_batch_get_option(bfb_batch batch, int option, int *value);
 BFB_API int bfb_batch_simulate(bfb_batch batch, double dt, int n_steps, int flags);
 BFB_API int bfb_batch_simulate_loop(bfb_batch batch, double dt, int n_steps, int flags);
+/* A batch owns a non-blocking stream; bfb_batch_set_stream issues its steps
+ * (and orders bfb_batch_simulate_loop's per-env work) on the caller's stream
+ * instead (NULL: back to its own), e.g. to time them with events there. */
+BFB_API int bfb_batch_set_stream(bfb_batch batch, void *cuda_stream);
 BFB_API int bfb_batch_synchronize(bfb_batch batch);
 /* Times bfb_batch_simulate in the staged mode with warps per CTA {1, 2, 4}
  * and in the persistent mode with warps per CTA {1, 2, 4} x tiles per item

@@ -134,7 +134,8 @@ def test_cube75_s1_full_size_fp64(bfb, oracle):
 
 SHAPES = [((1, 1, 1), 1), ((1, 4, 6), 2), ((2, 3, 1), 3), ((3, 2, 2), 1), ((5, 17, 3), 4), ((17, 5, 2), 6),
           ((8, 8, 8), 4), ((8, 8, 8), 8), ((7, 5, 9), 3), ((33, 31, 35), 5), ((64, 2, 3), 2), ((2, 64, 40), 1),
-          ((40, 3, 64), 7), ((6, 5, 7), 40), ((3, 9, 4), 33)]  # S > 32: lanes solve several z lines each
+          ((40, 3, 64), 7), ((6, 5, 7), 40), ((3, 9, 4), 33),  # S > 32: lanes solve several z lines each
+          ((100, 6, 8), 3), ((5, 130, 4), 2), ((97, 96, 4), 1)]  # lines of about 100 rows
 
 
 @pytest.mark.parametrize("tma", [1, 0], ids=["tma", "cpasync"])
@@ -183,6 +184,18 @@ def test_long_lines_use_fallback_kernels(bfb, oracle, rng, shape, S, prec):
         assert rel_linf(got, want) <= FP32_TOL
 
 
+def test_factors_without_a_constant_tail(bfb, oracle, rng):
+    """With a huge D (c1 = 2500) the Thomas factors still vary at the end of a
+    96-row line, so no row uses the register copies of the tail factors; the
+    head-table path alone must reproduce the reference."""
+    shape, S = (96, 4, 4), 1
+    D, lam = np.array([1e8]), np.array([0.1])
+    rho0 = rng.random((*shape, S))
+    env = make_env(bfb, rho0, D, lam, bfb.FP64)
+    env.diffusion_step(0.01, 2)
+    assert np.array_equal(env.get_field(), oracle.lod_steps(rho0, 0.01, 20.0, D, lam, 2))
+
+
 def test_agents_random_fp64_and_fp32(bfb, oracle, rng):
     shape, S = (20, 18, 16), 3
     dx, dt = 20.0, 0.01
@@ -213,13 +226,54 @@ def test_agents_random_fp64_and_fp32(bfb, oracle, rng):
             assert rel_linf(got, want) <= FP32_TOL
 
 
-def test_checksum_matches_oracle(bfb, oracle, rng):
-    rho = rng.random((30, 20, 25, 3))
+@pytest.mark.parametrize("shape,S", [((30, 20, 25), 3), ((7, 5, 3), 64), ((2, 3, 1), 1), ((40, 3, 64), 7),
+                                     ((5, 4, 3), 33), ((64, 64, 64), 8)])
+def test_checksum_matches_oracle(bfb, oracle, rng, shape, S):
+    """One pass of per-substrate FP64 sums, against the oracle's voxel-order sum
+    (fewer voxels than reduction blocks included)."""
+    rho = rng.random((*shape, S))
     for prec in (bfb.FP64, bfb.FP32):
-        env = make_env(bfb, rho, [1e3] * 3, [0.1] * 3, prec)
+        env = make_env(bfb, rho, [1e3] * S, [0.1] * S, prec)
         want = oracle.checksum(rho if prec == bfb.FP64 else rho.astype(np.float32).astype(np.float64))
         got = env.checksum()
         assert np.allclose(got, want, rtol=1e-12, atol=0)
+        env.close()
+
+
+def test_checksum_256cube_bandwidth(bfb):
+    """The per-substrate mass checksum at the bench size reads the field once;
+    timed with CUDA events on one stream (through the allocation-free entry
+    point, which queues the same kernels without waiting) and reported."""
+    import ctypes
+
+    import torch
+
+    S, n = 8, 256 ** 3
+    L = bfb.load_library()
+    out = torch.zeros(S, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    for prec, eb in ((bfb.FP32, 4), (bfb.FP64, 8)):
+        env = bfb.Env((256, 256, 256), S, precision=prec)
+        torch.cuda.synchronize()
+
+        def call():
+            rc = L.bfb_checksum_noalloc(ctypes.c_void_p(env.field_device_ptr()), prec, n, S,
+                                        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+            assert rc == 0, L.bfb_last_error()
+
+        for _ in range(3):
+            call()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(10):
+            call()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        print(f"\nchecksum 256^3 x 8 {'FP32' if eb == 4 else 'FP64'}: {ms:.3f} ms per call, "
+              f"{n * S * eb / (ms / 1e3) / 1e9:.0f} GB/s (one read of the field)")
+        assert ms > 0
+        env.close()
 
 
 def test_graph_replay_equals_direct_launches(bfb, rng):

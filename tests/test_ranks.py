@@ -81,15 +81,19 @@ def _rank_main(rank, world, port, q):
         import datetime
         dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
         ranks, bench = load_ranks(), load_bench()
-        w = ensemble_weights()
-        # every rank derives the same partition without communicating
+        # the benchmark's uneven ensemble: every rank derives the same specs and
+        # the same partition without communicating
+        specs = bench.ensemble_specs()
+        w = [ranks.instance_bytes(sp["shape"], sp["S"], 4) for sp in specs]
         owner = ranks.shard_instances(w, world)
         mine = ranks.local_instances(w, rank, world)
         assert all(owner[i] == rank for i in mine)
-        # stand-in per-instance results: a checksum per substrate slot computed from the instance id
-        vals = [[float(i), float(i) * 0.5] for i in mine]
-        g = bench.gather_by_instance(mine, vals, len(w), 2)
-        expect = np.stack([np.arange(len(w), dtype=float), np.arange(len(w)) * 0.5], axis=1)
+        loads = [sum(x for x, o in zip(w, owner) if o == r) for r in range(world)]
+        assert max(loads) - sum(w) / world <= max(w)
+        # host-computed per-instance values, gathered by instance id
+        vals = [[float(specs[i]["D"].sum()), float(specs[i]["lam"].sum()), float(specs[i]["agents"])] for i in mine]
+        g = bench.gather_by_instance(mine, vals, len(specs), 3)
+        expect = np.array([[sp["D"].sum(), sp["lam"].sum(), sp["agents"]] for sp in specs])
         assert np.array_equal(g, expect)
         # timed region of a multi-GPU run: the slowest rank's
         t = 1.25 + rank
