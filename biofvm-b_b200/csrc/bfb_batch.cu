@@ -407,8 +407,13 @@ static int batch_upload(bfb_batch_s *b, double dt) {
         {
             const long long L = (long long)e->nz * e->S;
             const bool base16 = (reinterpret_cast<uintptr_t>(e->field) & 15) == 0;
-            I.tma[2] = e->use_tma && e->tuning.tma[2] && e->S <= 32 && base16 && (L * eb) % 16 == 0 &&
-                       ((long long)I.gz.RS * eb) % 16 == 0 && (L * eb) * I.gz.R < (1 << 20);
+            const bool tma_ok = e->use_tma && e->tuning.tma[2] && e->S <= 32 && base16 && (L * eb) % 16 == 0;
+            if (tma_ok && ((long long)I.gz.RS * eb) % 16 != 0 &&
+                contig_aligned_geom(e->nz, e->S, eb, &I.gz.R, &I.gz.RS)) {  // 16-byte shared rows, fewer rows
+                I.tiles[2] = (int)((I.gz.nrows + I.gz.R - 1) / I.gz.R);
+                I.items[2] = (I.tiles[2] + b->tiles_per_item - 1) / b->tiles_per_item;
+            }
+            I.tma[2] = tma_ok && ((long long)I.gz.RS * eb) % 16 == 0 && (L * eb) * I.gz.R < (1 << 20);
             int q = 16;
             for (int v = e->S * eb; v % 2 == 0 && q > 1; v /= 2) q /= 2;  // q = 16 / gcd(16, S*elem)
             const int chunks = e->tuning.chunks[2];

@@ -398,6 +398,32 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, co
                     : go_strided<T, (int)sizeof(T), false>(a, g, warps, smem, s);
 }
 
+bool contig_aligned_geom(int nz, int S, int elem, int *R, int *RS) {
+    if (elem != 4 || S > 32) return false;
+    const int L = nz * S;
+    const int base = (L + 3) / 4 * 4;
+    int best_r = 0, best_rs = 0;
+    for (int t = 0; t < 8; ++t) {  // base + 4t: every multiple of 4 (mod 32) once
+        const int rs = base + 4 * t;
+        unsigned used = 0;
+        int r = 0;
+        for (; r < 32 / S; ++r) {
+            unsigned m = 0;
+            for (int d = 0; d < S; ++d) m |= 1u << ((r * rs + d) % 32);
+            if (m & used) break;
+            used |= m;
+        }
+        if (r > best_r) {
+            best_r = r;
+            best_rs = rs;
+        }
+    }
+    if (best_r * S < 16) return false;
+    *R = best_r;
+    *RS = best_rs;
+    return true;
+}
+
 template <typename T, int VB>
 static int go_contig(const SweepArgs<T> &a, const ContigGeom &g, int warps, size_t smem, cudaStream_t s) {
     const long long tiles = (g.nrows + g.R - 1) / g.R;
@@ -437,9 +463,15 @@ int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s
     const long long L = (long long)a.nz * a.S;
     const bool base16 = (reinterpret_cast<uintptr_t>(a.f) & 15) == 0;
     const int eb = (int)sizeof(T);
-    if (use_tma && base16 && (L * eb) % 16 == 0 && ((long long)g.RS * eb) % 16 == 0 && (L * eb) * g.R < (1 << 20)) {
-        const int st = launch_contig_tma<T>(a, g, warps, s, chunks);
-        if (st != kNotApplicable) return st;
+    if (use_tma && base16 && (L * eb) % 16 == 0) {
+        // the bulk-copy tile needs 16-byte shared rows: contig_smem's
+        // conflict-free stride where it is one, else contig_aligned_geom's
+        ContigGeom gt = g;
+        const bool ok = ((long long)g.RS * eb) % 16 == 0 || contig_aligned_geom(a.nz, a.S, eb, &gt.R, &gt.RS);
+        if (ok && (L * eb) * gt.R < (1 << 20)) {
+            const int st = launch_contig_tma<T>(a, gt, warps, s, chunks);
+            if (st != kNotApplicable) return st;
+        }
     }
     if (base16 && (L * eb) % 16 == 0 && ((long long)g.RS * eb) % 16 == 0) return go_contig<T, 16>(a, g, warps, smem, s);
     if (eb < 8 && (L * eb) % 8 == 0 && ((long long)g.RS * eb) % 8 == 0) return go_contig<T, 8>(a, g, warps, smem, s);

@@ -128,6 +128,13 @@ int launch_bulk(const SweepArgs<T> &a, long long N, cudaStream_t s);
 // shared-memory bytes a strided / contiguous CTA needs (0 if it does not fit)
 size_t strided_smem(int n, int elem, int warps);
 size_t contig_smem(int nz, int S, int elem, int warps, int *R, int *RS);
+// Rows per warp tile R and shared row stride RS for the bulk-copy z tile where
+// contig_smem's conflict-free stride (RS = S mod 32) is not a multiple of 16
+// bytes (S not a multiple of 4 in FP32): RS >= nz*S a multiple of 16 bytes,
+// chosen among the eight residues mod 32 so that the most rows keep lane
+// (r, d)'s words r*RS + d apart mod 32 (no bank conflicts). FP32 only (FP64
+// words pair banks); false when fewer than 16 lanes would be busy (S = 1).
+bool contig_aligned_geom(int nz, int S, int elem, int *R, int *RS);
 
 // Opt the shared-memory kernels into 227 KB, once per device.
 void sweeps_prepare_device();

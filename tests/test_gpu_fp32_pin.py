@@ -74,7 +74,8 @@ def run_both(bfb, oracle, rng, shape, S, tma, mode, steps=3):
 
 PIN_SHAPES = [((24, 20, 16), 1), ((24, 20, 16), 3), ((24, 20, 16), 8), ((15, 13, 11), 3), ((17, 9, 33), 5),
               ((6, 5, 7), 33), ((1, 4, 6), 2), ((2, 3, 1), 3), ((40, 3, 64), 7),
-              ((100, 6, 8), 3), ((5, 130, 4), 2)]  # lines of about 100 rows
+              ((100, 6, 8), 3), ((5, 130, 4), 2),  # lines of about 100 rows
+              ((20, 9, 16), 5), ((10, 10, 10), 6), ((9, 7, 12), 7)]  # z rows of whole 16-byte vectors, S not 4 or 8
 
 
 @pytest.mark.parametrize("mode", ["none", "all_faces_uniform", "x_faces_only", "per_voxel_values"])
