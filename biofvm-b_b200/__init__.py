@@ -53,7 +53,7 @@ EXPORTS = [
     "bfb_last_error", "bfb_version", "bfb_create", "bfb_create_domain", "bfb_destroy", "bfb_get_shape",
     "bfb_set_stream", "bfb_set_option", "bfb_synchronize", "bfb_set_coefficients", "bfb_set_field",
     "bfb_get_field", "bfb_set_field_raw", "bfb_get_field_raw", "bfb_set_field_device", "bfb_get_field_device",
-    "bfb_compare_fields", "bfb_field_device_ptr", "bfb_set_dirichlet",
+    "bfb_compare_fields", "bfb_field_device_ptr", "bfb_field_pitch", "bfb_set_dirichlet",
     "bfb_set_dirichlet_uniform", "bfb_apply_dirichlet", "bfb_diffusion_step", "bfb_set_bulk", "bfb_bulk_step",
     "bfb_set_agents", "bfb_set_agent_constants", "bfb_agent_voxels", "bfb_cells_step", "bfb_simulate", "bfb_step_host", "bfb_profile_steps",
     "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_write_matlab", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_get_option", "bfb_batch_simulate",
@@ -106,6 +106,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_get_field_device": [_vp, _vp, ctypes.c_int],
         "bfb_compare_fields": [_vp, _vp, _dp],
         "bfb_field_device_ptr": [_vp, ctypes.POINTER(_vp)],
+        "bfb_field_pitch": [_vp, ctypes.POINTER(ctypes.c_int)],
         "bfb_set_dirichlet": [_vp, _vp, _vp, _vp],
         "bfb_set_dirichlet_uniform": [_vp, _vp, _vp, _vp],
         "bfb_apply_dirichlet": [_vp],
@@ -306,9 +307,16 @@ class Env:
         return out[0] / max(out[1], 1e-300), float(np.sqrt(out[2] / max(out[3], 1e-300)))
 
     def field_device_ptr(self) -> int:
+        """The device field: rows (i, j) of nz*S values, field_pitch() elements apart."""
         p = _vp()
         _check(self.L.bfb_field_device_ptr(self.h, ctypes.byref(p)))
         return p.value
+
+    def field_pitch(self) -> int:
+        """Elements between the device field's (i, j) rows: nz*S, or that padded to 16 bytes."""
+        n = ctypes.c_int()
+        _check(self.L.bfb_field_pitch(self.h, ctypes.byref(n)))
+        return n.value
 
     # -- stepping -------------------------------------------------------
     def diffusion_step(self, dt, n=1):

@@ -841,7 +841,7 @@ namespace bfb {
 int env_prepare_step(bfb_env_s *env, double dt, int flags);
 template <typename T>
 SweepArgs<T> env_sweep_args(bfb_env_s *env, int axis, double dt);
-int env_tile_plan(bfb_env_s *env, int elem, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]);
+int env_tile_plan(bfb_env_s *env, int elem, int Lp, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]);
 }  // namespace bfb
 
 using namespace bfb;
@@ -904,16 +904,22 @@ struct Adjoint {
     long long tiles_z = 0;
 
     // tensor maps with the env's row-group counts (so the recompute runs the
-    // env's tuned launch shape)
+    // env's tuned launch shape); workspace buffers are packed (rows nz*S apart)
     void map(Buf &b) {
         for (int a = 0; a < 2; ++a)
             b.ok[a] = env->use_tma && make_sweep_tensor_map(&b.map[a], &b.crow[a], b.p, sizeof(T), a, env->nx,
-                                                            env->ny, env->nz, S, env->tuning.chunks[a]);
+                                                            env->ny, env->nz, S, env->tuning.chunks[a], env->nz * S);
+    }
+    // the env's sweep arguments over packed workspace buffers
+    SweepArgs<T> args(int axis) const {
+        SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
+        a.Lp = env->nz * S;
+        return a;
     }
 
     // one forward sweep, out of place, in the env's launch shape
     int fwd(int axis, Buf &in, Buf &out) {
-        SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
+        SweepArgs<T> a = args(axis);
         a.f = static_cast<T *>(in.p);
         a.fo = static_cast<T *>(out.p);
         const int warps = env->tuning.warps[axis];
@@ -963,7 +969,7 @@ struct Adjoint {
 
     // one adjoint sweep: lam (in) and y (stored forward output) -> mu (out)
     int adj(int axis, Buf &lam, Buf &y, Buf &mu) {
-        SweepArgs<T> a = env_sweep_args<T>(env, axis, dt);
+        SweepArgs<T> a = args(axis);
         a.f = static_cast<T *>(lam.p);
         a.fo = static_cast<T *>(mu.p);
         const AdjTerms t{coef, coef + S, axis == 0 ? part_x : (axis == 1 ? part_y : part_z)};
@@ -1022,7 +1028,7 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
     A.st = st;
     A.S = S;
     int vb16[3];
-    if ((rc = env_tile_plan(env, sizeof(T), &A.gx, &A.gy, &A.gz, vb16))) return rc;
+    if ((rc = env_tile_plan(env, sizeof(T), env->nz * S, &A.gx, &A.gy, &A.gz, vb16))) return rc;
     opt_in_all<T>();
     const long long tiles_x = (long long)A.gx.n_slabs * A.gx.ncb, tiles_y = (long long)A.gy.n_slabs * A.gy.ncb;
     A.tiles_z = (A.gz.nrows + A.gz.R - 1) / A.gz.R;
@@ -1050,6 +1056,11 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
     std::vector<T *> ckpt(nseg - 1);
     std::vector<Buf> S1(K), S2(K), W(K);
     Buf lam, mu, ck;
+    // the env's field rows are padded where nz*S elements are not whole 16-byte
+    // vectors; the workspace is packed, and the last segment then starts from
+    // a packed copy of the field (head)
+    const bool padded = env->Lp != env->nz * S;
+    T *head = nullptr;
     T *vkeep = nullptr;
     double *part = nullptr, *gacc = nullptr, *gt1 = nullptr, *gt2 = nullptr, *coef = nullptr;
     auto carve = [&](Carve &c) {
@@ -1065,6 +1076,7 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
             c.take(&p, fb);
             b->p = p;
         }
+        c.take(&head, padded ? fb : 0);
         c.take(&part, sizeof(double) * 2 * S * slots);
         c.take(&gacc, sizeof(double) * 2 * S);
         c.take(&coef, sizeof(double) * 2 * S);
@@ -1135,24 +1147,42 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
         return BFB_OK;
     };
 
+    // field (rows Lp apart) <-> packed workspace
+    const size_t row_b = (size_t)env->nz * S * sizeof(T), field_b = (size_t)env->Lp * sizeof(T);
+    const size_t nrows = (size_t)env->nx * env->ny;
+    auto from_field = [&](T *dst) {
+        return padded ? cudaMemcpy2DAsync(dst, row_b, env->field, field_b, row_b, nrows, cudaMemcpyDeviceToDevice, st)
+                      : cudaMemcpyAsync(dst, env->field, fb, cudaMemcpyDeviceToDevice, st);
+    };
+
     // ---- forward: checkpoints of the earlier segments, stage fields of the last
     const int fwd_flags = BFB_STEP_DIFFUSION | (cells ? BFB_STEP_CELLS : 0);
     for (int s = 0; s < nseg - 1; ++s) {
-        BFB_CUDA(cudaMemcpyAsync(ckpt[s], env->field, fb, cudaMemcpyDeviceToDevice, st));
+        BFB_CUDA(from_field(ckpt[s]));
         if ((rc = bfb_simulate(env, dt, K, fwd_flags))) return rc;
     }
     const int last_len = n_steps - (nseg - 1) * K;
     {
         Buf f;
-        f.p = env->field;
-        for (int a = 0; a < 2; ++a) {
-            f.ok[a] = env->use_tma && env->tma_ok[a];
-            f.map[a] = env->tmap[a];
-            f.crow[a] = env->tma_crow[a];
+        if (padded) {
+            BFB_CUDA(from_field(head));
+            f.p = head;
+            A.map(f);
+        } else {  // the field itself, with its own tensor maps
+            f.p = env->field;
+            for (int a = 0; a < 2; ++a) {
+                f.ok[a] = env->use_tma && env->tma_ok[a];
+                f.map[a] = env->tmap[a];
+                f.crow[a] = env->tma_crow[a];
+            }
         }
         if ((rc = segment(f, last_len))) return rc;
     }
-    BFB_CUDA(cudaMemcpyAsync(env->field, W[last_len - 1].p, fb, cudaMemcpyDeviceToDevice, st));
+    if (padded)
+        BFB_CUDA(cudaMemcpy2DAsync(env->field, field_b, W[last_len - 1].p, row_b, row_b, nrows,
+                                   cudaMemcpyDeviceToDevice, st));
+    else
+        BFB_CUDA(cudaMemcpyAsync(env->field, W[last_len - 1].p, fb, cudaMemcpyDeviceToDevice, st));
     if (final_field) BFB_CUDA(cudaMemcpyAsync(final_field, W[last_len - 1].p, fb, cudaMemcpyDeviceToDevice, st));
     BFB_CUDA(cudaMemcpyAsync(lam.p, dL_dfinal, fb, cudaMemcpyDeviceToDevice, st));
 

@@ -20,6 +20,34 @@ __global__ void f2d_kernel(const float *__restrict__ s, double *__restrict__ d, 
 }
 static unsigned grid_for(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 32); }
 
+template <typename TS, typename TD>
+__global__ void convert_rows_kernel(const TS *__restrict__ s, TD *__restrict__ d, long long rows, int L, int sp,
+                                    int dp) {
+    const long long n = rows * L;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long r = e / L, q = e - r * L;
+        if constexpr (sizeof(TD) == 4)
+            d[r * dp + q] = __double2float_rn(s[r * sp + q]);
+        else
+            d[r * dp + q] = (double)s[r * sp + q];
+    }
+}
+
+int launch_convert_d2f_rows(const double *src, float *dst, long long rows, int L, int sp, int dp, cudaStream_t s) {
+    if (sp == L && dp == L) return launch_convert_d2f(src, dst, rows * L, s);
+    if (rows * L <= 0) return BFB_OK;
+    convert_rows_kernel<double, float><<<grid_for(rows * L), 256, 0, s>>>(src, dst, rows, L, sp, dp);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+int launch_convert_f2d_rows(const float *src, double *dst, long long rows, int L, int sp, int dp, cudaStream_t s) {
+    if (sp == L && dp == L) return launch_convert_f2d(src, dst, rows * L, s);
+    if (rows * L <= 0) return BFB_OK;
+    convert_rows_kernel<float, double><<<grid_for(rows * L), 256, 0, s>>>(src, dst, rows, L, sp, dp);
+    BFB_CUDA(cudaGetLastError());
+    return BFB_OK;
+}
+
 int launch_convert_d2f(const double *src, float *dst, long long n, cudaStream_t s) {
     if (n <= 0) return BFB_OK;
     d2f_kernel<<<grid_for(n), 256, 0, s>>>(src, dst, n);
@@ -105,12 +133,12 @@ __global__ void gather_constants_kernel(int n_active, int S, const int *__restri
 
 // BioFVM_basic_agent.cpp:291-296 for all agents of one voxel, in list order.
 template <typename T>
-__global__ void cells_kernel(T *__restrict__ f, int S, int n_occ, const int *__restrict__ seg_start,
+__global__ void cells_kernel(T *__restrict__ f, int S, int nz, int Lp, int n_occ, const int *__restrict__ seg_start,
                              const int *__restrict__ seg_voxel, const T *__restrict__ t1, const T *__restrict__ t2) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)n_occ * S) return;
     const int s = (int)(e / S), d = (int)(e % S);
-    const size_t fe = (size_t)seg_voxel[s] * S + d;
+    const size_t fe = voxel_elem(seg_voxel[s], d, nz, S, Lp);
     T x = f[fe];
     const int a1 = seg_start[s + 1];
     for (int a = seg_start[s]; a < a1; ++a) {
@@ -281,10 +309,12 @@ int launch_cells(bfb_env_s *env, cudaStream_t s) {
     const long long tot = (long long)env->n_occ * env->S;
     const unsigned gb = (unsigned)((tot + 255) / 256);
     if (env->precision == BFB_FP64)
-        cells_kernel<double><<<gb, 256, 0, s>>>((double *)env->field, env->S, env->n_occ, env->seg_start,
+        cells_kernel<double><<<gb, 256, 0, s>>>((double *)env->field, env->S, env->nz, env->Lp, env->n_occ,
+                                                env->seg_start,
                                                 env->seg_voxel, (const double *)env->ag_t1, (const double *)env->ag_t2);
     else
-        cells_kernel<float><<<gb, 256, 0, s>>>((float *)env->field, env->S, env->n_occ, env->seg_start,
+        cells_kernel<float><<<gb, 256, 0, s>>>((float *)env->field, env->S, env->nz, env->Lp, env->n_occ,
+                                               env->seg_start,
                                                env->seg_voxel, (const float *)env->ag_t1, (const float *)env->ag_t2);
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
@@ -381,6 +411,33 @@ __global__ void __launch_bounds__(kSumThreads) checksum_partial_kernel(const T *
     }
 }
 
+// The same sums over a field with padded rows (rows of L = nz*S elements, Lp
+// apart): block b sums rows [r0, r1); thread t < W = R*S takes positions
+// t, t + W, ... of every row, all of substrate t mod S; then, as above,
+// thread d < S adds its substrate's W / S accumulators in order.
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads) checksum_rows_kernel(const T *__restrict__ f, long long rows, int L,
+                                                                    int Lp, int S, double *__restrict__ partials) {
+    __shared__ double red[kSumThreads];
+    const int W = kSumThreads / S * S;
+    const int t = threadIdx.x;
+    const long long per = (rows + gridDim.x - 1) / gridDim.x;
+    const long long r0 = min(rows, (long long)blockIdx.x * per), r1 = min(rows, r0 + per);
+    double acc = 0.0;
+    if (t < W)
+        for (long long r = r0; r < r1; ++r) {
+            const T *__restrict__ row = f + (size_t)r * Lp;
+            for (int q = t; q < L; q += W) acc += (double)row[q];
+        }
+    red[t] = t < W ? acc : 0.0;
+    __syncthreads();
+    if (t < S) {
+        double sum = 0.0;
+        for (int q = t; q < W; q += S) sum += red[q];
+        partials[(size_t)blockIdx.x * S + t] = sum;
+    }
+}
+
 __global__ void checksum_final_kernel(const double *__restrict__ partials, int nblocks, int S, double *__restrict__ out) {
     const int d = threadIdx.x;
     if (d >= S) return;
@@ -398,6 +455,18 @@ int checksum_prepare(bfb_env_s *env) {
 
 int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s) {
     if (env->S > kMaxSumS) return fail(BFB_ERR_UNSUPPORTED, "checksum supports at most 64 substrates");
+    if (env->Lp != env->nz * env->S) {  // padded rows
+        const long long rows = (long long)env->nx * env->ny;
+        if (env->precision == BFB_FP64)
+            checksum_rows_kernel<double><<<kSumBlocks, kSumThreads, 0, s>>>(
+                (const double *)env->field, rows, env->nz * env->S, env->Lp, env->S, env->partials);
+        else
+            checksum_rows_kernel<float><<<kSumBlocks, kSumThreads, 0, s>>>(
+                (const float *)env->field, rows, env->nz * env->S, env->Lp, env->S, env->partials);
+        checksum_final_kernel<<<1, kMaxSumS, 0, s>>>(env->partials, kSumBlocks, env->S, out_dev);
+        BFB_CUDA(cudaGetLastError());
+        return BFB_OK;
+    }
     if (env->precision == BFB_FP64)
         checksum_partial_kernel<double><<<kSumBlocks, kSumThreads, 0, s>>>((const double *)env->field, env->V, env->S,
                                                                          env->partials);
@@ -414,11 +483,14 @@ int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s) {
 // block, summed in block order on the host).
 // ---------------------------------------------------------------------------
 template <typename TA, typename TB>
-__global__ void compare_kernel(const TA *__restrict__ a, const TB *__restrict__ b, long long N, double *__restrict__ part) {
+__global__ void compare_kernel(const TA *__restrict__ a, int la, const TB *__restrict__ b, int lb, long long rows, int L,
+                               double *__restrict__ part) {
     __shared__ double s0[256], s1[256], s2[256], s3[256];
     double mx = 0, mb = 0, sd = 0, sb = 0;
+    const long long N = rows * L;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (long long)gridDim.x * blockDim.x) {
-        const double x = (double)a[e], y = (double)b[e], df = x - y;
+        const long long r = (la == L && lb == L) ? 0 : e / L, q = e - r * L;
+        const double x = (double)a[r * la + q], y = (double)b[r * lb + q], df = x - y;
         mx = fmax(mx, fabs(df));
         mb = fmax(mb, fabs(y));
         sd += df * df;
@@ -446,18 +518,19 @@ __global__ void compare_kernel(const TA *__restrict__ a, const TB *__restrict__ 
     }
 }
 
-int compare_fields(const void *a, int pa, const void *b, int pb, long long N, double *out4, cudaStream_t s) {
+int compare_fields(const void *a, int pa, int la, const void *b, int pb, int lb, long long rows, int L, double *out4,
+                   cudaStream_t s) {
     const int blocks = 592;
     double *part = nullptr;
     BFB_CUDA(cudaMalloc(&part, sizeof(double) * 4 * blocks));
     if (pa == BFB_FP64 && pb == BFB_FP64)
-        compare_kernel<<<blocks, 256, 0, s>>>((const double *)a, (const double *)b, N, part);
+        compare_kernel<<<blocks, 256, 0, s>>>((const double *)a, la, (const double *)b, lb, rows, L, part);
     else if (pa == BFB_FP32 && pb == BFB_FP64)
-        compare_kernel<<<blocks, 256, 0, s>>>((const float *)a, (const double *)b, N, part);
+        compare_kernel<<<blocks, 256, 0, s>>>((const float *)a, la, (const double *)b, lb, rows, L, part);
     else if (pa == BFB_FP64 && pb == BFB_FP32)
-        compare_kernel<<<blocks, 256, 0, s>>>((const double *)a, (const float *)b, N, part);
+        compare_kernel<<<blocks, 256, 0, s>>>((const double *)a, la, (const float *)b, lb, rows, L, part);
     else
-        compare_kernel<<<blocks, 256, 0, s>>>((const float *)a, (const float *)b, N, part);
+        compare_kernel<<<blocks, 256, 0, s>>>((const float *)a, la, (const float *)b, lb, rows, L, part);
     std::vector<double> h(4 * blocks);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), part, sizeof(double) * 4 * blocks, cudaMemcpyDeviceToHost, s);

@@ -7,6 +7,10 @@ namespace bfb {
 // Field precision conversion (device).
 int launch_convert_d2f(const double *src, float *dst, long long n, cudaStream_t s);
 int launch_convert_f2d(const float *src, double *dst, long long n, cudaStream_t s);
+// The same over `rows` rows of L elements, src rows `sp` and dst rows `dp`
+// elements apart (packed V*S <-> a field with padded rows).
+int launch_convert_d2f_rows(const double *src, float *dst, long long rows, int L, int sp, int dp, cudaStream_t s);
+int launch_convert_f2d_rows(const float *src, double *dst, long long rows, int L, int sp, int dp, cudaStream_t s);
 
 // Agents: binning + cached constants (FP64, bit-exact with the reference),
 // then a stable voxel sort and per-voxel segments. All device memory of the
@@ -24,8 +28,10 @@ int launch_cells(bfb_env_s *env, cudaStream_t s);
 // env->partials (allocated on demand, outside any stream capture).
 int checksum_prepare(bfb_env_s *env);
 int launch_checksum(bfb_env_s *env, double *out_dev, cudaStream_t s);
-// max|a-b|, max|b|, sum (a-b)^2, sum b^2 of two device fields of N elements.
-int compare_fields(const void *a, int pa, const void *b, int pb, long long N, double *out4, cudaStream_t s);
+// max|a-b|, max|b|, sum (a-b)^2, sum b^2 of two device fields of `rows` rows
+// of L elements, a's rows la and b's rows lb elements apart.
+int compare_fields(const void *a, int pa, int la, const void *b, int pb, int lb, long long rows, int L, double *out4,
+                   cudaStream_t s);
 // The same kernels on caller-provided scratch (partials: nblocks*S doubles).
 int launch_checksum_raw(const void *field, int precision, long long V, int S, double *partials, int nblocks,
                         double *out_dev, cudaStream_t s);

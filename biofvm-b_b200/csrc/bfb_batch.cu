@@ -55,8 +55,8 @@ struct BatchInst {
     int crow[2];         // rows per TMA box (x, y)
     int kc;              // z row-group length of the pipelined tile
     const CUtensorMap *map[2];  // the env field's x / y tensor maps, in global memory
-    T *f;
-    int S, n_occ;
+    T *f;                // the env's field, (i, j) rows Lp elements apart
+    int S, nz, Lp, n_occ;
     const int *seg_start, *seg_voxel;
     const T *t1, *t2;
 };
@@ -123,7 +123,7 @@ __device__ void cells_chunk(const BatchInst<T> &I, int chunk) {
     const long long e1 = min(total, e0 + kCellChunk);
     for (long long e = e0 + lane; e < e1; e += 32) {
         const int sidx = (int)(e / I.S), d = (int)(e % I.S);
-        const size_t fe = (size_t)I.seg_voxel[sidx] * I.S + d;
+        const size_t fe = voxel_elem(I.seg_voxel[sidx], d, I.nz, I.S, I.Lp);
         T x = I.f[fe];
         const int a1 = I.seg_start[sidx + 1];
         for (int q = I.seg_start[sidx]; q < a1; ++q) {
@@ -366,7 +366,7 @@ namespace bfb {
 int env_prepare_step(bfb_env_s *env, double dt, int flags);
 template <typename T>
 SweepArgs<T> env_sweep_args(bfb_env_s *env, int axis, double dt);
-int env_tile_plan(bfb_env_s *env, int elem, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]);
+int env_tile_plan(bfb_env_s *env, int elem, int Lp, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]);
 }  // namespace bfb
 
 using namespace bfb;
@@ -385,7 +385,7 @@ static int batch_upload(bfb_batch_s *b, double dt) {
         bfb_env_s *e = b->envs[k];
         BatchInst<T> &I = inst[k];
         for (int a = 0; a < 3; ++a) I.ax[a] = env_sweep_args<T>(e, a, dt);
-        int st = env_tile_plan(e, sizeof(T), &I.gx, &I.gy, &I.gz, I.vb16);
+        int st = env_tile_plan(e, sizeof(T), e->Lp, &I.gx, &I.gy, &I.gz, I.vb16);
         if (st) return st;
         I.tiles[0] = I.gx.n_slabs * I.gx.ncb;
         I.tiles[1] = I.gy.n_slabs * I.gy.ncb;
@@ -405,11 +405,11 @@ static int batch_upload(bfb_batch_s *b, double dt) {
             ebytes[(size_t)a * b->n + k] = tb;
         }
         {
-            const long long L = (long long)e->nz * e->S;
+            const long long L = e->Lp;  // row pitch
             const bool base16 = (reinterpret_cast<uintptr_t>(e->field) & 15) == 0;
             const bool tma_ok = e->use_tma && e->tuning.tma[2] && e->S <= 32 && base16 && (L * eb) % 16 == 0;
             if (tma_ok && ((long long)I.gz.RS * eb) % 16 != 0 &&
-                contig_aligned_geom(e->nz, e->S, eb, &I.gz.R, &I.gz.RS)) {  // 16-byte shared rows, fewer rows
+                contig_aligned_geom(e->nz, e->S, e->Lp, eb, &I.gz.R, &I.gz.RS)) {  // 16-byte shared rows, fewer rows
                 I.tiles[2] = (int)((I.gz.nrows + I.gz.R - 1) / I.gz.R);
                 I.items[2] = (I.tiles[2] + b->tiles_per_item - 1) / b->tiles_per_item;
             }
@@ -425,6 +425,8 @@ static int batch_upload(bfb_batch_s *b, double dt) {
         }
         I.f = static_cast<T *>(e->field);
         I.S = e->S;
+        I.nz = e->nz;
+        I.Lp = e->Lp;
         I.n_occ = e->n_occ;
         I.seg_start = e->seg_start;
         I.seg_voxel = e->seg_voxel;
@@ -774,8 +776,8 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
     for (int k = 0; k < b->n && !st; ++k) {
         bfb_env_s *e = b->envs[k];
         cudaError_t ce = cudaStreamSynchronize(e->stream);
-        if (ce == cudaSuccess) ce = cudaMalloc(&saved[k], e->elem * e->N);
-        if (ce == cudaSuccess) ce = cudaMemcpy(saved[k], e->field, e->elem * e->N, cudaMemcpyDeviceToDevice);
+        if (ce == cudaSuccess) ce = cudaMalloc(&saved[k], e->elem * e->Np);
+        if (ce == cudaSuccess) ce = cudaMemcpy(saved[k], e->field, e->elem * e->Np, cudaMemcpyDeviceToDevice);
         if (ce != cudaSuccess) st = cuda_fail(ce, "bfb_batch_autotune: field copy");
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -828,7 +830,7 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
     for (int k = 0; k < b->n; ++k) {
         if (!saved[k]) continue;
         bfb_env_s *e = b->envs[k];
-        const cudaError_t ce = cudaMemcpy(e->field, saved[k], e->elem * e->N, cudaMemcpyDeviceToDevice);
+        const cudaError_t ce = cudaMemcpy(e->field, saved[k], e->elem * e->Np, cudaMemcpyDeviceToDevice);
         if (ce != cudaSuccess && !st) st = cuda_fail(ce, "bfb_batch_autotune: field restore");
         cudaFree(saved[k]);
     }

@@ -80,6 +80,22 @@ static int upload_table(bfb_env_s *env, void *dst, const std::vector<double> &v)
     return BFB_OK;
 }
 
+// A packed V*S host table (the reference layout) into a device array laid
+// out like the field (rows at the pitch Lp), in the env's precision.
+static int upload_pitched_table(bfb_env_s *env, void *dst, const std::vector<double> &v) {
+    const size_t rows = (size_t)env->nx * env->ny, L = (size_t)env->nz * env->S;
+    const size_t eb = env->elem;
+    std::vector<float> f;
+    const void *src = v.data();
+    if (env->precision == BFB_FP32) {
+        f.resize(v.size());
+        for (size_t q = 0; q < v.size(); ++q) f[q] = (float)v[q];
+        src = f.data();
+    }
+    BFB_CUDA(cudaMemcpy2D(dst, (size_t)env->Lp * eb, src, L * eb, L * eb, rows, cudaMemcpyHostToDevice));
+    return BFB_OK;
+}
+
 // First row from which every table is bitwise constant up to row n-2, over
 // all substrates (at least 1; n-1 when there is no such tail).
 static int tail_start(const std::vector<std::vector<double>> &tabs, int n, int S) {
@@ -187,6 +203,7 @@ static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
     a.ny = env->ny;
     a.nz = env->nz;
     a.S = env->S;
+    a.Lp = env->Lp;
     const int ns[3] = {env->nx, env->ny, env->nz};
     const size_t nS = (size_t)ns[axis] * env->S;
     const T *tab = static_cast<const T *>(env->fac_tab[axis]);
@@ -223,7 +240,7 @@ static const CUtensorMap *tma_map(bfb_env_s *env, int axis) {
 static void encode_field_maps(bfb_env_s *env) {
     for (int a = 0; a < 2; ++a)
         env->tma_ok[a] = make_sweep_tensor_map(&env->tmap[a], &env->tma_crow[a], env->field, (int)env->elem, a,
-                                               env->nx, env->ny, env->nz, env->S, env->tuning.chunks[a]);
+                                               env->nx, env->ny, env->nz, env->S, env->tuning.chunks[a], env->Lp);
 }
 
 // One LOD diffusion step; `bulk` fuses a preceding bulk source/sink update
@@ -251,7 +268,7 @@ static int run_steps(bfb_env_s *env, double dt, int n, int flags, cudaStream_t s
         if (flags & BFB_STEP_DIFFUSION) {
             st = run_diffusion<T>(env, dt, (flags & BFB_STEP_BULK) != 0, s);
         } else if (flags & BFB_STEP_BULK) {
-            st = launch_bulk<T>(make_args<T>(env, 0, true, dt), env->N, s);
+            st = launch_bulk<T>(make_args<T>(env, 0, true, dt), env->Np, s);
         }
         if (st) return st;
         if (flags & BFB_STEP_CELLS) {
@@ -281,29 +298,29 @@ SweepArgs<T> env_sweep_args(bfb_env_s *env, int axis, double dt) {
 template SweepArgs<double> env_sweep_args<double>(bfb_env_s *, int, double);
 template SweepArgs<float> env_sweep_args<float>(bfb_env_s *, int, double);
 
-int env_tile_plan(bfb_env_s *env, int elem, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]) {
+int env_tile_plan(bfb_env_s *env, int elem, int Lp, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]) {
     const bool base16 = (reinterpret_cast<uintptr_t>(env->field) & 15) == 0;
     gx->axis = 0;
     gx->n = env->nx;
-    gx->P = (long long)env->ny * env->nz * env->S;
+    gx->P = (long long)env->ny * Lp;
     gx->slab_stride = 0;
     gx->n_slabs = 1;
     gx->ncb = (int)((gx->P + 31) / 32);
     gy->axis = 1;
     gy->n = env->ny;
-    gy->P = (long long)env->nz * env->S;
-    gy->slab_stride = (long long)env->ny * env->nz * env->S;
+    gy->P = Lp;
+    gy->slab_stride = (long long)env->ny * Lp;
     gy->n_slabs = env->nx;
     gy->ncb = (int)((gy->P + 31) / 32);
     vb16[0] = base16 && (gx->P * elem) % 16 == 0;
     vb16[1] = base16 && (gy->P * elem) % 16 == 0 && (gy->slab_stride * elem) % 16 == 0;
     gz->nz = env->nz;
     gz->nrows = (long long)env->nx * env->ny;
+    gz->Lp = Lp;
     if (!strided_smem(env->nx, elem, 1) || !strided_smem(env->ny, elem, 1) ||
-        !contig_smem(env->nz, env->S, elem, 1, &gz->R, &gz->RS))
+        !contig_smem(env->nz, env->S, Lp, elem, 1, &gz->R, &gz->RS))
         return fail(BFB_ERR_UNSUPPORTED, "batch: an env's lines are too long for a shared-memory tile");
-    const long long L = (long long)env->nz * env->S;
-    vb16[2] = base16 && (L * elem) % 16 == 0 && ((long long)gz->RS * elem) % 16 == 0;
+    vb16[2] = base16 && ((long long)Lp * elem) % 16 == 0 && ((long long)gz->RS * elem) % 16 == 0;
     return BFB_OK;
 }
 
@@ -328,12 +345,20 @@ static int bulk_tabulate(bfb_env_s *env, const double *Sr, const double *T, cons
         A[e] = T[e] * Sr[e];
         B[e] = U[e] + Sr[e];
     }
-    if (!env->bulkA) BFB_CUDA(cudaMalloc(&env->bulkA, env->elem * N));
-    if (!env->bulkB) BFB_CUDA(cudaMalloc(&env->bulkB, env->elem * N));
+    // laid out like the field (rows at its pitch), which the fused x load indexes
+    // (row padding zero, so a whole-array pass leaves padded field entries finite)
+    if (!env->bulkA) {
+        BFB_CUDA(cudaMalloc(&env->bulkA, env->elem * env->Np));
+        BFB_CUDA(cudaMemset(env->bulkA, 0, env->elem * env->Np));
+    }
+    if (!env->bulkB) {
+        BFB_CUDA(cudaMalloc(&env->bulkB, env->elem * env->Np));
+        BFB_CUDA(cudaMemset(env->bulkB, 0, env->elem * env->Np));
+    }
     BFB_CUDA(cudaStreamSynchronize(env->stream));
-    int st = upload_table(env, env->bulkA, A);
+    int st = upload_pitched_table(env, env->bulkA, A);
     if (st) return st;
-    return upload_table(env, env->bulkB, B);
+    return upload_pitched_table(env, env->bulkB, B);
 }
 
 }  // namespace bfb
@@ -387,6 +412,15 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
     env->elem = precision == BFB_FP64 ? 8 : 4;
     env->V = V;
     env->N = V * n_substrates;
+    {   // rows padded to whole 16-byte vectors where nz*S elements are not (TMA needs 16-byte pitches)
+        const long long L = (long long)nz * n_substrates, epv = 16 / (long long)env->elem;
+        if (L > 0x7fffffffLL - epv) {
+            delete env;
+            return fail(BFB_ERR_SIZE, "nz * substrates too large");
+        }
+        env->Lp = (int)((L + epv - 1) / epv * epv);
+        env->Np = (long long)nx * ny * env->Lp;
+    }
     env->D.assign(n_substrates, 0.0);
     env->lambda.assign(n_substrates, 0.0);
     env->activation.assign(n_substrates, 0);
@@ -397,7 +431,7 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
         cudaError_t e = cudaMalloc(p, bytes ? bytes : 1);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaMalloc");
     };
-    alloc(&env->field, env->elem * env->N);
+    alloc(&env->field, env->elem * env->Np);
     const int ns[3] = {nx, ny, nz};
     for (int a = 0; a < 3; ++a) {
         alloc(&env->fac_tab[a], env->elem * 4 * (size_t)ns[a] * n_substrates);
@@ -419,7 +453,7 @@ BFB_API int bfb_create(bfb_env *out, int nx, int ny, int nz, int n_substrates, d
         env->stream = env->own_stream;
     }
     if (!st) {
-        cudaError_t e = cudaMemset(env->field, 0, env->elem * env->N);
+        cudaError_t e = cudaMemset(env->field, 0, env->elem * env->Np);
         if (e == cudaSuccess) e = cudaMemset(env->d_mask, 0, n_substrates);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaMemset");
     }
@@ -553,17 +587,51 @@ static int ensure_staging(bfb_env_s *env) {
     return BFB_OK;
 }
 
+// Field transfers between the packed V*S reference layout (host or device
+// buffers) and the env's field, whose rows may be padded (bfb_env_s::Lp).
+// Same element type: one copy (2-D when the rows are padded).
+static int copy_rows(bfb_env_s *env, void *dst, bool dst_is_field, const void *src, cudaMemcpyKind kind,
+                     size_t eb, cudaStream_t s) {
+    const size_t rows = (size_t)env->nx * env->ny, w = (size_t)env->nz * env->S * eb, pitched = (size_t)env->Lp * eb;
+    if (pitched == w) {
+        BFB_CUDA(cudaMemcpyAsync(dst, src, rows * w, kind, s));
+    } else {
+        BFB_CUDA(cudaMemcpy2DAsync(dst, dst_is_field ? pitched : w, src, dst_is_field ? w : pitched, w, rows, kind, s));
+    }
+    return BFB_OK;
+}
+// Device conversion between FP64 and FP32, packed <-> field layout.
+static int convert_rows(bfb_env_s *env, const void *src, int src_prec, void *dst, bool dst_is_field, cudaStream_t s) {
+    const long long rows = (long long)env->nx * env->ny;
+    const int L = env->nz * env->S;
+    const int sp = dst_is_field ? L : env->Lp, dp = dst_is_field ? env->Lp : L;
+    if (src_prec == BFB_FP64)
+        return launch_convert_d2f_rows((const double *)src, (float *)dst, rows, L, sp, dp, s);
+    return launch_convert_f2d_rows((const float *)src, (double *)dst, rows, L, sp, dp, s);
+}
+// host doubles (packed) -> the field, converting on the device for FP32
+static int field_from_host_doubles(bfb_env_s *env, const double *host, cudaStream_t s) {
+    if (env->precision == BFB_FP64) return copy_rows(env, env->field, true, host, cudaMemcpyHostToDevice, 8, s);
+    int st = ensure_staging(env);
+    if (st) return st;
+    BFB_CUDA(cudaMemcpyAsync(env->staging, host, sizeof(double) * env->N, cudaMemcpyHostToDevice, s));
+    return convert_rows(env, env->staging, BFB_FP64, env->field, true, s);
+}
+// the field -> host doubles (packed)
+static int field_to_host_doubles(bfb_env_s *env, double *host, cudaStream_t s) {
+    if (env->precision == BFB_FP64) return copy_rows(env, host, false, env->field, cudaMemcpyDeviceToHost, 8, s);
+    int st = ensure_staging(env);
+    if (st) return st;
+    if ((st = convert_rows(env, env->field, BFB_FP32, env->staging, false, s))) return st;
+    BFB_CUDA(cudaMemcpyAsync(host, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, s));
+    return BFB_OK;
+}
+
 BFB_API int bfb_set_field(bfb_env env, const double *host) {
     int st = check_env(env);
     if (st) return st;
     if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
-    if (env->precision == BFB_FP64) {
-        BFB_CUDA(cudaMemcpyAsync(env->field, host, sizeof(double) * env->N, cudaMemcpyHostToDevice, env->stream));
-    } else {
-        if ((st = ensure_staging(env))) return st;
-        BFB_CUDA(cudaMemcpyAsync(env->staging, host, sizeof(double) * env->N, cudaMemcpyHostToDevice, env->stream));
-        if ((st = launch_convert_d2f((const double *)env->staging, (float *)env->field, env->N, env->stream))) return st;
-    }
+    if ((st = field_from_host_doubles(env, host, env->stream))) return st;
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     return BFB_OK;
 }
@@ -572,13 +640,7 @@ BFB_API int bfb_get_field(bfb_env env, double *host) {
     int st = check_env(env);
     if (st) return st;
     if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
-    if (env->precision == BFB_FP64) {
-        BFB_CUDA(cudaMemcpyAsync(host, env->field, sizeof(double) * env->N, cudaMemcpyDeviceToHost, env->stream));
-    } else {
-        if ((st = ensure_staging(env))) return st;
-        if ((st = launch_convert_f2d((const float *)env->field, (double *)env->staging, env->N, env->stream))) return st;
-        BFB_CUDA(cudaMemcpyAsync(host, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, env->stream));
-    }
+    if ((st = field_to_host_doubles(env, host, env->stream))) return st;
     return env_check_device_error(env);
 }
 
@@ -586,7 +648,7 @@ BFB_API int bfb_set_field_raw(bfb_env env, const void *host) {
     int st = check_env(env);
     if (st) return st;
     if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
-    BFB_CUDA(cudaMemcpyAsync(env->field, host, env->elem * env->N, cudaMemcpyHostToDevice, env->stream));
+    if ((st = copy_rows(env, env->field, true, host, cudaMemcpyHostToDevice, env->elem, env->stream))) return st;
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     return BFB_OK;
 }
@@ -595,7 +657,7 @@ BFB_API int bfb_get_field_raw(bfb_env env, void *host) {
     int st = check_env(env);
     if (st) return st;
     if (!host) return fail(BFB_ERR_INVALID_ARG, "host is NULL");
-    BFB_CUDA(cudaMemcpyAsync(host, env->field, env->elem * env->N, cudaMemcpyDeviceToHost, env->stream));
+    if ((st = copy_rows(env, host, false, env->field, cudaMemcpyDeviceToHost, env->elem, env->stream))) return st;
     return env_check_device_error(env);
 }
 
@@ -606,11 +668,9 @@ BFB_API int bfb_set_field_device(bfb_env env, const void *src, int src_precision
     if (!src) return fail(BFB_ERR_INVALID_ARG, "src is NULL");
     if (src_precision != BFB_FP64 && src_precision != BFB_FP32) return fail(BFB_ERR_INVALID_ARG, "bad precision");
     if (src_precision == env->precision) {
-        BFB_CUDA(cudaMemcpyAsync(env->field, src, env->elem * env->N, cudaMemcpyDeviceToDevice, env->stream));
-    } else if (src_precision == BFB_FP64) {
-        if ((st = launch_convert_d2f((const double *)src, (float *)env->field, env->N, env->stream))) return st;
+        if ((st = copy_rows(env, env->field, true, src, cudaMemcpyDeviceToDevice, env->elem, env->stream))) return st;
     } else {
-        if ((st = launch_convert_f2d((const float *)src, (double *)env->field, env->N, env->stream))) return st;
+        if ((st = convert_rows(env, src, src_precision, env->field, true, env->stream))) return st;
     }
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     return BFB_OK;
@@ -622,11 +682,9 @@ BFB_API int bfb_get_field_device(bfb_env env, void *dst, int dst_precision) {
     if (!dst) return fail(BFB_ERR_INVALID_ARG, "dst is NULL");
     if (dst_precision != BFB_FP64 && dst_precision != BFB_FP32) return fail(BFB_ERR_INVALID_ARG, "bad precision");
     if (dst_precision == env->precision) {
-        BFB_CUDA(cudaMemcpyAsync(dst, env->field, env->elem * env->N, cudaMemcpyDeviceToDevice, env->stream));
-    } else if (dst_precision == BFB_FP64) {
-        if ((st = launch_convert_f2d((const float *)env->field, (double *)dst, env->N, env->stream))) return st;
+        if ((st = copy_rows(env, dst, false, env->field, cudaMemcpyDeviceToDevice, env->elem, env->stream))) return st;
     } else {
-        if ((st = launch_convert_d2f((const double *)env->field, (float *)dst, env->N, env->stream))) return st;
+        if ((st = convert_rows(env, env->field, env->precision, dst, false, env->stream))) return st;
     }
     return env_check_device_error(env);
 }
@@ -635,15 +693,23 @@ BFB_API int bfb_compare_fields(bfb_env test, bfb_env ref, double *out4) {
     int st = check_env(test);
     if (st) return st;
     if (!ref || !out4) return fail(BFB_ERR_INVALID_ARG, "null argument");
-    if (test->N != ref->N || test->S != ref->S || test->device != ref->device)
+    if (test->nx != ref->nx || test->ny != ref->ny || test->nz != ref->nz || test->S != ref->S ||
+        test->device != ref->device)
         return fail(BFB_ERR_SIZE, "fields differ in shape or device");
     BFB_CUDA(cudaStreamSynchronize(ref->stream));
-    return compare_fields(test->field, test->precision, ref->field, ref->precision, test->N, out4, test->stream);
+    return compare_fields(test->field, test->precision, test->Lp, ref->field, ref->precision, ref->Lp,
+                          (long long)test->nx * test->ny, test->nz * test->S, out4, test->stream);
 }
 
 BFB_API int bfb_field_device_ptr(bfb_env env, void **dptr) {
     if (!env || !dptr) return fail(BFB_ERR_INVALID_ARG, "null argument");
     *dptr = env->field;
+    return BFB_OK;
+}
+
+BFB_API int bfb_field_pitch(bfb_env env, int *row_elems) {
+    if (!env || !row_elems) return fail(BFB_ERR_INVALID_ARG, "null argument");
+    *row_elems = env->Lp;
     return BFB_OK;
 }
 
@@ -872,23 +938,12 @@ BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_step
     if ((st = ensure_factors(env, dt))) return st;
     NvtxRange range("bfb_step_host");
     cudaStream_t s = env->stream;
-    if (env->precision == BFB_FP64) {
-        BFB_CUDA(cudaMemcpyAsync(env->field, host_field, sizeof(double) * env->N, cudaMemcpyHostToDevice, s));
-    } else {
-        if ((st = ensure_staging(env))) return st;
-        BFB_CUDA(cudaMemcpyAsync(env->staging, host_field, sizeof(double) * env->N, cudaMemcpyHostToDevice, s));
-        if ((st = launch_convert_d2f((const double *)env->staging, (float *)env->field, env->N, s))) return st;
-    }
+    if ((st = field_from_host_doubles(env, host_field, s))) return st;
     if ((st = run_steps_any(env, dt, n_steps, BFB_STEP_DIFFUSION, s))) return st;
     // a wait that ran out leaves the device field untrustworthy: report it and
     // leave the caller's host field as it was
     if ((st = env_check_device_error(env))) return st;
-    if (env->precision == BFB_FP64) {
-        BFB_CUDA(cudaMemcpyAsync(host_field, env->field, sizeof(double) * env->N, cudaMemcpyDeviceToHost, s));
-    } else {
-        if ((st = launch_convert_f2d((const float *)env->field, (double *)env->staging, env->N, s))) return st;
-        BFB_CUDA(cudaMemcpyAsync(host_field, env->staging, sizeof(double) * env->N, cudaMemcpyDeviceToHost, s));
-    }
+    if ((st = field_to_host_doubles(env, host_field, s))) return st;
     BFB_CUDA(cudaStreamSynchronize(s));
     return BFB_OK;
 }
@@ -976,9 +1031,9 @@ static int time_candidates(bfb_env_s *env, double dt, int trials, void *scratch,
                     bool maps = false;
                     if (axis < 2 && tma && env->use_tma)
                         maps = make_sweep_tensor_map(&mi, &ci, env->field, (int)env->elem, axis, env->nx, env->ny,
-                                                     env->nz, env->S, chunks) &&
+                                                     env->nz, env->S, chunks, env->Lp) &&
                                make_sweep_tensor_map(&mo, &co, scratch, (int)env->elem, axis, env->nx, env->ny,
-                                                     env->nz, env->S, chunks);
+                                                     env->nz, env->S, chunks, env->Lp);
                     auto launch = [&]() -> int {
                         if (axis < 2)
                             return launch_strided<T>(a, axis, axis == 0, warps, maps ? &mi : nullptr,
@@ -1019,7 +1074,7 @@ BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double
     if ((st = ensure_factors(env, dt))) return st;
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     void *scratch = nullptr;
-    BFB_CUDA(cudaMalloc(&scratch, env->elem * env->N));
+    BFB_CUDA(cudaMalloc(&scratch, env->elem * env->Np));
     int best[9];
     double ms[3];
     bfb_get_tuning(env, best);
@@ -1081,8 +1136,8 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
                 });
         } else if (flags & BFB_STEP_BULK) {
             st = phase_ms(3, [&] {
-                return fp64 ? launch_bulk<double>(make_args<double>(env, 0, true, dt), env->N, s)
-                            : launch_bulk<float>(make_args<float>(env, 0, true, dt), env->N, s);
+                return fp64 ? launch_bulk<double>(make_args<double>(env, 0, true, dt), env->Np, s)
+                            : launch_bulk<float>(make_args<float>(env, 0, true, dt), env->Np, s);
             });
         }
         if (!st && (flags & BFB_STEP_CELLS)) st = phase_ms(4, [&] { return launch_cells(env, s); });

@@ -18,7 +18,8 @@
 // in FP32, h and 2h rounded once to FP32, the quotient by the binary32 form of
 // the same correction (bit for bit with IEEE FP32 division).
 //
-// One block per (i, j) row of nz*S contiguous elements. The x and y
+// One block per (i, j) row of nz*S contiguous elements (field rows are Lp
+// elements apart; the output is packed, 3*nz*S per row). The x and y
 // neighbours are the same element of the rows ny and 1 away, so the field is
 // read from DRAM about once and its neighbour re-reads hit L2. The output is
 // 3x the field.
@@ -50,15 +51,14 @@ __device__ __forceinline__ float grad_diff(float a, float b, float h, float rh) 
 
 template <typename T, int SC>  // SC: the substrate count when a compile-time constant (else 0)
 __global__ void __launch_bounds__(256) gradient_kernel(const T *__restrict__ f, T *__restrict__ out, int nx, int ny,
-                                                       int nz, int S_, T h1, T r1, T h2, T r2) {
+                                                       int nz, int S_, int Lp, T h1, T r1, T h2, T r2) {
     const int S = SC > 0 ? SC : S_;
     const long long row = blockIdx.x;  // i * ny + j
     const int i = (int)(row / ny), j = (int)(row - (long long)i * ny);
     const int L = nz * S;
-    const size_t base = (size_t)row * L;
-    const long long jx = (long long)ny * L, jy = L;
-    const T *__restrict__ fr = f + base;
-    T *__restrict__ o = out + base * 3;
+    const long long jx = (long long)ny * Lp, jy = Lp;  // field rows are Lp elements apart
+    const T *__restrict__ fr = f + (size_t)row * Lp;
+    T *__restrict__ o = out + (size_t)row * L * 3;
     for (int t = threadIdx.x; t < L; t += blockDim.x) {
         const int k = t / S;
         const T v = fr[t];
@@ -142,22 +142,22 @@ __device__ __forceinline__ void axis_grad(const T *p, long long off, bool lo, bo
 
 // The vectorised form of gradient_kernel: same values, same operations per
 // element. Requires nz*S a multiple of VW and 16-byte aligned f and out (the
-// host checks both); every vector then lies in one row, its x / y neighbours
+// host checks both; a row of a multiple of VW elements is never padded, so
+// the field's rows are then L elements apart too); every vector then lies in one row, its x / y neighbours
 // are whole vectors, and so are its z neighbours when S is a multiple of VW
 // (ZV; otherwise they are read per element).
 template <typename T, int SC>
 __global__ void __launch_bounds__(256) gradient_vec_kernel(const T *__restrict__ f, T *__restrict__ out, int nx,
-                                                           int ny, int nz, int S_, T h1, T r1, T h2, T r2) {
+                                                           int ny, int nz, int S_, int Lp, T h1, T r1, T h2, T r2) {
     constexpr int VW = Vec16<T>::n;
     constexpr bool ZV = SC > 0 && SC % VW == 0;
     const int S = SC > 0 ? SC : S_;
     const long long row = blockIdx.x;  // i * ny + j
     const int i = (int)(row / ny), j = (int)(row - (long long)i * ny);
     const int L = nz * S;
-    const size_t base = (size_t)row * L;
-    const long long jx = (long long)ny * L, jy = L;
-    const T *__restrict__ fr = f + base;
-    T *__restrict__ o = out + base * 3;
+    const long long jx = (long long)ny * Lp, jy = Lp;
+    const T *__restrict__ fr = f + (size_t)row * Lp;
+    T *__restrict__ o = out + (size_t)row * L * 3;
     for (int t = threadIdx.x * VW; t < L; t += blockDim.x * VW) {
         T v[VW], g[3][VW];
         ld16(fr + t, v);
@@ -204,7 +204,7 @@ int launch_typed(bfb_env_s *env, void *out, T h1, T r1, T h2, T r2) {
     const T *f = static_cast<const T *>(env->field);
     T *o = static_cast<T *>(out);
     cudaStream_t s = env->stream;
-    const int nx = env->nx, ny = env->ny, nz = env->nz, S = env->S;
+    const int nx = env->nx, ny = env->ny, nz = env->nz, S = env->S, Lp = env->Lp;
     constexpr int VW = Vec16<T>::n;
     const bool vec = L % VW == 0 && (reinterpret_cast<uintptr_t>(f) & 15) == 0 &&
                      (reinterpret_cast<uintptr_t>(o) & 15) == 0;
@@ -212,22 +212,22 @@ int launch_typed(bfb_env_s *env, void *out, T h1, T r1, T h2, T r2) {
         const int nv = L / VW;  // vectors per row
         const int threads = nv >= 256 ? 256 : ((nv + 31) / 32) * 32;
         switch (S) {
-        case 1: gradient_vec_kernel<T, 1><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-        case 2: gradient_vec_kernel<T, 2><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-        case 4: gradient_vec_kernel<T, 4><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-        case 8: gradient_vec_kernel<T, 8><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-        default: gradient_vec_kernel<T, 0><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
+        case 1: gradient_vec_kernel<T, 1><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+        case 2: gradient_vec_kernel<T, 2><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+        case 4: gradient_vec_kernel<T, 4><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+        case 8: gradient_vec_kernel<T, 8><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+        default: gradient_vec_kernel<T, 0><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
         }
         BFB_CUDA(cudaGetLastError());
         return BFB_OK;
     }
     const int threads = L >= 256 ? 256 : ((L + 31) / 32) * 32;
     switch (S) {
-    case 1: gradient_kernel<T, 1><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-    case 2: gradient_kernel<T, 2><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-    case 4: gradient_kernel<T, 4><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-    case 8: gradient_kernel<T, 8><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
-    default: gradient_kernel<T, 0><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, h1, r1, h2, r2); break;
+    case 1: gradient_kernel<T, 1><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+    case 2: gradient_kernel<T, 2><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+    case 4: gradient_kernel<T, 4><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+    case 8: gradient_kernel<T, 8><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
+    default: gradient_kernel<T, 0><<<rows, threads, 0, s>>>(f, o, nx, ny, nz, S, Lp, h1, r1, h2, r2); break;
     }
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;

@@ -51,6 +51,13 @@ int env_check_device_error(::bfb_env_s *env);
 // A voxel on several faces (edges, corners) has the same value in every face
 // array, because all are cut from one per-voxel array.
 // ---------------------------------------------------------------------------
+// The field element of voxel v = (i*ny + j)*nz + k, substrate d, with the
+// (i, j) rows Lp elements apart.
+__device__ __forceinline__ size_t voxel_elem(int v, int d, int nz, int S, int Lp) {
+    const int row = v / nz;
+    return (size_t)row * Lp + (size_t)(v - row * nz) * S + d;
+}
+
 template <typename T>
 struct DirFaces {
     const T *face[6];
@@ -92,7 +99,14 @@ struct bfb_env_s {
     cudaStream_t own_stream = nullptr;   // created by bfb_create, used unless bfb_set_stream overrides
     size_t elem = 8;                     // bytes per field element
     int64_t V = 0;                       // voxels
-    int64_t N = 0;                       // V * S
+    int64_t N = 0;                       // V * S (the packed, reference layout)
+    // Row pitch of the device field: the nz*S values of an (i, j) row are
+    // followed by padding up to a whole number of 16-byte vectors when nz*S*elem
+    // is not one (so that every sweep can use the TMA tiles); Lp = nz*S
+    // otherwise. rho(i,j,k,d) lives at (i*ny + j)*Lp + k*S + d, and the field
+    // holds Np = nx*ny*Lp elements.
+    int Lp = 0;
+    int64_t Np = 0;
 
     void *field = nullptr;               // device, N elements
     void *staging = nullptr;             // device, N doubles (host double <-> env precision)

@@ -20,7 +20,7 @@ namespace bfb {
 
 template <typename T>
 __global__ void matlab_pack_kernel(const T *__restrict__ f, double *__restrict__ out, int nx, int ny, int nz, int S,
-                                   double x0, double y0, double z0, double dx, double vol) {
+                                   int Lp, double x0, double y0, double z0, double dx, double vol) {
     const int rows = 4 + S;
     const long long V = (long long)nx * ny * nz;
     const long long total = V * rows;
@@ -30,7 +30,8 @@ __global__ void matlab_pack_kernel(const T *__restrict__ f, double *__restrict__
         const int r = (int)(e - n * rows);
         double v;
         if (r >= 4) {
-            v = (double)f[n * S + (r - 4)];
+            const long long row = n / nz;  // field rows (i, j) are Lp elements apart
+            v = (double)f[row * Lp + (n - row * nz) * S + (r - 4)];
         } else if (r == 3) {
             v = vol;
         } else {
@@ -67,10 +68,10 @@ extern "C" BFB_API int bfb_write_matlab(bfb_env env, const char *filename) {
     const int blocks = 148 * 8;
     if (env->precision == BFB_FP64)
         matlab_pack_kernel<double><<<blocks, 256, 0, env->stream>>>(static_cast<const double *>(env->field), dbuf,
-                                                                    env->nx, env->ny, env->nz, S, x0, y0, z0, dx, vol);
+                                                                    env->nx, env->ny, env->nz, S, env->Lp, x0, y0, z0, dx, vol);
     else
         matlab_pack_kernel<float><<<blocks, 256, 0, env->stream>>>(static_cast<const float *>(env->field), dbuf,
-                                                                   env->nx, env->ny, env->nz, S, x0, y0, z0, dx, vol);
+                                                                   env->nx, env->ny, env->nz, S, env->Lp, x0, y0, z0, dx, vol);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(hbuf, dbuf, count * sizeof(double), cudaMemcpyDeviceToHost, env->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(env->stream);

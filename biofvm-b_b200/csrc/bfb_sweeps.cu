@@ -195,19 +195,10 @@ __global__ void sweep_strided_global_kernel(SweepArgs<T> a, StridedGeom g) {
     if (t >= (long long)g.n_slabs * g.P) return;
     const int slab = (int)(t / g.P);
     const long long col = t % g.P;
-    const int S = a.S, n = g.n;
-    const int d = (int)(col % S);
-    int ci, cj, ck;
-    if (g.axis == 0) {
-        const long long q = col / S;
-        ck = (int)(q % a.nz);
-        cj = (int)(q / a.nz);
-        ci = 0;
-    } else {
-        ck = (int)(col / S);
-        ci = slab;
-        cj = 0;
-    }
+    const int n = g.n;
+    const StridedColumn col_at = strided_column(a, g, slab, col);
+    if (!col_at.real) return;  // padding of a padded row: no line
+    const int d = col_at.d, ci = col_at.ci, cj = col_at.cj, ck = col_at.ck;
     const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
     bool col_dir, lo_dir, hi_dir;
     if (g.axis == 0) {
@@ -260,9 +251,9 @@ __global__ void sweep_contig_global_kernel(SweepArgs<T> a, long long nrows) {
     const bool line_dir = ((m & 1u) && i == 0) || ((m & 2u) && i == a.nx - 1) || ((m & 4u) && j == 0) ||
                           ((m & 8u) && j == a.ny - 1);
     const bool lo_dir = m & 16u, hi_dir = m & 32u;
-    T *line = a.fo + (size_t)row * nz * S + d;  // solved in place in the output
+    T *line = a.fo + (size_t)row * a.Lp + d;  // solved in place in the output
     if (a.fo != a.f) {
-        const T *src = a.f + (size_t)row * nz * S + d;
+        const T *src = a.f + (size_t)row * a.Lp + d;
         for (int k = 0; k < nz; ++k) line[(size_t)k * S] = src[(size_t)k * S];
     }
     auto pre = [](int, T x) -> T { return x; };
@@ -306,7 +297,7 @@ __global__ void dirichlet_kernel(SweepArgs<T> a) {
         i = (int)(q / a.ny);
         j = (int)(q % a.ny);
     }
-    const size_t vb = (((size_t)i * a.ny + j) * a.nz + k) * a.S;
+    const size_t vb = ((size_t)i * a.ny + j) * a.Lp + (size_t)k * a.S;
     for (int d = 0; d < a.S; ++d) {
         if (on_active_face(a.dir.mask[d], i, j, k, a.nx, a.ny, a.nz)) a.f[vb + d] = dir_value(a.dir, i, j, k, d);
     }
@@ -326,8 +317,9 @@ size_t strided_smem(int n, int elem, int warps) {
     return b <= (size_t)kMaxSmem ? b : 0;
 }
 
-size_t contig_smem(int nz, int S, int elem, int warps, int *R, int *RS) {
-    const int L = nz * S;
+size_t contig_smem(int nz, int S, int Lp, int elem, int warps, int *R, int *RS) {
+    (void)nz;
+    const int L = Lp;  // a shared row holds a whole (padded) row
     int r = S <= 32 ? 32 / S : 1;
     int rs = L;
     if (r > 1) {
@@ -358,13 +350,13 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, co
     g.axis = axis;
     if (axis == 0) {
         g.n = a.nx;
-        g.P = (long long)a.ny * a.nz * a.S;
+        g.P = (long long)a.ny * a.Lp;
         g.slab_stride = 0;
         g.n_slabs = 1;
     } else {
         g.n = a.ny;
-        g.P = (long long)a.nz * a.S;
-        g.slab_stride = (long long)a.ny * a.nz * a.S;
+        g.P = a.Lp;
+        g.slab_stride = (long long)a.ny * a.Lp;
         g.n_slabs = a.nx;
     }
     g.ncb = (int)((g.P + 31) / 32);
@@ -398,10 +390,10 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, co
                     : go_strided<T, (int)sizeof(T), false>(a, g, warps, smem, s);
 }
 
-bool contig_aligned_geom(int nz, int S, int elem, int *R, int *RS) {
+bool contig_aligned_geom(int nz, int S, int Lp, int elem, int *R, int *RS) {
     if (elem != 4 || S > 32) return false;
-    const int L = nz * S;
-    const int base = (L + 3) / 4 * 4;
+    (void)nz;
+    const int base = (Lp + 3) / 4 * 4;  // a shared row holds a whole (padded) row
     int best_r = 0, best_rs = 0;
     for (int t = 0; t < 8; ++t) {  // base + 4t: every multiple of 4 (mod 32) once
         const int rs = base + 4 * t;
@@ -451,23 +443,24 @@ int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s
     ContigGeom g;
     g.nz = a.nz;
     g.nrows = (long long)a.nx * a.ny;
+    g.Lp = a.Lp;
     warps = std::max(1, std::min(warps, 4));
-    size_t smem = contig_smem(a.nz, a.S, sizeof(T), warps, &g.R, &g.RS);
-    while (smem == 0 && warps > 1) smem = contig_smem(a.nz, a.S, sizeof(T), --warps, &g.R, &g.RS);
+    size_t smem = contig_smem(a.nz, a.S, a.Lp, sizeof(T), warps, &g.R, &g.RS);
+    while (smem == 0 && warps > 1) smem = contig_smem(a.nz, a.S, a.Lp, sizeof(T), --warps, &g.R, &g.RS);
     if (smem == 0) {
         const long long threads = g.nrows * a.S;
         sweep_contig_global_kernel<T><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, g.nrows);
         BFB_CUDA(cudaGetLastError());
         return BFB_OK;
     }
-    const long long L = (long long)a.nz * a.S;
+    const long long L = a.Lp;  // row pitch: copies cover whole (padded) rows
     const bool base16 = (reinterpret_cast<uintptr_t>(a.f) & 15) == 0;
     const int eb = (int)sizeof(T);
     if (use_tma && base16 && (L * eb) % 16 == 0) {
         // the bulk-copy tile needs 16-byte shared rows: contig_smem's
         // conflict-free stride where it is one, else contig_aligned_geom's
         ContigGeom gt = g;
-        const bool ok = ((long long)g.RS * eb) % 16 == 0 || contig_aligned_geom(a.nz, a.S, eb, &gt.R, &gt.RS);
+        const bool ok = ((long long)g.RS * eb) % 16 == 0 || contig_aligned_geom(a.nz, a.S, a.Lp, eb, &gt.R, &gt.RS);
         if (ok && (L * eb) * gt.R < (1 << 20)) {
             const int st = launch_contig_tma<T>(a, gt, warps, s, chunks);
             if (st != kNotApplicable) return st;

@@ -73,6 +73,9 @@ struct SweepArgs {
     T *f;          // input field
     T *fo;         // output field (== f for the in-place sweeps of a step)
     int nx, ny, nz, S;
+    int Lp;        // elements between consecutive (i, j) rows: nz*S, or nz*S rounded up to whole
+                   // 16-byte vectors when the field is padded (bfb_env_s::Lp); rho(i,j,k,d) is at
+                   // (i*ny + j)*Lp + k*S + d
     Factors<T> fac;
     const T *c1;   // FP64: [S] c1 = dt*D/dx^2
     const T *g;    // FP32: [2*S] g = 1/(1 + c2) as hi, lo
@@ -83,7 +86,8 @@ struct SweepArgs {
 
 struct StridedGeom {
     int n;                 // line length
-    long long P;           // lines per slab == element stride between line elements
+    long long P;           // lines per slab == element stride between line elements (x: ny*Lp,
+                           // y: Lp; the columns q >= nz*S of a padded row are padding, not lines)
     long long slab_stride; // elements between slabs
     int n_slabs;
     int ncb;               // 32-column blocks per slab
@@ -93,9 +97,38 @@ struct StridedGeom {
 struct ContigGeom {
     int nz;
     long long nrows;       // nx * ny rows of nz*S elements
+    int Lp;                // elements between consecutive rows (SweepArgs::Lp)
     int R;                 // rows per warp tile
     int RS;                // shared-memory row stride (elements), RS = S (mod 32)
 };
+
+// The voxel and substrate of strided column `cl` of slab `slab` (x: cl =
+// j*Lp + q, y: cl = q, with q = k*S + d); `real` is false for columns past P
+// and for the padding of a padded row (q >= nz*S), whose lanes run along but
+// read no Dirichlet value or bulk term.
+struct StridedColumn {
+    int d, ci, cj, ck;
+    bool real;
+};
+template <typename T>
+__device__ __forceinline__ StridedColumn strided_column(const SweepArgs<T> &a, const StridedGeom &g, int slab,
+                                                        long long cl) {
+    StridedColumn c;
+    long long q;
+    if (g.axis == 0) {
+        c.cj = (int)(cl / a.Lp);
+        q = cl - (long long)c.cj * a.Lp;
+        c.ci = 0;
+    } else {
+        q = cl;
+        c.ci = slab;
+        c.cj = 0;
+    }
+    c.real = cl < g.P && q < (long long)a.nz * a.S;
+    c.ck = (int)(q / a.S);
+    c.d = (int)(q - (long long)c.ck * a.S);
+    return c;
+}
 
 // launchers (bfb_sweeps.cu). `map` (may be NULL) is the field's tensor map
 // for this axis; with it the TMA kernels run, otherwise cp.async ones.
@@ -113,9 +146,10 @@ int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtens
                        const CUtensorMap *map_out, int crow, bool fuse_pre, int warps, cudaStream_t s);
 template <typename T>
 int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s, int chunks);
-// `chunks` row groups per tile: box rows = ceil(n / chunks) (<= 256).
+// `chunks` row groups per tile: box rows = ceil(n / chunks) (<= 256); Lp the
+// (i, j) rows' pitch in elements.
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
-                           int S, int chunks = kChunks);
+                           int S, int chunks, int Lp);
 void tma_prepare_device();
 // One bounded mbarrier wait that nothing completes, `polls` polls long; sets
 // *err like a stalled copy would (bfb_watchdog_selftest).
@@ -125,16 +159,17 @@ int launch_dirichlet(const SweepArgs<T> &a, cudaStream_t s);
 template <typename T>
 int launch_bulk(const SweepArgs<T> &a, long long N, cudaStream_t s);
 
-// shared-memory bytes a strided / contiguous CTA needs (0 if it does not fit)
+// shared-memory bytes a strided / contiguous CTA needs (0 if it does not fit);
+// Lp is the z rows' pitch in elements (a shared row holds a whole padded row)
 size_t strided_smem(int n, int elem, int warps);
-size_t contig_smem(int nz, int S, int elem, int warps, int *R, int *RS);
+size_t contig_smem(int nz, int S, int Lp, int elem, int warps, int *R, int *RS);
 // Rows per warp tile R and shared row stride RS for the bulk-copy z tile where
 // contig_smem's conflict-free stride (RS = S mod 32) is not a multiple of 16
 // bytes (S not a multiple of 4 in FP32): RS >= nz*S a multiple of 16 bytes,
 // chosen among the eight residues mod 32 so that the most rows keep lane
 // (r, d)'s words r*RS + d apart mod 32 (no bank conflicts). FP32 only (FP64
 // words pair banks); false when fewer than 16 lanes would be busy (S = 1).
-bool contig_aligned_geom(int nz, int S, int elem, int *R, int *RS);
+bool contig_aligned_geom(int nz, int S, int Lp, int elem, int *R, int *RS);
 
 // Opt the shared-memory kernels into 227 KB, once per device.
 void sweeps_prepare_device();

@@ -57,22 +57,12 @@ __device__ __forceinline__ void strided_tile(const SweepArgs<T> &a, const Stride
         return;
     }
 
-    // ---- line coordinates of this lane
+    // ---- line coordinates of this lane (padding columns of a padded row run
+    // along with no Dirichlet value and no bulk term)
     const long long col = col0 + lane;
-    const int S = a.S;
-    const int d = (int)(col % S);
-    int ci, cj, ck;  // voxel coordinates with the line coordinate left at 0
-    if (g.axis == 0) {
-        const long long t = col / S;
-        ck = (int)(t % a.nz);
-        cj = (int)(t / a.nz);
-        ci = 0;
-    } else {
-        ck = (int)(col / S);
-        ci = slab;
-        cj = 0;
-    }
-    const unsigned m = a.dir.any ? a.dir.mask[d] : 0u;
+    const StridedColumn col_at = strided_column(a, g, slab, col);
+    const int d = col_at.d, ci = col_at.ci, cj = col_at.cj, ck = col_at.ck;
+    const unsigned m = (a.dir.any && col_at.real) ? a.dir.mask[d] : 0u;
     bool col_dir, lo_dir, hi_dir;
     if (g.axis == 0) {
         col_dir = ((m & 4u) && cj == 0) || ((m & 8u) && cj == a.ny - 1) || ((m & 16u) && ck == 0) ||
@@ -95,7 +85,9 @@ __device__ __forceinline__ void strided_tile(const SweepArgs<T> &a, const Stride
     }
     auto load = [&](int r) -> T {
         T x = sm[r * 32 + lane];
-        if constexpr (BULK) x = bulk_update(x, bA[(size_t)r * P], bB[(size_t)r * P], a.bulk.dt);
+        if constexpr (BULK) {
+            if (col_at.real) x = bulk_update(x, bA[(size_t)r * P], bB[(size_t)r * P], a.bulk.dt);
+        }
         return x;
     };
 
@@ -167,7 +159,7 @@ __device__ __forceinline__ void contig_tile_wide(const SweepArgs<T> &a, const Co
     const long long row0 = tile * g.R;
     const int nr = (int)min((long long)g.R, g.nrows - row0);
     const int S = a.S, nz = g.nz;
-    const int L = nz * S;
+    const int L = g.Lp;  // row pitch: a padded row's padding is copied along
     T *__restrict__ base = a.f + (size_t)row0 * L;
     T *__restrict__ obase = a.fo + (size_t)row0 * L;
     constexpr int EPV = VB / (int)sizeof(T);
@@ -256,7 +248,7 @@ __device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigG
     const long long row0 = tile * g.R;
     const int nr = (int)min((long long)g.R, g.nrows - row0);
     const int nz = g.nz;
-    const int L = nz * S;
+    const int L = g.Lp;  // row pitch: the last row group copies a padded row's padding along
     const int RS = g.RS;
     T *__restrict__ base = a.f + (size_t)row0 * L;
     T *__restrict__ obase = a.fo + (size_t)row0 * L;
@@ -267,9 +259,10 @@ __device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigG
     int kc = (nz + 1) / 2;
     kc = (kc + qa - 1) / qa * qa;
     const int nch = (nz + kc - 1) / kc;  // 1 or 2
+    auto span_of = [&](int c) { return (c == nch - 1 ? L : (c + 1) * kc * S) - c * kc * S; };
 
     for (int c = 0; c < nch; ++c) {
-        const int k0 = c * kc, span = (min(nz, k0 + kc) - k0) * S, vspan = span / EPV;
+        const int k0 = c * kc, span = span_of(c), vspan = span / EPV;
         for (int r = 0; r < nr; ++r) {
             const T *src = base + (size_t)r * L + (size_t)k0 * S + lane * EPV;
             unsigned dst = (unsigned)__cvta_generic_to_shared(sm + (size_t)r * RS + (size_t)k0 * S + lane * EPV);
@@ -283,7 +276,7 @@ __device__ __forceinline__ void contig_tile(const SweepArgs<T> &a, const ContigG
         __syncwarp();
     };
     auto store_c = [&](int c) {  // row group c of every row, shared -> global
-        const int k0 = c * kc, span = (min(nz, k0 + kc) - k0) * S, vspan = span / EPV;
+        const int k0 = c * kc, span = span_of(c), vspan = span / EPV;
         for (int r = 0; r < nr; ++r) {
             const T *src = sm + (size_t)r * RS + (size_t)k0 * S;
             T *dst = obase + (size_t)r * L + (size_t)k0 * S;

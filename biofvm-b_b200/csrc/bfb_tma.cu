@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(128, 1) sweep_contig_tma_kernel(SweepArgs<T> a
     if (row0 >= g.nrows) return;
     const int nr = (int)min((long long)g.R, g.nrows - row0);
     const int S = a.S, nz = g.nz;
-    const int L = nz * S;
+    const int L = g.Lp;  // row pitch: whole padded rows are copied
     const size_t wbytes = 128 + (size_t)g.R * g.RS * sizeof(T);
     unsigned char *wbase = smem_raw + (size_t)warp * ((wbytes + 127) / 128 * 128);
     const unsigned bar = smem_u32(wbase);
@@ -280,17 +280,20 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// Tensor map of the field for the x (axis 0) or y (axis 1) sweep:
-//   x: 2-D {P = ny*nz*S, nx},      box {32, crow}
-//   y: 3-D {P = nz*S, ny, nx},     box {32, crow, 1}
+// Tensor map of the field for the x (axis 0) or y (axis 1) sweep, with Lp the
+// (i, j) rows' pitch in elements (nz*S, or more for a padded field):
+//   x: 2-D {P = ny*Lp, nx},        box {32, crow}
+//   y: 3-D {P = Lp, ny, nx},       box {32, crow, 1}
 // Returns false when the grid does not meet TMA's rules (row pitch a multiple
 // of 16 bytes, box rows <= 256); the cp.async kernels handle those grids.
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
-                           int S, int chunks) {
+                           int S, int chunks, int Lp) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
+    (void)nz;
+    (void)S;
     const int n = axis == 0 ? nx : ny;
-    const long long P = axis == 0 ? (long long)ny * nz * S : (long long)nz * S;
+    const long long P = axis == 0 ? (long long)ny * Lp : (long long)Lp;
     if (chunks < 1 || chunks > 16) return false;  // one mbarrier per row group in a 128-byte header
     const int crow = (n + chunks - 1) / chunks;
     if (crow > 256 || (P * elem) % 16 != 0 || (reinterpret_cast<uintptr_t>(field) & 15)) return false;

@@ -23,22 +23,12 @@ __device__ __forceinline__ bool strided_solve(const SweepArgs<T> &a, const Strid
     const long long P = g.P;
     const int nch = (n + crow - 1) / crow;
 
-    // ---- line coordinates of this lane (lanes past P run along, unstored)
+    // ---- line coordinates of this lane (lanes past P and padding columns
+    // run along; past P nothing is stored, padding holds no field value)
     const long long cl = col0 + lane;
-    const bool valid = cl < P;
-    const int S = a.S;
-    const int d = (int)(cl % S);
-    int ci, cj, ck;
-    if (g.axis == 0) {
-        const long long t = cl / S;
-        ck = (int)(t % a.nz);
-        cj = (int)(t / a.nz);
-        ci = 0;
-    } else {
-        ck = (int)(cl / S);
-        ci = slab;
-        cj = 0;
-    }
+    const StridedColumn col_at = strided_column(a, g, slab, cl);
+    const bool valid = col_at.real;
+    const int d = col_at.d, ci = col_at.ci, cj = col_at.cj, ck = col_at.ck;
     const unsigned m = (a.dir.any && valid) ? a.dir.mask[d] : 0u;
     bool col_dir, lo_dir, hi_dir;
     if (g.axis == 0) {
@@ -181,13 +171,16 @@ __device__ __forceinline__ bool contig_pipe_tile(const SweepArgs<T> &a, const Co
     const int nr = (int)min((long long)g.R, g.nrows - row0);
     const int S = SC > 0 ? SC : a.S;
     const int nz = g.nz;
-    const int L = nz * S;
+    const int L = g.Lp;  // row pitch; the last row group copies a padded row's padding along
     const int nch = (nz + kc - 1) / kc;
     const unsigned bar0 = smem_u32(wbase);
     T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
     T *__restrict__ base = a.f + (size_t)row0 * L;
     T *__restrict__ obase = a.fo + (size_t)row0 * L;
-    auto seg_bytes = [&](int c) -> unsigned { return (unsigned)((min(nz, (c + 1) * kc) - c * kc) * S * (int)sizeof(T)); };
+    auto seg_bytes = [&](int c) -> unsigned {
+        const int end = c == nch - 1 ? L : (c + 1) * kc * S;
+        return (unsigned)((end - c * kc * S) * (int)sizeof(T));
+    };
 
     if (lane == 0) {
         for (int c = 0; c < nch; ++c) {

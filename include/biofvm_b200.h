@@ -130,8 +130,15 @@ BFB_API int bfb_get_field_device(bfb_env env, void *dst, int dst_precision);
  * in FP64 on the device. Relative L-inf = out4[0]/out4[1], relative
  * L2 = sqrt(out4[2]/out4[3]). */
 BFB_API int bfb_compare_fields(bfb_env test, bfb_env ref, double *out4);
-/* Device pointer of the field (env precision); valid until bfb_destroy. */
+/* Device pointer of the field (env precision); valid until bfb_destroy.
+ * Voxel (i, j, k), substrate d is element (i*ny + j)*Lp + k*S + d, Lp from
+ * bfb_field_pitch: nz*S (the packed reference layout) unless nz*S elements
+ * are not a whole number of 16-byte vectors, when each (i, j) row is padded
+ * to the next 16 bytes (the tensor-tile copies need 16-byte row pitches).
+ * Padding entries are not part of the field; the transfer calls above take
+ * and return the packed layout. */
 BFB_API int bfb_field_device_ptr(bfb_env env, void **dptr);
+BFB_API int bfb_field_pitch(bfb_env env, int *row_elems);
 
 /* Dirichlet conditions on the outer faces.
  *   values     V*S per-voxel values like the reference's dirichlet_value_vectors

@@ -42,6 +42,7 @@ def test_null_handle_is_rejected_without_gpu(bfb):
     assert L.bfb_watchdog_selftest(None, 8) == -1
     assert L.bfb_host_register(None, 8) == -1
     assert L.bfb_host_unregister(None) == -1
+    assert L.bfb_field_pitch(None, None) == -1
 
 
 def test_create_validates_arguments_before_touching_a_device(bfb):

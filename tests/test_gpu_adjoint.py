@@ -93,6 +93,7 @@ def _rel(a, b):
     (5, 2, (10, 12, 11), 2, 120),
     (4, 4, (33, 9, 40), 1, 60),
     (3, 2, (24, 20, 32), 8, 150),
+    (4, 3, (9, 11, 13), 3, 80),  # rows of 39 doubles: the device field's rows are padded
 ])
 def test_adjoint_fp64_matches_oracle(bfb, oracle, n_steps, K, shape, S, agents):
     rng = np.random.default_rng(500 + n_steps * 7 + S)

@@ -41,9 +41,12 @@ def test_matlab_fp64_byte_identical_to_reference(bfb, tmp_path, box, S):
     env.close()
 
 
-def test_matlab_fp32_layout(bfb, tmp_path):
+# (12, 10, 9) x 4: rows of 36 floats (packed); (7, 5, 3) x 3: rows of 9 floats,
+# padded on the device to 12
+@pytest.mark.parametrize("shape,S", [((12, 10, 9), 4), ((7, 5, 3), 3)])
+def test_matlab_fp32_layout(bfb, tmp_path, shape, S):
     rng = np.random.default_rng(7)
-    shape, S, dx = (12, 10, 9), 4, 20.0
+    dx = 20.0
     env = bfb.Env(shape, S, dx=dx, precision=bfb.FP32)
     env.set_field(rng.random((*shape, S)))
     env.write_matlab(tmp_path / "f.mat")

@@ -240,6 +240,22 @@ def test_checksum_matches_oracle(bfb, oracle, rng, shape, S):
         env.close()
 
 
+@pytest.mark.parametrize("shape,S", [((6, 5, 7), 3), ((4, 3, 9), 1), ((5, 4, 8), 2), ((3, 3, 5), 5)])
+def test_field_rows_padded_to_16_bytes(bfb, rng, shape, S):
+    """The device field's (i, j) rows are nz*S elements apart when that is a
+    whole number of 16-byte vectors, else padded to the next one; the
+    transfer calls still take and return the packed layout, bit for bit."""
+    rho = rng.random((*shape, S))
+    L = shape[2] * S
+    for prec, eb in ((bfb.FP64, 8), (bfb.FP32, 4)):
+        env = make_env(bfb, rho, [1e3] * S, [0.1] * S, prec)
+        epv = 16 // eb
+        assert env.field_pitch() == (L + epv - 1) // epv * epv
+        want = rho if prec == bfb.FP64 else rho.astype(np.float32)
+        assert np.array_equal(env.get_field_raw(), want)
+        env.close()
+
+
 def test_checksum_256cube_bandwidth(bfb):
     """The per-substrate mass checksum at the bench size reads the field once;
     timed with CUDA events on one stream (through the allocation-free entry
