@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(128, 1)
     const long long P = g.P;
     const int nch = (n + crow - 1) / crow;
     const int rank = g.axis == 0 ? 2 : 3;
-    unsigned char *wbase = smem_raw + (size_t)warp * strided_tma_warp_bytes(n, crow, sizeof(T));
+    unsigned char *wbase = smem_raw + (size_t)warp * strided_tma_warp_bytes(n, crow, sizeof(T), 32);
     const unsigned bar0 = smem_u32(wbase);
     T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
     const unsigned sm_u32 = smem_u32(sm);
@@ -904,11 +904,13 @@ struct Adjoint {
     long long tiles_z = 0;
 
     // tensor maps with the env's row-group counts (so the recompute runs the
-    // env's tuned launch shape); workspace buffers are packed (rows nz*S apart)
+    // env's tuned launch shape) and warp tiles of 32 lines (the adjoint
+    // kernels' tiles); workspace buffers are packed (rows nz*S apart)
     void map(Buf &b) {
         for (int a = 0; a < 2; ++a)
             b.ok[a] = env->use_tma && make_sweep_tensor_map(&b.map[a], &b.crow[a], b.p, sizeof(T), a, env->nx,
-                                                            env->ny, env->nz, S, env->tuning.chunks[a], env->nz * S);
+                                                            env->ny, env->nz, S, env->tuning.chunks[a], env->nz * S,
+                                                            32);
     }
     // the env's sweep arguments over packed workspace buffers
     SweepArgs<T> args(int axis) const {
@@ -926,7 +928,7 @@ struct Adjoint {
         if (axis < 2) {
             const bool tma = env->tuning.tma[axis] && in.ok[axis] && out.ok[axis];
             return launch_strided<T>(a, axis, axis == 0, warps, tma ? &in.map[axis] : nullptr,
-                                     tma ? &out.map[axis] : nullptr, in.crow[axis], st);
+                                     tma ? &out.map[axis] : nullptr, in.crow[axis], 32, st);
         }
         return launch_contig<T>(a, warps, env->use_tma && env->tuning.tma[2], st, env->tuning.chunks[2]);
     }
@@ -979,7 +981,7 @@ struct Adjoint {
             const unsigned tiles = (unsigned)((long long)g.n_slabs * g.ncb);
             if (lam.ok[axis] && mu.ok[axis]) {
                 const int crow = lam.crow[axis];
-                const size_t wb = strided_tma_warp_bytes(g.n, crow, sizeof(T));
+                const size_t wb = strided_tma_warp_bytes(g.n, crow, sizeof(T), 32);
                 if (wb <= (size_t)kMaxSmem) {
                     adjoint_solve_strided_tma_kernel<T><<<tiles, 32, wb, st>>>(lam.map[axis], mu.map[axis], a, g, crow);
                     BFB_CUDA(cudaGetLastError());
@@ -1163,19 +1165,10 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
     }
     const int last_len = n_steps - (nseg - 1) * K;
     {
-        Buf f;
-        if (padded) {
-            BFB_CUDA(from_field(head));
-            f.p = head;
-            A.map(f);
-        } else {  // the field itself, with its own tensor maps
-            f.p = env->field;
-            for (int a = 0; a < 2; ++a) {
-                f.ok[a] = env->use_tma && env->tma_ok[a];
-                f.map[a] = env->tmap[a];
-                f.crow[a] = env->tma_crow[a];
-            }
-        }
+        Buf f;  // the field itself where its rows are packed, else a packed copy
+        if (padded) BFB_CUDA(from_field(head));
+        f.p = padded ? static_cast<void *>(head) : env->field;
+        A.map(f);
         if ((rc = segment(f, last_len))) return rc;
     }
     if (padded)

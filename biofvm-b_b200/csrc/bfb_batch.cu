@@ -392,15 +392,23 @@ static int batch_upload(bfb_batch_s *b, double dt) {
         I.tiles[2] = (int)((I.gz.nrows + I.gz.R - 1) / I.gz.R);
         for (int a = 0; a < 3; ++a) I.items[a] = (I.tiles[a] + b->tiles_per_item - 1) / b->tiles_per_item;
         I.items[3] = (int)(((long long)e->n_occ * e->S + kCellChunk - 1) / kCellChunk);
-        // TMA tiles where the env's own launch shape would use them
+        // TMA tiles where the env's own launch shape would use them, as wide
+        // as the env's maps' boxes
         for (int a = 0; a < 2; ++a) {
-            const StridedGeom &g = a == 0 ? I.gx : I.gy;
+            StridedGeom &g = a == 0 ? I.gx : I.gy;
+            const int lines = e->tma_lines[a];
             I.tma[a] = e->use_tma && e->tuning.tma[a] && e->tma_ok[a] &&
-                       strided_tma_warp_bytes(g.n, e->tma_crow[a], eb) <= (size_t)kMaxSmem;
+                       strided_tma_warp_bytes(g.n, e->tma_crow[a], eb, lines) <= (size_t)kMaxSmem;
+            if (I.tma[a]) {
+                g.tw = lines;
+                g.ncb = (int)((g.P + lines - 1) / lines);
+                I.tiles[a] = g.n_slabs * g.ncb;
+                I.items[a] = (I.tiles[a] + b->tiles_per_item - 1) / b->tiles_per_item;
+            }
             I.crow[a] = e->tma_crow[a];
             maps[2 * (size_t)k + a] = e->tmap[a];
             I.map[a] = dmaps + 2 * (size_t)k + a;
-            const size_t tb = I.tma[a] ? strided_tma_warp_bytes(g.n, I.crow[a], eb) - 128 : (size_t)g.n * 32 * eb;
+            const size_t tb = I.tma[a] ? strided_tma_warp_bytes(g.n, I.crow[a], eb, lines) - 128 : (size_t)g.n * 32 * eb;
             tile_bytes = std::max(tile_bytes, tb);
             ebytes[(size_t)a * b->n + k] = tb;
         }

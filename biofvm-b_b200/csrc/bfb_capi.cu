@@ -238,9 +238,13 @@ static const CUtensorMap *tma_map(bfb_env_s *env, int axis) {
 
 // the field's x / y tensor maps for the current row-group counts
 static void encode_field_maps(bfb_env_s *env) {
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 2; ++a) {
+        const int chunks = env->tuning.chunks[a];
+        env->tma_lines[a] = strided_tile_lines(a == 0 ? env->nx : env->ny, (int)env->elem, chunks);
         env->tma_ok[a] = make_sweep_tensor_map(&env->tmap[a], &env->tma_crow[a], env->field, (int)env->elem, a,
-                                               env->nx, env->ny, env->nz, env->S, env->tuning.chunks[a], env->Lp);
+                                               env->nx, env->ny, env->nz, env->S, chunks, env->Lp,
+                                               env->tma_lines[a]);
+    }
 }
 
 // One LOD diffusion step; `bulk` fuses a preceding bulk source/sink update
@@ -248,7 +252,7 @@ static void encode_field_maps(bfb_env_s *env) {
 template <typename T>
 static int launch_strided_env(bfb_env_s *env, int axis, bool bulk, double dt, cudaStream_t s) {
     return launch_strided<T>(make_args<T>(env, axis, bulk, dt), axis, axis == 0, env->tuning.warps[axis],
-                             tma_map(env, axis), tma_map(env, axis), env->tma_crow[axis], s);
+                             tma_map(env, axis), tma_map(env, axis), env->tma_crow[axis], env->tma_lines[axis], s);
 }
 
 template <typename T>
@@ -1029,15 +1033,16 @@ static int time_candidates(bfb_env_s *env, double dt, int trials, void *scratch,
                     CUtensorMap mi, mo;
                     int ci = 0, co = 0;
                     bool maps = false;
+                    const int lines = strided_tile_lines(axis == 0 ? env->nx : env->ny, (int)env->elem, chunks);
                     if (axis < 2 && tma && env->use_tma)
                         maps = make_sweep_tensor_map(&mi, &ci, env->field, (int)env->elem, axis, env->nx, env->ny,
-                                                     env->nz, env->S, chunks, env->Lp) &&
+                                                     env->nz, env->S, chunks, env->Lp, lines) &&
                                make_sweep_tensor_map(&mo, &co, scratch, (int)env->elem, axis, env->nx, env->ny,
-                                                     env->nz, env->S, chunks, env->Lp);
+                                                     env->nz, env->S, chunks, env->Lp, lines);
                     auto launch = [&]() -> int {
                         if (axis < 2)
                             return launch_strided<T>(a, axis, axis == 0, warps, maps ? &mi : nullptr,
-                                                     maps ? &mo : nullptr, ci, s);
+                                                     maps ? &mo : nullptr, ci, lines, s);
                         return launch_contig<T>(a, warps, tma && env->use_tma, s, chunks);
                     };
                     if ((st = launch())) break;  // warm

@@ -169,6 +169,7 @@ struct bfb_env_s {
     int use_tma = 1;
     CUtensorMap tmap[2];
     int tma_crow[2] = {0, 0};
+    int tma_lines[2] = {32, 32};  // lines per warp tile of the maps' boxes
     int tma_ok[2] = {0, 0};
 
     // sticky device error flag (a bounded wait in a kernel ran out)

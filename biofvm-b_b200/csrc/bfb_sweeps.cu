@@ -345,7 +345,7 @@ static int go_strided(const SweepArgs<T> &a, const StridedGeom &g, int warps, si
 
 template <typename T>
 int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map,
-                   const CUtensorMap *map_out, int crow, cudaStream_t s) {
+                   const CUtensorMap *map_out, int crow, int lines, cudaStream_t s) {
     StridedGeom g;
     g.axis = axis;
     if (axis == 0) {
@@ -365,7 +365,7 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, co
     // plain kernel computes the same
     fuse_pre = fuse_pre && (a.dir.any || a.bulk.on);
     if (map && map_out) {
-        const int st = launch_strided_tma<T>(a, g, map, map_out, crow, fuse_pre, warps, s);
+        const int st = launch_strided_tma<T>(a, g, map, map_out, crow, lines, fuse_pre, warps, s);
         if (st != kNotApplicable) return st;
     }
     size_t smem = strided_smem(g.n, sizeof(T), warps);
@@ -391,19 +391,29 @@ int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, co
 }
 
 bool contig_aligned_geom(int nz, int S, int Lp, int elem, int *R, int *RS) {
-    if (elem != 4 || S > 32) return false;
+    if ((elem != 4 && elem != 8) || S > 32) return false;
     (void)nz;
-    const int base = (Lp + 3) / 4 * 4;  // a shared row holds a whole (padded) row
+    // A warp's access to element r*rs + k*S + d (lane (r, d)) is conflict-free
+    // when no 4-byte bank holds more words of it than the element has words:
+    // every element index mod `slots` at most `words` times (FP32: 32 slots,
+    // once each; FP64: 16 slots of two banks, twice each -- the two
+    // wavefronts that 256 bytes take anyway).
+    const int epv = 16 / elem, words = elem / 4, slots = 32 / words;
+    const int base = (Lp + epv - 1) / epv * epv;  // a shared row holds a whole (padded) row
     int best_r = 0, best_rs = 0;
-    for (int t = 0; t < 8; ++t) {  // base + 4t: every multiple of 4 (mod 32) once
-        const int rs = base + 4 * t;
-        unsigned used = 0;
+    for (int t = 0; t < slots / epv; ++t) {  // base + epv*t: every multiple of epv (mod slots) once
+        const int rs = base + epv * t;
+        int used[32] = {0};
         int r = 0;
         for (; r < 32 / S; ++r) {
-            unsigned m = 0;
-            for (int d = 0; d < S; ++d) m |= 1u << ((r * rs + d) % 32);
-            if (m & used) break;
-            used |= m;
+            int add[32] = {0};
+            bool ok = true;
+            for (int d = 0; d < S; ++d) {
+                const int q = (int)(((long long)r * rs + d) % slots);
+                ok = ok && used[q] + ++add[q] <= words;
+            }
+            if (!ok) break;
+            for (int q = 0; q < slots; ++q) used[q] += add[q];
         }
         if (r > best_r) {
             best_r = r;
@@ -544,9 +554,9 @@ void sweeps_prepare_device() {
 }
 
 template int launch_strided<double>(const SweepArgs<double> &, int, bool, int, const CUtensorMap *,
-                                    const CUtensorMap *, int, cudaStream_t);
+                                    const CUtensorMap *, int, int, cudaStream_t);
 template int launch_strided<float>(const SweepArgs<float> &, int, bool, int, const CUtensorMap *, const CUtensorMap *,
-                                   int, cudaStream_t);
+                                   int, int, cudaStream_t);
 template int launch_contig<double>(const SweepArgs<double> &, int, bool, cudaStream_t, int);
 template int launch_contig<float>(const SweepArgs<float> &, int, bool, cudaStream_t, int);
 template int launch_dirichlet<double>(const SweepArgs<double> &, cudaStream_t);

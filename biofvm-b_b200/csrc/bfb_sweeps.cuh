@@ -90,8 +90,9 @@ struct StridedGeom {
                            // y: Lp; the columns q >= nz*S of a padded row are padding, not lines)
     long long slab_stride; // elements between slabs
     int n_slabs;
-    int ncb;               // 32-column blocks per slab
+    int ncb;               // column blocks (warp tiles) per slab
     int axis;              // 0 = x, 1 = y
+    int tw = 32;           // lines per warp tile: 32, or fewer for the TMA tiles (strided_tile_lines)
 };
 
 struct ContigGeom {
@@ -134,7 +135,7 @@ __device__ __forceinline__ StridedColumn strided_column(const SweepArgs<T> &a, c
 // for this axis; with it the TMA kernels run, otherwise cp.async ones.
 template <typename T>
 int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map,
-                   const CUtensorMap *map_out, int crow, cudaStream_t s);
+                   const CUtensorMap *map_out, int crow, int lines, cudaStream_t s);
 template <typename T>
 int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s, int chunks = kChunks);
 
@@ -143,13 +144,19 @@ int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s
 constexpr int kNotApplicable = 1;
 template <typename T>
 int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map,
-                       const CUtensorMap *map_out, int crow, bool fuse_pre, int warps, cudaStream_t s);
+                       const CUtensorMap *map_out, int crow, int lines, bool fuse_pre, int warps, cudaStream_t s);
 template <typename T>
 int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cudaStream_t s, int chunks);
 // `chunks` row groups per tile: box rows = ceil(n / chunks) (<= 256); Lp the
-// (i, j) rows' pitch in elements.
+// (i, j) rows' pitch in elements; `lines` the box's columns (the lines of one
+// warp tile, <= 32, a whole number of 16-byte vectors).
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
-                           int S, int chunks, int Lp);
+                           int S, int chunks, int Lp, int lines);
+// Lines per strided TMA warp tile for lines of n rows in `chunks` row groups:
+// the width that keeps the most lines resident per SM (a line's rows all sit
+// in shared memory, so FP64 tiles of 32 long lines leave few warps per SM and
+// a narrower tile fits more of them); 32 on ties.
+int strided_tile_lines(int n, int elem, int chunks);
 void tma_prepare_device();
 // One bounded mbarrier wait that nothing completes, `polls` polls long; sets
 // *err like a stalled copy would (bfb_watchdog_selftest).
@@ -165,10 +172,10 @@ size_t strided_smem(int n, int elem, int warps);
 size_t contig_smem(int nz, int S, int Lp, int elem, int warps, int *R, int *RS);
 // Rows per warp tile R and shared row stride RS for the bulk-copy z tile where
 // contig_smem's conflict-free stride (RS = S mod 32) is not a multiple of 16
-// bytes (S not a multiple of 4 in FP32): RS >= nz*S a multiple of 16 bytes,
-// chosen among the eight residues mod 32 so that the most rows keep lane
-// (r, d)'s words r*RS + d apart mod 32 (no bank conflicts). FP32 only (FP64
-// words pair banks); false when fewer than 16 lanes would be busy (S = 1).
+// bytes (S not a multiple of 4 in FP32, odd S in FP64): RS >= nz*S a multiple
+// of 16 bytes, chosen among its residues so that the most rows keep the warp's
+// accesses free of bank conflicts (lane (r, d) reads element r*RS + k*S + d);
+// false when fewer than 16 lanes would be busy (FP32 S = 1).
 bool contig_aligned_geom(int nz, int S, int Lp, int elem, int *R, int *RS);
 
 // Opt the shared-memory kernels into 227 KB, once per device.

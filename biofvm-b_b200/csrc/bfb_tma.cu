@@ -17,6 +17,8 @@
 // flag and the warp returns.
 #include <cuda.h>
 
+#include <algorithm>
+
 #include "bfb_tma_tiles.cuh"
 
 namespace bfb {
@@ -33,7 +35,7 @@ __global__ void __launch_bounds__(128, 1)
     const int warp = threadIdx.x >> 5;
     const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
     if (tile >= (long long)g.n_slabs * g.ncb) return;
-    unsigned char *wbase = smem_raw + (size_t)warp * strided_tma_warp_bytes(g.n, crow, sizeof(T));
+    unsigned char *wbase = smem_raw + (size_t)warp * strided_tma_warp_bytes(g.n, crow, sizeof(T), g.tw);
     if (lane == 0) {
         const int nch = (g.n + crow - 1) / crow;
         for (int ch = 0; ch < nch; ++ch) mbar_init(smem_u32(wbase) + 8 * ch, 1);
@@ -179,9 +181,12 @@ int launch_watchdog_probe(int polls, int *err, cudaStream_t s) {
 // Host side
 // ---------------------------------------------------------------------------
 template <typename T>
-int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g, const CUtensorMap *map,
-                       const CUtensorMap *map_out, int crow, bool fuse_pre, int warps, cudaStream_t s) {
-    const size_t wb = strided_tma_warp_bytes(g.n, crow, sizeof(T));
+int launch_strided_tma(const SweepArgs<T> &a, const StridedGeom &g_in, const CUtensorMap *map,
+                       const CUtensorMap *map_out, int crow, int lines, bool fuse_pre, int warps, cudaStream_t s) {
+    StridedGeom g = g_in;  // warp tiles of the maps' width
+    g.tw = lines;
+    g.ncb = (int)((g.P + lines - 1) / lines);
+    const size_t wb = strided_tma_warp_bytes(g.n, crow, sizeof(T), lines);
     while (warps > 1 && wb * warps > (size_t)kMaxSmem) --warps;
     if (wb * warps > (size_t)kMaxSmem) return kNotApplicable;  // the caller takes another kernel
     const long long tiles = (long long)g.n_slabs * g.ncb;
@@ -227,9 +232,9 @@ int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cud
 }
 
 template int launch_strided_tma<double>(const SweepArgs<double> &, const StridedGeom &, const CUtensorMap *,
-                                        const CUtensorMap *, int, bool, int, cudaStream_t);
+                                        const CUtensorMap *, int, int, bool, int, cudaStream_t);
 template int launch_strided_tma<float>(const SweepArgs<float> &, const StridedGeom &, const CUtensorMap *,
-                                       const CUtensorMap *, int, bool, int, cudaStream_t);
+                                       const CUtensorMap *, int, int, bool, int, cudaStream_t);
 template int launch_contig_tma<double>(const SweepArgs<double> &, const ContigGeom &, int, cudaStream_t, int);
 template int launch_contig_tma<float>(const SweepArgs<float> &, const ContigGeom &, int, cudaStream_t, int);
 
@@ -282,25 +287,26 @@ static EncodeTiledFn encode_fn() {
 
 // Tensor map of the field for the x (axis 0) or y (axis 1) sweep, with Lp the
 // (i, j) rows' pitch in elements (nz*S, or more for a padded field):
-//   x: 2-D {P = ny*Lp, nx},        box {32, crow}
-//   y: 3-D {P = Lp, ny, nx},       box {32, crow, 1}
+//   x: 2-D {P = ny*Lp, nx},        box {lines, crow}
+//   y: 3-D {P = Lp, ny, nx},       box {lines, crow, 1}
 // Returns false when the grid does not meet TMA's rules (row pitch a multiple
 // of 16 bytes, box rows <= 256); the cp.async kernels handle those grids.
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
-                           int S, int chunks, int Lp) {
+                           int S, int chunks, int Lp, int lines) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
+    if (lines < 1 || lines > 32 || (lines * elem) % 16 != 0) return false;  // tile x offsets stay 16-byte aligned
     (void)nz;
     (void)S;
     const int n = axis == 0 ? nx : ny;
     const long long P = axis == 0 ? (long long)ny * Lp : (long long)Lp;
     if (chunks < 1 || chunks > 16) return false;  // one mbarrier per row group in a 128-byte header
-    const int crow = (n + chunks - 1) / chunks;
+    const int crow = strided_box_rows(n, chunks, lines, elem);
     if (crow > 256 || (P * elem) % 16 != 0 || (reinterpret_cast<uintptr_t>(field) & 15)) return false;
     if (P > 0xffffffffLL) return false;
     cuuint64_t dims[3] = {(cuuint64_t)P, (cuuint64_t)n, (cuuint64_t)nx};
     cuuint64_t strides[2] = {(cuuint64_t)(P * elem), (cuuint64_t)((long long)ny * P * elem)};
-    cuuint32_t box[3] = {32, (cuuint32_t)crow, 1};
+    cuuint32_t box[3] = {(cuuint32_t)lines, (cuuint32_t)crow, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     const cuuint32_t rank = axis == 0 ? 2 : 3;
     const CUresult r = fn(out, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank,
@@ -309,6 +315,40 @@ bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int ele
     if (r != CUDA_SUCCESS) return false;
     *crow_out = crow;
     return true;
+}
+
+// Resident lines per SM as the occupancy calculator gives them for the
+// sweep's kernel at each width (shared memory, its per-CTA reservation,
+// registers and the CTA limit all count). FP64 takes a narrower tile where it
+// keeps at least 1/8 more lines resident than 32 (256^3 x 8: 22 lines, five
+// warps per SM instead of three, x/y sweeps 0.520 -> 0.489 ms); FP32 tiles stay
+// at 32 lines (narrower ones measured 3-10% slower at 128^3 to 256^3).
+int strided_tile_lines(int n, int elem, int chunks) {
+    if (elem != 8) return 32;
+    if (chunks < 1) chunks = 1;
+    const void *kernel = (const void *)sweep_strided_tma_kernel<double, false, false>;
+    auto resident = [&](int w) -> long long {  // lines per SM at width w (0: does not fit)
+        const int crow = strided_box_rows(n, chunks, w, elem);
+        const size_t wb = strided_tma_warp_bytes(n, crow, elem, w);
+        if (crow > 256 || wb > (size_t)kMaxSmem) return 0;
+        int ctas = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kernel, 32, wb) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return 0;
+        }
+        return (long long)ctas * w;
+    };
+    const long long base = resident(32);
+    int best = 32;
+    long long best_resident = base + base / 8;
+    for (int w = 30; w >= 16; w -= 2) {  // FP64: tile x offsets of whole 16-byte vectors
+        const long long r = resident(w);
+        if (r >= best_resident && r > 0) {
+            best_resident = r;
+            best = w;
+        }
+    }
+    return best;
 }
 
 }  // namespace bfb

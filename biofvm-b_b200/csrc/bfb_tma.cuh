@@ -73,12 +73,23 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
+// Rows per TMA box (one row group) of a strided tile of `lines` lines of n
+// rows in `chunks` groups: ceil(n / chunks), rounded up so that every group's
+// shared-memory start (a multiple of crow*lines*elem bytes past the 128-byte
+// aligned tile) is 128-byte aligned, as tensor copies require.
+__host__ __device__ inline int strided_box_rows(int n, int chunks, int lines, int elem) {
+    int m = 128;  // 128 / gcd(128, lines*elem)
+    for (int v = lines * elem; v % 2 == 0 && m > 1; v /= 2) m /= 2;
+    const int crow = (n + chunks - 1) / chunks;
+    return (crow + m - 1) / m * m;
+}
+
 // Bytes of one warp's region in a strided TMA CTA: kChunks mbarriers padded to
-// 128 B, then the tile of nch*crow rows x 32 lines (the last box may reach
-// past row n; TMA zero-fills those rows and the store clips them).
-__host__ __device__ inline size_t strided_tma_warp_bytes(int n, int crow, int elem) {
+// 128 B, then the tile of nch*crow rows x `lines` lines (the last box may
+// reach past row n; TMA zero-fills those rows and the store clips them).
+__host__ __device__ inline size_t strided_tma_warp_bytes(int n, int crow, int elem, int lines) {
     const int nch = (n + crow - 1) / crow;
-    return 128 + (size_t)nch * crow * 32 * elem;
+    return 128 + (size_t)nch * crow * lines * elem;
 }
 
 }  // namespace bfb

@@ -7,9 +7,10 @@
 
 namespace bfb {
 
-// The line solve of one strided warp tile (32 lines of one slab, one lane
-// per line), shared by the TMA tiles of the forward sweeps. Row q of this
-// lane's line is col[q * rs] in shared memory. wait(ch) returns once row
+// The line solve of one strided warp tile (g.tw <= 32 lines of one slab, one
+// lane per line; lanes past g.tw have no line), shared by the TMA tiles of
+// the forward sweeps. Row q of this lane's line is col[q * rs] in shared
+// memory. wait(ch) returns once row
 // group ch (rows [ch*crow, (ch+1)*crow)) has landed, false when its bounded
 // wait ran out; flush(ch) writes row group ch back once its rows are final
 // (the back substitution finishes the groups from the last to the first).
@@ -22,6 +23,12 @@ __device__ __forceinline__ bool strided_solve(const SweepArgs<T> &a, const Strid
     const int n = g.n;
     const long long P = g.P;
     const int nch = (n + crow - 1) / crow;
+    if (lane >= g.tw) {  // no line: follow the row groups' waits and flushes
+        for (int ch = 0; ch < nch; ++ch)
+            if (!wait(ch)) return false;
+        for (int ch = nch - 1; ch >= 0; --ch) flush(ch);
+        return true;
+    }
 
     // ---- line coordinates of this lane (lanes past P and padding columns
     // run along; past P nothing is stored, padding holds no field value)
@@ -116,7 +123,7 @@ __device__ __forceinline__ bool strided_solve(const SweepArgs<T> &a, const Strid
     return true;
 }
 
-// One warp tile of a strided sweep with TMA: 32 lines of `tile`, in the
+// One warp tile of a strided sweep with TMA: g.tw lines of `tile`, in the
 // warp's region `wbase` (128-byte header of row-group mbarriers, then the
 // tile). The mbarriers are initialised by the caller; row group ch waits for
 // parity bit ch of `phase`, and every call completes one phase of each of
@@ -127,13 +134,13 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
                                                  unsigned char *wbase, unsigned phase) {
     const int lane = threadIdx.x & 31;
     const int slab = (int)(tile / g.ncb);
-    const int col0 = (int)((tile % g.ncb) * 32);
+    const int col0 = (int)((tile % g.ncb) * g.tw);
     const int nch = (g.n + crow - 1) / crow;
     const int rank = g.axis == 0 ? 2 : 3;
     const unsigned bar0 = smem_u32(wbase);
     T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
     const unsigned sm_u32 = smem_u32(sm);
-    const unsigned chunk_bytes = (unsigned)crow * 32u * (unsigned)sizeof(T);
+    const unsigned chunk_bytes = (unsigned)crow * (unsigned)g.tw * (unsigned)sizeof(T);
 
     if (lane == 0) {
         for (int ch = 0; ch < nch; ++ch) {
@@ -154,7 +161,7 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
             bulk_commit();
         }
     };
-    if (!strided_solve<T, FUSE_PRE, BULK>(a, g, crow, slab, col0, sm + lane, 32, wait, flush)) return false;
+    if (!strided_solve<T, FUSE_PRE, BULK>(a, g, crow, slab, col0, sm + lane, g.tw, wait, flush)) return false;
     if (lane == 0) bulk_wait_read_all();  // the tile must outlive the stores' reads
     __syncwarp();
     return true;

@@ -135,7 +135,8 @@ def test_cube75_s1_full_size_fp64(bfb, oracle):
 SHAPES = [((1, 1, 1), 1), ((1, 4, 6), 2), ((2, 3, 1), 3), ((3, 2, 2), 1), ((5, 17, 3), 4), ((17, 5, 2), 6),
           ((8, 8, 8), 4), ((8, 8, 8), 8), ((7, 5, 9), 3), ((33, 31, 35), 5), ((64, 2, 3), 2), ((2, 64, 40), 1),
           ((40, 3, 64), 7), ((6, 5, 7), 40), ((3, 9, 4), 33),  # S > 32: lanes solve several z lines each
-          ((100, 6, 8), 3), ((5, 130, 4), 2), ((97, 96, 4), 1)]  # lines of about 100 rows
+          ((100, 6, 8), 3), ((5, 130, 4), 2), ((97, 96, 4), 1),  # lines of about 100 rows
+          ((256, 10, 6), 3), ((6, 256, 10), 2)]  # 256-row lines: FP64 tiles narrower than a warp
 
 
 @pytest.mark.parametrize("tma", [1, 0], ids=["tma", "cpasync"])
