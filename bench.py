@@ -263,15 +263,20 @@ def build_instance(bfb, spec, precision, device):
     return env
 
 
+BATCH_MODE_NAMES = {0: "persistent", 1: "staged", 2: "graph"}
+
+
 def time_ensemble(bfb, envs, K, stream):
-    """Device time per step of the envs stepped together (bfb_batch_simulate)
-    and one by one (bfb_batch_simulate_loop), CUDA events on one stream."""
+    """Device time per step of the envs stepped together (bfb_batch_simulate,
+    in the mode and launch shape bfb_batch_autotune picks, and in each mode
+    at its default shape) and one by one (bfb_batch_simulate_loop), CUDA
+    events on one stream. The autotuner restores every field it advances."""
     import torch
     flags = bfb.STEP_DIFFUSION | bfb.STEP_CELLS
     batch = bfb.Batch(envs)
     batch.set_stream(stream.cuda_stream)
-    out = {}
-    for name, run in (("batch", batch.simulate), ("loop", batch.simulate_loop)):
+
+    def timed(run):
         run(DT, 3, flags)  # warm-up (graph captures)
         stream.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -279,7 +284,16 @@ def time_ensemble(bfb, envs, K, stream):
         run(DT, K, flags)
         e1.record(stream)
         e1.synchronize()
-        out[name] = e0.elapsed_time(e1) / K
+        return e0.elapsed_time(e1) / K
+
+    out = {"modes": {}}
+    for mode in (1, 0, 2):
+        batch.set_mode(mode)
+        out["modes"][BATCH_MODE_NAMES[mode]] = timed(batch.simulate)
+    tuned, _ = batch.autotune(DT, flags, trials=2)
+    out["tuned"] = {"mode": BATCH_MODE_NAMES[batch.mode], "warps_per_cta": tuned[0], "tiles_per_item": tuned[1]}
+    out["batch"] = timed(batch.simulate)
+    out["loop"] = timed(batch.simulate_loop)
     batch.synchronize()
     batch.close()
     return out
@@ -484,6 +498,7 @@ def run_our_arm(args):
                            "substrates, 0-20k agents each, x-face Dirichlet on substrate 0, FP32, diffusion + agents",
                "voxel_substrates": vs, "steps": K_ens,
                "batch_ms_per_step": t["batch"], "loop_ms_per_step": t["loop"],
+               "batch_autotuned": t["tuned"], "mode_ms_per_step": t["modes"],
                "batch_value": vs / (t["batch"] / 1e3), "loop_value": vs / (t["loop"] / 1e3),
                "batch_over_loop_time": t["batch"] / t["loop"],
                "step_roofline_frac": {"batch": step_bytes_ens / (t["batch"] / 1e3) / 1e9 / peak_e,
@@ -589,6 +604,8 @@ def run_ensemble_arm(args):
     stream = torch.cuda.Stream(device=dev)
     batch = bfb.Batch(envs)
     batch.set_stream(stream.cuda_stream)
+    tuned, _ = batch.autotune(DT, flags, trials=2)  # mode and launch shape; the fields are restored
+    tuned = {"mode": BATCH_MODE_NAMES[batch.mode], "warps_per_cta": tuned[0], "tiles_per_item": tuned[1]}
     batch.simulate(DT, warm, flags)
     stream.synchronize()
     rank_barrier(dev)
@@ -657,6 +674,7 @@ def run_ensemble_arm(args):
         "gpu_launches": None,
         "checksum_of_checksums": float(sums.sum()),
         "rank0_share": vs_mine / vs_all,
+        "batch_autotuned": tuned,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -37,6 +37,7 @@ BATCH_OPT_TILES_PER_ITEM = 2
 BATCH_OPT_MODE = 3
 BATCH_MODE_PERSISTENT = 0
 BATCH_MODE_STAGED = 1
+BATCH_MODE_GRAPH = 2
 
 ERRORS = {
     -1: "BFB_ERR_INVALID_ARG",
@@ -411,8 +412,9 @@ class Env:
 
 class Batch:
     """Many envs stepped together (a ``bfb_batch``): one launch per stage over
-    every env's tiles (``BATCH_MODE_STAGED``, the default) or one persistent
-    launch per step (``BATCH_MODE_PERSISTENT``)."""
+    every env's tiles (``BATCH_MODE_STAGED``, the default), one persistent
+    launch per step (``BATCH_MODE_PERSISTENT``), or every env's own kernels as
+    independent branches of one graph (``BATCH_MODE_GRAPH``)."""
 
     def __init__(self, envs):
         self.L = load_library()

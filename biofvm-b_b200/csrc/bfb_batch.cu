@@ -355,7 +355,9 @@ struct bfb_batch_s {
     int n_groups = 1;
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kSide] = {};
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;        // one step
+    cudaGraphExec_t graph_multi = nullptr;  // kMultiSteps steps (both built together)
+    static constexpr int kMultiSteps = 8;
     int graph_flags = -1;
     double graph_dt = 0;
     std::vector<uint64_t> graph_epochs;
@@ -367,6 +369,7 @@ int env_prepare_step(bfb_env_s *env, double dt, int flags);
 template <typename T>
 SweepArgs<T> env_sweep_args(bfb_env_s *env, int axis, double dt);
 int env_tile_plan(bfb_env_s *env, int elem, int Lp, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]);
+int env_run_steps(bfb_env_s *env, double dt, int n, int flags, cudaStream_t s);
 }  // namespace bfb
 
 using namespace bfb;
@@ -589,6 +592,22 @@ static int batch_launch_staged(bfb_batch_s *b, int flags, cudaStream_t s) {
     return BFB_OK;
 }
 
+// The graph mode: `steps` steps of each env as bfb_simulate launches them, on
+// the env's own stream, forked from and joined back into `s` (captured, the
+// envs are independent branches of one graph, each running its steps back to
+// back without waiting for the other envs between steps).
+static int batch_launch_graph(bfb_batch_s *b, double dt, int flags, int steps, cudaStream_t s) {
+    BFB_CUDA(cudaEventRecord(b->fork_ev, s));
+    for (bfb_env e : b->envs) BFB_CUDA(cudaStreamWaitEvent(e->stream, b->fork_ev, 0));
+    for (bfb_env e : b->envs) {
+        const int st = env_run_steps(e, dt, steps, flags, e->stream);
+        if (st) return st;
+        BFB_CUDA(cudaEventRecord(b->join_ev[0], e->stream));
+        BFB_CUDA(cudaStreamWaitEvent(s, b->join_ev[0], 0));
+    }
+    return BFB_OK;
+}
+
 template <typename T>
 static int batch_launch(bfb_batch_s *b, int flags, cudaStream_t s) {
     if (b->mode == BFB_BATCH_MODE_STAGED) return batch_launch_staged<T>(b, flags, s);
@@ -617,7 +636,9 @@ static int batch_launch(bfb_batch_s *b, int flags, cudaStream_t s) {
 
 static void batch_drop_graph(bfb_batch_s *b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->graph_multi) cudaGraphExecDestroy(b->graph_multi);
     b->graph = nullptr;
+    b->graph_multi = nullptr;
     b->graph_flags = -1;
 }
 
@@ -693,7 +714,8 @@ BFB_API int bfb_batch_set_option(bfb_batch b, int option, int value) {
         b->warps = value;
     else if (option == BFB_BATCH_OPT_TILES_PER_ITEM && value >= 1 && value <= 64)
         b->tiles_per_item = value;
-    else if (option == BFB_BATCH_OPT_MODE && (value == BFB_BATCH_MODE_PERSISTENT || value == BFB_BATCH_MODE_STAGED))
+    else if (option == BFB_BATCH_OPT_MODE && (value == BFB_BATCH_MODE_PERSISTENT || value == BFB_BATCH_MODE_STAGED ||
+                                             value == BFB_BATCH_MODE_GRAPH))
         b->mode = value;
     else
         return fail(BFB_ERR_INVALID_ARG, "bfb_batch_set_option: unknown option or value");
@@ -729,6 +751,33 @@ BFB_API int bfb_batch_synchronize(bfb_batch b) {
     return BFB_OK;
 }
 
+// `steps` steps of the batch in its mode, captured from its stream into one
+// graph (the envs' streams are idle: the caller synchronised them).
+static int batch_capture(bfb_batch_s *b, double dt, int flags, int steps, cudaGraphExec_t *out) {
+    cudaGraph_t g = nullptr;
+    BFB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int st = BFB_OK;
+    if (b->mode == BFB_BATCH_MODE_GRAPH)
+        st = batch_launch_graph(b, dt, flags, steps, b->stream);
+    else
+        for (int q = 0; q < steps && !st; ++q)
+            st = b->precision == BFB_FP64 ? batch_launch<double>(b, flags, b->stream)
+                                          : batch_launch<float>(b, flags, b->stream);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (st) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    return BFB_OK;
+}
+
 BFB_API int bfb_batch_simulate(bfb_batch b, double dt, int n_steps, int flags) {
     if (!b) return fail(BFB_ERR_INVALID_ARG, "null bfb_batch");
     if (n_steps < 0 || !(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "bad dt or n_steps");
@@ -745,24 +794,13 @@ BFB_API int bfb_batch_simulate(bfb_batch b, double dt, int n_steps, int flags) {
     }
     if (changed || !b->graph) {
         batch_drop_graph(b);
-        int st = b->precision == BFB_FP64 ? batch_upload<double>(b, dt) : batch_upload<float>(b, dt);
+        int st = b->mode == BFB_BATCH_MODE_GRAPH ? BFB_OK  // the envs' own launches need no tables
+                 : b->precision == BFB_FP64     ? batch_upload<double>(b, dt)
+                                                : batch_upload<float>(b, dt);
         if (st) return st;
         for (bfb_env e : b->envs) BFB_CUDA(cudaStreamSynchronize(e->stream));
-        cudaGraph_t g = nullptr;
-        BFB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        st = b->precision == BFB_FP64 ? batch_launch<double>(b, flags, b->stream) : batch_launch<float>(b, flags, b->stream);
-        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-        if (st) {
-            if (g) cudaGraphDestroy(g);
-            return st;
-        }
-        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&b->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            b->graph = nullptr;
-            return cuda_fail(e, "cudaGraphInstantiate");
-        }
+        if ((st = batch_capture(b, dt, flags, 1, &b->graph))) return st;
+        if ((st = batch_capture(b, dt, flags, bfb_batch_s::kMultiSteps, &b->graph_multi))) return st;
         b->graph_flags = flags;
         b->graph_dt = dt;
         b->graph_epochs.resize(b->n);
@@ -770,7 +808,10 @@ BFB_API int bfb_batch_simulate(bfb_batch b, double dt, int n_steps, int flags) {
     } else {
         for (bfb_env e : b->envs) BFB_CUDA(cudaStreamSynchronize(e->stream));
     }
-    for (int q = 0; q < n_steps; ++q) BFB_CUDA(cudaGraphLaunch(b->graph, b->stream));
+    int left = n_steps;
+    for (; b->graph_multi && left >= bfb_batch_s::kMultiSteps; left -= bfb_batch_s::kMultiSteps)
+        BFB_CUDA(cudaGraphLaunch(b->graph_multi, b->stream));
+    for (; left > 0; --left) BFB_CUDA(cudaGraphLaunch(b->graph, b->stream));
     return BFB_OK;
 }
 
@@ -805,6 +846,7 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
     for (int w : {1, 2, 4}) shapes.push_back({BFB_BATCH_MODE_STAGED, w, old_t});
     for (int w : {1, 2, 4})
         for (int tpi : {1, 2, 4, 8}) shapes.push_back({BFB_BATCH_MODE_PERSISTENT, w, tpi});
+    shapes.push_back({BFB_BATCH_MODE_GRAPH, old_w, old_t});
     for (const Shape &sh : shapes) {
         {
             const int w = sh.w, tpi = sh.tpi;
@@ -813,9 +855,11 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
             b->warps = w;
             b->tiles_per_item = tpi;
             batch_drop_graph(b);
-            if ((st = bfb_batch_simulate(b, dt, 1, flags))) break;  // builds the graph; warm
+            // builds both graphs and warms; then `trials` launches of the multi-step graph
+            const int steps = trials * bfb_batch_s::kMultiSteps;
+            if ((st = bfb_batch_simulate(b, dt, bfb_batch_s::kMultiSteps, flags))) break;
             cudaError_t ce = cudaEventRecord(e0, b->stream);
-            if (ce == cudaSuccess && (st = bfb_batch_simulate(b, dt, trials, flags))) break;
+            if (ce == cudaSuccess && (st = bfb_batch_simulate(b, dt, steps, flags))) break;
             if (ce == cudaSuccess) ce = cudaEventRecord(e1, b->stream);
             if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
             float ms = 0;
@@ -824,8 +868,8 @@ BFB_API int bfb_batch_autotune(bfb_batch b, double dt, int flags, int trials, in
                 st = cuda_fail(ce, "bfb_batch_autotune: timing");
                 break;
             }
-            if (best < 0 || ms / trials < best) {
-                best = ms / trials;
+            if (best < 0 || ms / steps < best) {
+                best = ms / steps;
                 best_w = w;
                 best_t = tpi;
                 best_m = sh.mode;

@@ -302,6 +302,12 @@ SweepArgs<T> env_sweep_args(bfb_env_s *env, int axis, double dt) {
 template SweepArgs<double> env_sweep_args<double>(bfb_env_s *, int, double);
 template SweepArgs<float> env_sweep_args<float>(bfb_env_s *, int, double);
 
+// One or more steps of the env on stream s, as bfb_simulate issues them (the
+// batch's graph mode captures these per env).
+int env_run_steps(bfb_env_s *env, double dt, int n, int flags, cudaStream_t s) {
+    return run_steps_any(env, dt, n, flags, s);
+}
+
 int env_tile_plan(bfb_env_s *env, int elem, int Lp, StridedGeom *gx, StridedGeom *gy, ContigGeom *gz, int vb16[3]) {
     const bool base16 = (reinterpret_cast<uintptr_t>(env->field) & 15) == 0;
     gx->axis = 0;

@@ -317,12 +317,13 @@ bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int ele
     return true;
 }
 
-// Resident lines per SM as the occupancy calculator gives them for the
-// sweep's kernel at each width (shared memory, its per-CTA reservation,
-// registers and the CTA limit all count). FP64 takes a narrower tile where it
-// keeps at least 1/8 more lines resident than 32 (256^3 x 8: 22 lines, five
-// warps per SM instead of three, x/y sweeps 0.520 -> 0.489 ms); FP32 tiles stay
-// at 32 lines (narrower ones measured 3-10% slower at 128^3 to 256^3).
+// Lines per strided TMA warp tile: 32, or for FP64 kNarrowLinesF64 where that
+// keeps at least 1/8 more lines resident per SM (by the occupancy calculator:
+// shared memory with its per-CTA reservation, registers and the CTA limit all
+// count). At 256^3 x 8 FP64 the narrow tile keeps five warps per SM instead
+// of three. FP32 tiles stay at 32 lines (narrower ones measured 3-10% slower
+// at 128^3 to 256^3). The tile's row stride is a compile-time constant, so
+// only these two widths are built.
 int strided_tile_lines(int n, int elem, int chunks) {
     if (elem != 8) return 32;
     if (chunks < 1) chunks = 1;
@@ -338,17 +339,8 @@ int strided_tile_lines(int n, int elem, int chunks) {
         }
         return (long long)ctas * w;
     };
-    const long long base = resident(32);
-    int best = 32;
-    long long best_resident = base + base / 8;
-    for (int w = 30; w >= 16; w -= 2) {  // FP64: tile x offsets of whole 16-byte vectors
-        const long long r = resident(w);
-        if (r >= best_resident && r > 0) {
-            best_resident = r;
-            best = w;
-        }
-    }
-    return best;
+    const long long base = resident(32), narrow = resident(kNarrowLinesF64);
+    return narrow > 0 && narrow >= base + base / 8 ? kNarrowLinesF64 : 32;
 }
 
 }  // namespace bfb

@@ -73,6 +73,10 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
+// Lines of the narrow FP64 strided tile: 22 x 8 B rows are whole 16-byte
+// vectors, and at 256 rows five such tiles fit an SM where three of 32 do.
+constexpr int kNarrowLinesF64 = 22;
+
 // Rows per TMA box (one row group) of a strided tile of `lines` lines of n
 // rows in `chunks` groups: ceil(n / chunks), rounded up so that every group's
 // shared-memory start (a multiple of crow*lines*elem bytes past the 128-byte

@@ -7,23 +7,23 @@
 
 namespace bfb {
 
-// The line solve of one strided warp tile (g.tw <= 32 lines of one slab, one
-// lane per line; lanes past g.tw have no line), shared by the TMA tiles of
-// the forward sweeps. Row q of this lane's line is col[q * rs] in shared
+// The line solve of one strided warp tile (RS <= 32 lines of one slab, one
+// lane per line; lanes past RS have no line), shared by the TMA tiles of
+// the forward sweeps. Row q of this lane's line is col[q * RS] in shared
 // memory. wait(ch) returns once row
 // group ch (rows [ch*crow, (ch+1)*crow)) has landed, false when its bounded
 // wait ran out; flush(ch) writes row group ch back once its rows are final
 // (the back substitution finishes the groups from the last to the first).
 // Returns false when a wait ran out.
-template <typename T, bool FUSE_PRE, bool BULK, typename WAIT, typename FLUSH>
+template <typename T, bool FUSE_PRE, bool BULK, int RS, typename WAIT, typename FLUSH>
 __device__ __forceinline__ bool strided_solve(const SweepArgs<T> &a, const StridedGeom &g, int crow, int slab,
-                                              long long col0, T *__restrict__ col, const int rs, WAIT wait,
-                                              FLUSH flush) {
+                                              long long col0, T *__restrict__ col, WAIT wait, FLUSH flush) {
+    constexpr int rs = RS;  // a compile-time row stride keeps the row loops free of address arithmetic
     const int lane = threadIdx.x & 31;
     const int n = g.n;
     const long long P = g.P;
     const int nch = (n + crow - 1) / crow;
-    if (lane >= g.tw) {  // no line: follow the row groups' waits and flushes
+    if (lane >= rs) {  // no line: follow the row groups' waits and flushes
         for (int ch = 0; ch < nch; ++ch)
             if (!wait(ch)) return false;
         for (int ch = nch - 1; ch >= 0; --ch) flush(ch);
@@ -123,24 +123,24 @@ __device__ __forceinline__ bool strided_solve(const SweepArgs<T> &a, const Strid
     return true;
 }
 
-// One warp tile of a strided sweep with TMA: g.tw lines of `tile`, in the
+// One warp tile of a strided sweep with TMA: TW lines of `tile`, in the
 // warp's region `wbase` (128-byte header of row-group mbarriers, then the
 // tile). The mbarriers are initialised by the caller; row group ch waits for
 // parity bit ch of `phase`, and every call completes one phase of each of
 // its row groups. Returns false (error flag set) when a bounded wait ran out.
-template <typename T, bool FUSE_PRE, bool BULK>
-__device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const CUtensorMap *map_out,
-                                                 const SweepArgs<T> &a, const StridedGeom &g, int crow, long long tile,
-                                                 unsigned char *wbase, unsigned phase) {
+template <typename T, bool FUSE_PRE, bool BULK, int TW>
+__device__ __forceinline__ bool strided_tma_tile_w(const CUtensorMap *map, const CUtensorMap *map_out,
+                                                   const SweepArgs<T> &a, const StridedGeom &g, int crow,
+                                                   long long tile, unsigned char *wbase, unsigned phase) {
     const int lane = threadIdx.x & 31;
     const int slab = (int)(tile / g.ncb);
-    const int col0 = (int)((tile % g.ncb) * g.tw);
+    const int col0 = (int)((tile % g.ncb) * TW);
     const int nch = (g.n + crow - 1) / crow;
     const int rank = g.axis == 0 ? 2 : 3;
     const unsigned bar0 = smem_u32(wbase);
     T *__restrict__ sm = reinterpret_cast<T *>(wbase + 128);
     const unsigned sm_u32 = smem_u32(sm);
-    const unsigned chunk_bytes = (unsigned)crow * (unsigned)g.tw * (unsigned)sizeof(T);
+    const unsigned chunk_bytes = (unsigned)crow * (unsigned)TW * (unsigned)sizeof(T);
 
     if (lane == 0) {
         for (int ch = 0; ch < nch; ++ch) {
@@ -161,10 +161,23 @@ __device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const C
             bulk_commit();
         }
     };
-    if (!strided_solve<T, FUSE_PRE, BULK>(a, g, crow, slab, col0, sm + lane, g.tw, wait, flush)) return false;
+    if (!strided_solve<T, FUSE_PRE, BULK, TW>(a, g, crow, slab, col0, sm + lane, wait, flush)) return false;
     if (lane == 0) bulk_wait_read_all();  // the tile must outlive the stores' reads
     __syncwarp();
     return true;
+}
+
+// The tile at the geometry's width: 32 lines, or kNarrowLinesF64 for FP64.
+template <typename T, bool FUSE_PRE, bool BULK>
+__device__ __forceinline__ bool strided_tma_tile(const CUtensorMap *map, const CUtensorMap *map_out,
+                                                 const SweepArgs<T> &a, const StridedGeom &g, int crow, long long tile,
+                                                 unsigned char *wbase, unsigned phase) {
+    if constexpr (sizeof(T) == 8) {
+        if (g.tw == kNarrowLinesF64)
+            return strided_tma_tile_w<T, FUSE_PRE, BULK, kNarrowLinesF64>(map, map_out, a, g, crow, tile, wbase,
+                                                                         phase);
+    }
+    return strided_tma_tile_w<T, FUSE_PRE, BULK, 32>(map, map_out, a, g, crow, tile, wbase, phase);
 }
 
 // One warp tile of the pipelined z sweep (rows row0 .. row0 + R - 1 of

@@ -261,11 +261,14 @@ BFB_API int bfb_checksum(bfb_env env, double *out);
  * Many independent envs (uneven shapes and substrate counts; one device and
  * one precision) stepped together: bfb_batch_simulate runs one LOD step of
  * every env -- and, with BFB_STEP_CELLS, its agents -- replayed from a CUDA
- * graph, in one of two modes:
+ * graph, in one of three modes:
  *   BFB_BATCH_MODE_STAGED (default): one launch per stage (x, y, z sweeps,
  *     agents), each a flat grid over every env's tiles, one warp per tile;
  *   BFB_BATCH_MODE_PERSISTENT: ONE persistent kernel launch per step whose
- *     warps pull (env, stage, tile) work items from a device queue.
+ *     warps pull (env, stage, tile) work items from a device queue;
+ *   BFB_BATCH_MODE_GRAPH: every env's own step kernels (as bfb_simulate
+ *     launches them), one independent branch per env of the step's graph,
+ *     so the hardware schedules the envs' CTAs side by side.
  * The batch references the envs; they must outlive it, and their own settings
  * (coefficients, Dirichlet, agents) are the ones used.
  * bfb_batch_simulate_loop runs the same steps as one bfb_simulate call per
@@ -274,9 +277,10 @@ BFB_API int bfb_checksum(bfb_env env, double *out);
 typedef struct bfb_batch_s *bfb_batch;
 #define BFB_BATCH_OPT_WARPS_PER_CTA 1   /* 1..4, default 1 */
 #define BFB_BATCH_OPT_TILES_PER_ITEM 2  /* warp tiles per queue item (persistent mode), 1..64, default 2 */
-#define BFB_BATCH_OPT_MODE 3            /* BFB_BATCH_MODE_STAGED (default) or BFB_BATCH_MODE_PERSISTENT */
+#define BFB_BATCH_OPT_MODE 3            /* BFB_BATCH_MODE_STAGED (default), _PERSISTENT or _GRAPH */
 #define BFB_BATCH_MODE_PERSISTENT 0
 #define BFB_BATCH_MODE_STAGED 1
+#define BFB_BATCH_MODE_GRAPH 2
 BFB_API int bfb_batch_create(bfb_batch *out, int n_envs, const bfb_env *envs);
 BFB_API int bfb_batch_destroy(bfb_batch batch);
 BFB_API int bfb_batch_set_option(bfb_batch batch, int option, int value);
@@ -288,14 +292,15 @@ BFB_API int bfb_batch_simulate_loop(bfb_batch batch, double dt, int n_steps, int
  * instead (NULL: back to its own), e.g. to time them with events there. */
 BFB_API int bfb_batch_set_stream(bfb_batch batch, void *cuda_stream);
 BFB_API int bfb_batch_synchronize(bfb_batch batch);
-/* Times bfb_batch_simulate in the staged mode with warps per CTA {1, 2, 4}
- * and in the persistent mode with warps per CTA {1, 2, 4} x tiles per item
- * {1, 2, 4, 8} (one warm step and `trials` timed steps each, CUDA events),
- * keeps the fastest and returns it in chosen[2] = {warps, tiles per item}
- * (the mode: bfb_batch_get_option with BFB_BATCH_OPT_MODE) and its
- * milliseconds per step in *best_ms (either may be NULL). The trial steps
- * advance the envs' fields, so every field is saved first and restored
- * before returning. Not in the reference. */
+/* Times bfb_batch_simulate in the staged mode with warps per CTA {1, 2, 4},
+ * in the persistent mode with warps per CTA {1, 2, 4} x tiles per item
+ * {1, 2, 4, 8} and in the graph mode (8 warm steps and 8*`trials` timed
+ * steps each, CUDA events; bfb_batch_simulate replays 8 steps per graph
+ * launch while at least 8 remain), keeps the fastest and returns it in
+ * chosen[2] = {warps, tiles per item} (the mode: bfb_batch_get_option with
+ * BFB_BATCH_OPT_MODE) and its milliseconds per step in *best_ms (either may
+ * be NULL). The trial steps advance the envs' fields, so every field is
+ * saved first and restored before returning. Not in the reference. */
 BFB_API int bfb_batch_autotune(bfb_batch batch, double dt, int flags, int trials, int *chosen, double *best_ms);
 
 /* ---- Reverse mode ---------------------------------------------------------

@@ -1,5 +1,6 @@
-"""Batched ensembles over many uneven envs, in both modes: one launch per
-stage over every env's tiles (staged) and one persistent launch per step."""
+"""Batched ensembles over many uneven envs, in all three modes: one launch per
+stage over every env's tiles (staged), one persistent launch per step, and
+the envs' own kernels as branches of one graph."""
 from __future__ import annotations
 
 import math
@@ -12,6 +13,7 @@ from conftest import log_uniform
 from oracle.oracle import face_mask_all
 
 pytestmark = pytest.mark.gpu
+MODES = {"persistent": 0, "staged": 1, "graph": 2}  # BFB_BATCH_MODE_*
 
 
 def make_instance(bfb, rng, edge_lo, edge_hi, n_agents_max, prec, dt):
@@ -58,14 +60,14 @@ def oracle_run(oracle, spec, dt, steps):
     return rho
 
 
-@pytest.mark.parametrize("mode", ["staged", "persistent"])
+@pytest.mark.parametrize("mode", ["staged", "persistent", "graph"])
 @pytest.mark.parametrize("warps", [1, 2])
 def test_batch_small_fp64_bitexact(bfb, oracle, warps, mode):
     rng = np.random.default_rng(404)
     dt, steps = 0.01, 4
     specs, envs = zip(*[make_instance(bfb, rng, 2, 24, 300, bfb.FP64, dt) for _ in range(12)])
     batch = bfb.Batch(envs)
-    batch.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
+    batch.set_mode(MODES[mode])
     batch.set_warps(warps)
     batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
     batch.synchronize()
@@ -94,14 +96,15 @@ def make_aligned_instance(bfb, rng, prec, dt, n_agents=400):
 
 
 @pytest.mark.parametrize("mode,warps,tiles", [("persistent", 1, 1), ("persistent", 2, 3), ("persistent", 4, 8),
-                                              ("persistent", 1, 64), ("staged", 1, 2), ("staged", 4, 2)])
+                                              ("persistent", 1, 64), ("staged", 1, 2), ("staged", 4, 2),
+                                              ("graph", 1, 2)])
 def test_batch_tma_items_fp64_bitexact(bfb, oracle, mode, warps, tiles):
     rng = np.random.default_rng(900 + warps * 10 + tiles)
     dt, steps = 0.01, 3
     specs, envs = zip(*[make_aligned_instance(bfb, rng, bfb.FP64, dt) for _ in range(6)])
     batch = bfb.Batch(envs)
-    batch.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
-    assert batch.mode == (bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
+    batch.set_mode(MODES[mode])
+    assert batch.mode == MODES[mode]
     batch.set_warps(warps)
     batch.set_tiles_per_item(tiles)
     batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
@@ -110,7 +113,7 @@ def test_batch_tma_items_fp64_bitexact(bfb, oracle, mode, warps, tiles):
         assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps)), spec["shape"]
 
 
-@pytest.mark.parametrize("mode", ["staged", "persistent"])
+@pytest.mark.parametrize("mode", ["staged", "persistent", "graph"])
 def test_batch_wide_substrates_fp64_bitexact(bfb, oracle, mode):
     """Envs with more than 32 substrates (a lane solves several z lines) next
     to ordinary ones in one batch."""
@@ -128,7 +131,7 @@ def test_batch_wide_substrates_fp64_bitexact(bfb, oracle, mode):
         specs.append(spec)
         envs.append(build(bfb, spec, bfb.FP64, dt))
     batch = bfb.Batch(envs)
-    batch.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
+    batch.set_mode(MODES[mode])
     batch.simulate(dt, steps, bfb.STEP_DIFFUSION)
     batch.synchronize()
     for spec, env in zip(specs, envs):
@@ -143,7 +146,7 @@ def test_batch_autotune_restores_fields(bfb, oracle):
     before = [e.get_field_raw() for e in envs]
     (w, t), ms = batch.autotune(dt, bfb.STEP_DIFFUSION | bfb.STEP_CELLS, trials=1)
     assert w in (1, 2, 4) and t in (1, 2, 4, 8) and ms > 0
-    assert batch.mode in (bfb.BATCH_MODE_STAGED, bfb.BATCH_MODE_PERSISTENT)
+    assert batch.mode in (bfb.BATCH_MODE_STAGED, bfb.BATCH_MODE_PERSISTENT, bfb.BATCH_MODE_GRAPH)
     for e, b0 in zip(envs, before):
         assert np.array_equal(e.get_field_raw(), b0)
     batch.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
@@ -152,7 +155,7 @@ def test_batch_autotune_restores_fields(bfb, oracle):
         assert np.array_equal(env.get_field(), oracle_run(oracle, spec, dt, steps))
 
 
-@pytest.mark.parametrize("mode", ["staged", "persistent"])
+@pytest.mark.parametrize("mode", ["staged", "persistent", "graph"])
 def test_batch_fp32_equals_per_instance_loop(bfb, mode):
     rng = np.random.default_rng(405)
     dt, steps = 0.01, 5
@@ -161,7 +164,7 @@ def test_batch_fp32_equals_per_instance_loop(bfb, mode):
     envs_b = [m[1] for m in made]
     envs_l = [build(bfb, sp, bfb.FP32, dt) for sp in specs]
     b = bfb.Batch(envs_b)
-    b.set_mode(bfb.BATCH_MODE_STAGED if mode == "staged" else bfb.BATCH_MODE_PERSISTENT)
+    b.set_mode(MODES[mode])
     b.simulate(dt, steps, bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
     b.synchronize()
     lp = bfb.Batch(envs_l)
@@ -198,9 +201,11 @@ def test_ensemble_256_batch_vs_loop_and_fp64_check(bfb):
     t_pers = timed(20)
     batch.set_mode(bfb.BATCH_MODE_STAGED)
     t_staged = timed(20)
+    batch.set_mode(bfb.BATCH_MODE_GRAPH)
+    t_graph = timed(20)
     tuned, _ = batch.autotune(dt, flags, trials=2)  # mode, warps per CTA and tiles per item
-    mode = "staged" if batch.mode == bfb.BATCH_MODE_STAGED else "persistent"
-    t_batch = timed(steps - 44)  # 202 steps in all (3 x 2 warm + 20 + 20 + 156), as the FP64 check below
+    mode = {v: k for k, v in MODES.items()}[batch.mode]
+    t_batch = timed(steps - 66)  # 202 steps in all (4 x 2 warm + 3 x 20 + 134), as the FP64 check below
     # per-instance launch loop over fresh copies of the same envs
     loop_envs = [build(bfb, sp, bfb.FP32, dt) for sp in specs]
     loop = bfb.Batch(loop_envs)
@@ -219,7 +224,8 @@ def test_ensemble_256_batch_vs_loop_and_fp64_check(bfb):
         e64.close()
     print(f"\nuneven ensemble (256 envs, {vs / 1e6:.0f} M voxel*substrates, 200 steps): batch, autotuned "
           f"({mode}, warps, tiles per item = {tuned}) {t_batch * 1e3:.3f} ms/step ({vs / t_batch:.3e} vox*sub/s); "
-          f"staged (1 warp) {t_staged * 1e3:.3f}, persistent (1 warp, 4 tiles) {t_pers * 1e3:.3f}; "
+          f"staged (1 warp) {t_staged * 1e3:.3f}, persistent (1 warp, 4 tiles) {t_pers * 1e3:.3f}, "
+          f"graph {t_graph * 1e3:.3f}; "
           f"per-instance loop {t_loop * 1e3:.3f} ms/step ({vs / t_loop:.3e}); "
           f"FP32 vs FP64 rel Linf on 8 envs: max {max(errs):.2e}")
     assert max(errs) <= 1e-5
