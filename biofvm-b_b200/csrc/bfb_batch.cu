@@ -303,7 +303,10 @@ __global__ void __launch_bounds__(128, 1)
                 switch (I.S) {  // the substrate count as a constant where it is a common one
                 case 1: contig_pipe_tile<T, 1>(ax, gz, I.kc, tile, wbase, 0u); break;
                 case 2: contig_pipe_tile<T, 2>(ax, gz, I.kc, tile, wbase, 0u); break;
+                case 3: contig_pipe_tile<T, 3>(ax, gz, I.kc, tile, wbase, 0u); break;
                 case 4: contig_pipe_tile<T, 4>(ax, gz, I.kc, tile, wbase, 0u); break;
+                case 5: contig_pipe_tile<T, 5>(ax, gz, I.kc, tile, wbase, 0u); break;
+                case 6: contig_pipe_tile<T, 6>(ax, gz, I.kc, tile, wbase, 0u); break;
                 case 8: contig_pipe_tile<T, 8>(ax, gz, I.kc, tile, wbase, 0u); break;
                 default: contig_pipe_tile<T, 0>(ax, gz, I.kc, tile, wbase, 0u); break;
                 }

@@ -174,8 +174,9 @@ size_t contig_smem(int nz, int S, int Lp, int elem, int warps, int *R, int *RS);
 // contig_smem's conflict-free stride (RS = S mod 32) is not a multiple of 16
 // bytes (S not a multiple of 4 in FP32, odd S in FP64): RS >= nz*S a multiple
 // of 16 bytes, chosen among its residues so that the most rows keep the warp's
-// accesses free of bank conflicts (lane (r, d) reads element r*RS + k*S + d);
-// false when fewer than 16 lanes would be busy (FP32 S = 1).
+// accesses free of bank conflicts (lane (r, d) reads element r*RS + k*S + d),
+// or with two-way conflicts where conflict-free strides keep fewer than 16
+// lanes busy (FP32 S = 1); false when even that leaves fewer than 16.
 bool contig_aligned_geom(int nz, int S, int Lp, int elem, int *R, int *RS);
 
 // Opt the shared-memory kernels into 227 KB, once per device.

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(128, 1) sweep_contig_tma_kernel(SweepArgs<T> a
 // forward elimination starts on group 0 while the later groups land, and the
 // back substitution stores each finished group while the lower ones are
 // still being computed. SC is the substrate count when it is a compile-time
-// constant (1, 2, 4, 8), 0 otherwise; every lane owns at most one line
+// constant (1 to 6, 8), 0 otherwise; every lane owns at most one line
 // (S <= 32 gives R = 32/S rows per warp).
 // ---------------------------------------------------------------------------
 template <typename T, int SC>
@@ -220,7 +220,10 @@ int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cud
         switch (a.S) {
         case 1: sweep_contig_pipe_kernel<T, 1><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
         case 2: sweep_contig_pipe_kernel<T, 2><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        case 3: sweep_contig_pipe_kernel<T, 3><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
         case 4: sweep_contig_pipe_kernel<T, 4><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        case 5: sweep_contig_pipe_kernel<T, 5><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
+        case 6: sweep_contig_pipe_kernel<T, 6><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
         case 8: sweep_contig_pipe_kernel<T, 8><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
         default: sweep_contig_pipe_kernel<T, 0><<<blocks, warps * 32, smem, s>>>(a, g, kc); break;
         }
@@ -254,12 +257,18 @@ void tma_prepare_device() {
     opt_in_tma(sweep_strided_tma_kernel<float, false, false>);
     opt_in_tma(sweep_contig_pipe_kernel<double, 1>);
     opt_in_tma(sweep_contig_pipe_kernel<double, 2>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 3>);
     opt_in_tma(sweep_contig_pipe_kernel<double, 4>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 5>);
+    opt_in_tma(sweep_contig_pipe_kernel<double, 6>);
     opt_in_tma(sweep_contig_pipe_kernel<double, 8>);
     opt_in_tma(sweep_contig_pipe_kernel<double, 0>);
     opt_in_tma(sweep_contig_pipe_kernel<float, 1>);
     opt_in_tma(sweep_contig_pipe_kernel<float, 2>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 3>);
     opt_in_tma(sweep_contig_pipe_kernel<float, 4>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 5>);
+    opt_in_tma(sweep_contig_pipe_kernel<float, 6>);
     opt_in_tma(sweep_contig_pipe_kernel<float, 8>);
     opt_in_tma(sweep_contig_pipe_kernel<float, 0>);
     opt_in_tma(sweep_contig_tma_kernel<double>);
