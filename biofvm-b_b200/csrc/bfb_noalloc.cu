@@ -8,6 +8,8 @@
 // synchronize the whole device. bfb_checksum_noalloc runs the same two
 // reduction kernels with their scratch in a fixed array compiled into this
 // library instead, so it allocates nothing.
+#include <mutex>
+
 #include "bfb_aux.cuh"
 #include "bfb_internal.cuh"
 
@@ -24,13 +26,21 @@ constexpr int kNoallocBlocks = 296;  // reduction blocks (2 per SM of a B200)
 static __device__ __align__(256) double g_noalloc_partials[kNoallocBlocks * BFB_NOALLOC_MAX_SUBSTRATES];
 
 // Host code may not take the array's address directly (its host-side name
-// is a stand-in, not a device address). It is looked up on every call, for
-// the current device: the lookup allocates nothing, and no address outlives
-// a device reset between calls.
+// is a stand-in, not a device address); it is looked up once per device.
+std::mutex g_mu;
+double *g_partials_dev[64] = {nullptr};
+
 int partials_for_current_device(double **out) {
-    void *p = nullptr;
-    BFB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partials));
-    *out = static_cast<double *>(p);
+    int dev = 0;
+    BFB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return bfb::fail(BFB_ERR_UNSUPPORTED, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_partials_dev[dev]) {
+        void *p = nullptr;
+        BFB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partials));
+        g_partials_dev[dev] = static_cast<double *>(p);
+    }
+    *out = g_partials_dev[dev];
     return BFB_OK;
 }
 

@@ -341,9 +341,12 @@ BFB_API int bfb_adjoint_run(bfb_env env, double dt, int n_steps, int flags, int 
  * and the call returns without waiting. Its scratch is a fixed array inside
  * the library, so at most BFB_NOALLOC_MAX_SUBSTRATES substrates (larger counts
  * return BFB_ERR_SIZE), and calls that overlap on the GPU share that array and
- * race: order them on one stream. Each call looks the array's device address
- * up on the current device (cudaGetSymbolAddress). The call allocates
- * nothing. */
+ * race: order them on one stream. The first call on each device looks the
+ * array's device address up (cudaGetSymbolAddress) and keeps it for the rest
+ * of the process; make that first call before capturing a stream. The kept
+ * address does not survive a reset of the device's primary context
+ * (cudaDeviceReset): do not call this entry point after one. The call
+ * allocates nothing. */
 #define BFB_NOALLOC_MAX_SUBSTRATES 64
 BFB_API int bfb_checksum_noalloc(const void *field_dev, int precision, long long n_voxels, int n_substrates,
                                  double *out_dev, void *stream);
