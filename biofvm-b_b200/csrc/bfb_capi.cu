@@ -244,6 +244,9 @@ static void encode_field_maps(bfb_env_s *env) {
         env->tma_ok[a] = make_sweep_tensor_map(&env->tmap[a], &env->tma_crow[a], env->field, (int)env->elem, a,
                                                env->nx, env->ny, env->nz, env->S, chunks, env->Lp,
                                                env->tma_lines[a]);
+        const int n = a == 0 ? env->nx : env->ny;
+        env->tmem_ok[a] = env->precision == BFB_FP64 && tmem_sweep_fits(n) &&
+                          make_tmem_sweep_map(&env->tmem_map[a], env->field, a, env->nx, env->ny, env->Lp);
     }
 }
 
@@ -251,8 +254,16 @@ static void encode_field_maps(bfb_env_s *env) {
 // into the x-sweep load.
 template <typename T>
 static int launch_strided_env(bfb_env_s *env, int axis, bool bulk, double dt, cudaStream_t s) {
-    return launch_strided<T>(make_args<T>(env, axis, bulk, dt), axis, axis == 0, env->tuning.warps[axis],
-                             tma_map(env, axis), tma_map(env, axis), env->tma_crow[axis], env->tma_lines[axis], s);
+    const SweepArgs<T> a = make_args<T>(env, axis, bulk, dt);
+    if constexpr (sizeof(T) == 8) {  // the tensor-memory tiles where the tuning asks for them
+        if (env->use_tma && env->tuning.tma[axis] == 2 && env->tmem_ok[axis]) {
+            const int st = launch_strided_tmem(a, strided_geometry(a, axis), &env->tmem_map[axis],
+                                               &env->tmem_map[axis], axis == 0 && (a.dir.any || a.bulk.on), s);
+            if (st != kNotApplicable) return st;
+        }
+    }
+    return launch_strided<T>(a, axis, axis == 0, env->tuning.warps[axis], tma_map(env, axis), tma_map(env, axis),
+                             env->tma_crow[axis], env->tma_lines[axis], s);
 }
 
 template <typename T>
@@ -982,7 +993,7 @@ BFB_API int bfb_host_unregister(void *host) {
 static bool tuning_valid(const int *v) {
     for (int a = 0; a < 3; ++a) {
         const int tma = v[3 * a], warps = v[3 * a + 1], chunks = v[3 * a + 2];
-        if (tma < 0 || tma > 1 || warps < 1 || warps > 4 || chunks < 1 || chunks > 16) return false;
+        if (tma < 0 || tma > 2 || warps < 1 || warps > 4 || chunks < 1 || chunks > 16) return false;
     }
     return true;
 }
@@ -1002,7 +1013,7 @@ BFB_API int bfb_set_tuning(bfb_env env, const int *shape) {
     int st = check_env(env);
     if (st) return st;
     if (!shape) return fail(BFB_ERR_INVALID_ARG, "shape is NULL");
-    if (!tuning_valid(shape)) return fail(BFB_ERR_INVALID_ARG, "tuning: tma 0/1, warps 1..4, chunks 1..16 per axis");
+    if (!tuning_valid(shape)) return fail(BFB_ERR_INVALID_ARG, "tuning: tma 0..2, warps 1..4, chunks 1..16 per axis");
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     apply_tuning(env, shape);
     return BFB_OK;

@@ -171,6 +171,9 @@ struct bfb_env_s {
     int tma_crow[2] = {0, 0};
     int tma_lines[2] = {32, 32};  // lines per warp tile of the maps' boxes
     int tma_ok[2] = {0, 0};
+    // FP64: maps of 16-row boxes for the tensor-memory x/y sweeps (tuning tma = 2)
+    CUtensorMap tmem_map[2];
+    int tmem_ok[2] = {0, 0};
 
     // sticky device error flag (a bounded wait in a kernel ran out)
     int *d_err = nullptr;

@@ -346,20 +346,7 @@ static int go_strided(const SweepArgs<T> &a, const StridedGeom &g, int warps, si
 template <typename T>
 int launch_strided(const SweepArgs<T> &a, int axis, bool fuse_pre, int warps, const CUtensorMap *map,
                    const CUtensorMap *map_out, int crow, int lines, cudaStream_t s) {
-    StridedGeom g;
-    g.axis = axis;
-    if (axis == 0) {
-        g.n = a.nx;
-        g.P = (long long)a.ny * a.Lp;
-        g.slab_stride = 0;
-        g.n_slabs = 1;
-    } else {
-        g.n = a.ny;
-        g.P = a.Lp;
-        g.slab_stride = (long long)a.ny * a.Lp;
-        g.n_slabs = a.nx;
-    }
-    g.ncb = (int)((g.P + 31) / 32);
+    StridedGeom g = strided_geometry(a, axis);
     warps = std::max(1, std::min(warps, 4));
     // the x sweep's load-time Dirichlet and bulk update: without either, the
     // plain kernel computes the same
@@ -557,6 +544,7 @@ void sweeps_prepare_device() {
     opt_in(sweep_contig_wide_kernel<float, 8>);
     opt_in(sweep_contig_wide_kernel<float, 4>);
     tma_prepare_device();
+    tmem_prepare_device();
     done |= 1ull << (dev & 63);
 }
 

@@ -152,11 +152,41 @@ int launch_contig_tma(const SweepArgs<T> &a, const ContigGeom &g, int warps, cud
 // warp tile, <= 32, a whole number of 16-byte vectors).
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
                            int S, int chunks, int Lp, int lines);
+// The same with the box's rows given (crow <= 256).
+bool make_sweep_tensor_map_rows(CUtensorMap *out, void *field, int elem, int axis, int nx, int ny, int Lp, int lines,
+                                int crow);
 // Lines per strided TMA warp tile for lines of n rows in `chunks` row groups:
 // the width that keeps the most lines resident per SM (a line's rows all sit
 // in shared memory, so FP64 tiles of 32 long lines leave few warps per SM and
 // a narrower tile fits more of them); 32 on ties.
 int strided_tile_lines(int n, int elem, int chunks);
+// FP64 x/y sweeps with each line's forward results in tensor memory
+// (bfb_tmem.cu): lines of 16 to 256 rows, 32-line tiles, tensor maps of
+// 16-row boxes. launch_strided_tmem returns kNotApplicable for other lines.
+bool tmem_sweep_fits(int n);
+bool make_tmem_sweep_map(CUtensorMap *out, void *field, int axis, int nx, int ny, int Lp);
+int launch_strided_tmem(const SweepArgs<double> &a, const StridedGeom &g, const CUtensorMap *map,
+                        const CUtensorMap *map_out, bool fuse_pre, cudaStream_t s);
+void tmem_prepare_device();
+// The strided geometry of a sweep over args a (axis 0: x, 1: y), 32-line tiles.
+template <typename T>
+inline StridedGeom strided_geometry(const SweepArgs<T> &a, int axis) {
+    StridedGeom g;
+    g.axis = axis;
+    if (axis == 0) {
+        g.n = a.nx;
+        g.P = (long long)a.ny * a.Lp;
+        g.slab_stride = 0;
+        g.n_slabs = 1;
+    } else {
+        g.n = a.ny;
+        g.P = a.Lp;
+        g.slab_stride = (long long)a.ny * a.Lp;
+        g.n_slabs = a.nx;
+    }
+    g.ncb = (int)((g.P + 31) / 32);
+    return g;
+}
 void tma_prepare_device();
 // One bounded mbarrier wait that nothing completes, `polls` polls long; sets
 // *err like a stalled copy would (bfb_watchdog_selftest).

@@ -302,16 +302,24 @@ static EncodeTiledFn encode_fn() {
 // of 16 bytes, box rows <= 256); the cp.async kernels handle those grids.
 bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int elem, int axis, int nx, int ny, int nz,
                            int S, int chunks, int Lp, int lines) {
-    EncodeTiledFn fn = encode_fn();
-    if (!fn) return false;
-    if (lines < 1 || lines > 32 || (lines * elem) % 16 != 0) return false;  // tile x offsets stay 16-byte aligned
     (void)nz;
     (void)S;
     const int n = axis == 0 ? nx : ny;
-    const long long P = axis == 0 ? (long long)ny * Lp : (long long)Lp;
     if (chunks < 1 || chunks > 16) return false;  // one mbarrier per row group in a 128-byte header
     const int crow = strided_box_rows(n, chunks, lines, elem);
-    if (crow > 256 || (P * elem) % 16 != 0 || (reinterpret_cast<uintptr_t>(field) & 15)) return false;
+    if (!make_sweep_tensor_map_rows(out, field, elem, axis, nx, ny, Lp, lines, crow)) return false;
+    *crow_out = crow;
+    return true;
+}
+
+bool make_sweep_tensor_map_rows(CUtensorMap *out, void *field, int elem, int axis, int nx, int ny, int Lp, int lines,
+                                int crow) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    if (lines < 1 || lines > 32 || (lines * elem) % 16 != 0) return false;  // tile x offsets stay 16-byte aligned
+    const int n = axis == 0 ? nx : ny;
+    const long long P = axis == 0 ? (long long)ny * Lp : (long long)Lp;
+    if (crow < 1 || crow > 256 || (P * elem) % 16 != 0 || (reinterpret_cast<uintptr_t>(field) & 15)) return false;
     if (P > 0xffffffffLL) return false;
     cuuint64_t dims[3] = {(cuuint64_t)P, (cuuint64_t)n, (cuuint64_t)nx};
     cuuint64_t strides[2] = {(cuuint64_t)(P * elem), (cuuint64_t)((long long)ny * P * elem)};
@@ -321,9 +329,7 @@ bool make_sweep_tensor_map(CUtensorMap *out, int *crow_out, void *field, int ele
     const CUresult r = fn(out, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank,
                           field, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return false;
-    *crow_out = crow;
-    return true;
+    return r == CUDA_SUCCESS;
 }
 
 // Lines per strided TMA warp tile: 32, or for FP64 kNarrowLinesF64 where that

@@ -217,11 +217,16 @@ BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, do
 /* ---- Launch-shape tuning -------------------------------------------------
  * No counterpart in the reference. The launch shape of the x, y and z sweeps:
  * shape[3*axis + 0] = 1 for TMA tiles (where the grid allows them), 0 for
- * cp.async tiles; shape[3*axis + 1] = warps (tiles) per CTA, 1..4;
- * shape[3*axis + 2] = row groups per TMA tile (pipeline stages), 1..16.
+ * cp.async tiles, 2 (FP64 x and y sweeps, lines of 16 to 256 rows; else as 1)
+ * for TMA tiles whose lines' forward results are held in tensor memory;
+ * shape[3*axis + 1] = warps (tiles) per CTA, 1..4;
+ * shape[3*axis + 2] = row groups per TMA tile (pipeline stages), 1..16
+ * (the tensor-memory tiles keep their own: 4 warps, 16-row groups).
  * Every shape computes the same numbers (FP64 bit for bit); only the speed
  * differs. Defaults {1, 1, 2} per axis. bfb_autotune times each candidate
- * (TMA / cp.async x 1, 2, 4 warps x 2, 4, 8 row groups) of each sweep with
+ * (TMA / cp.async x 1, 2, 4 warps x 2, 4, 8 row groups; not the
+ * tensor-memory tiles, which measured slower on every grid tried) of each
+ * sweep with
  * CUDA events over `trials` launches, out of place from the env's field into
  * a scratch field (the field is unchanged; the scratch is freed on return),
  * keeps the fastest and returns it in chosen[BFB_TUNING_FIELDS] and its

@@ -19,6 +19,7 @@ from oracle.oracle import face_mask_all
 pytestmark = pytest.mark.gpu
 
 SHAPES = [((tma, warps, chunks),) * 3 for tma, warps, chunks in itertools.product((1, 0), (1, 2, 4), (2, 4, 8))]
+SHAPES.append(((2, 1, 2),) * 3)  # FP64 x/y: the tensor-memory tiles (elsewhere as TMA tiles)
 
 
 def _problem(rng, shape=(40, 36, 48), S=2, n_agents=800, dx=20.0, dt=0.01):
@@ -94,7 +95,7 @@ def test_autotune_keeps_field_and_results(bfb, oracle):
     assert np.array_equal(env.get_field_raw(), before)  # tuning ran out of place
     assert env.get_tuning() == chosen
     for tma, warps, chunks in chosen:
-        assert tma in (0, 1) and 1 <= warps <= 4 and 1 <= chunks <= 16
+        assert tma in (0, 1, 2) and 1 <= warps <= 4 and 1 <= chunks <= 16
     assert np.all(ms > 0)
     env.simulate(P["dt"], STEPS, bfb.STEP_BULK | bfb.STEP_DIFFUSION | bfb.STEP_CELLS)
     assert np.array_equal(env.get_field(), want)
@@ -116,7 +117,7 @@ def test_autotune_large_fp32(bfb):
 
 
 @pytest.mark.parametrize("bad", [
-    [(2, 1, 4)] * 3,
+    [(3, 1, 4)] * 3,
     [(1, 0, 4)] * 3,
     [(1, 5, 4)] * 3,
     [(1, 1, 0)] * 3,
@@ -127,4 +128,39 @@ def test_set_tuning_rejects_bad_shapes(bfb, bad):
     with pytest.raises(bfb.BFBError):
         env.set_tuning(bad)
     assert env.get_tuning() == [(1, 1, 2)] * 3
+    env.close()
+
+
+# FP64 x/y sweeps with the lines' forward results in tensor memory: lines of
+# 16 to 256 rows, whole and partial 16-row groups and 8-row blocks, head rows
+# (factors that vary by row) and Dirichlet faces on either end; bit for bit
+# with the oracle, with the fused bulk update and per-face Dirichlet masks
+@pytest.mark.parametrize("shape,S", [((256, 10, 6), 3), ((6, 256, 10), 2), ((37, 45, 9), 3), ((250, 17, 4), 1),
+                                     ((16, 16, 16), 2), ((100, 100, 8), 4), ((23, 200, 5), 5)])
+def test_tensor_memory_tiles_fp64_bitexact(bfb, oracle, shape, S):
+    rng = np.random.default_rng(sum(shape) * 31 + S)
+    dt, dx = 0.01, 20.0
+    D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
+    rho0 = rng.random((*shape, S))
+    Sr, Tt, Ur = rng.random((3, *shape, S)) * 4.0
+    vals = rng.random((*shape, S)) * 30
+    act = (rng.random(S) < 0.8).astype(np.uint8)
+    fm = (rng.random((6, S)) < 0.6).astype(np.uint8)
+    env = bfb.Env(shape, S, dx=dx, precision=bfb.FP64)
+    env.set_tuning([(2, 1, 2), (2, 1, 2), (1, 1, 2)])
+    env.set_coefficients(D, lam)
+    env.set_field(rho0)
+    env.set_dirichlet(act, values=vals, face_mask=fm)
+    env.set_bulk(Sr, Tt, Ur)
+    env.simulate(dt, 3, bfb.STEP_BULK | bfb.STEP_DIFFUSION)
+    want = rho0
+    for _ in range(3):
+        want = oracle.bulk_step(want, dt, Sr, Tt, Ur)
+        want = oracle.lod_steps(want, dt, dx, D, lam, 1, vals, fm * act[None, :])
+    assert np.array_equal(env.get_field(), want)
+    # without the fused bulk update (the plain kernel instantiation)
+    env.set_field(rho0)
+    env.diffusion_step(dt, 2)
+    want = oracle.lod_steps(rho0, dt, dx, D, lam, 2, vals, fm * act[None, :])
+    assert np.array_equal(env.get_field(), want)
     env.close()
