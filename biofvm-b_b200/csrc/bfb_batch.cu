@@ -265,8 +265,12 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
 // tile code, as bfb_simulate's kernels do; the stages follow one another in
 // stream order, so no warp waits for another.
 constexpr int kPathTma = 0, kPathCp16 = 1, kPathCpElem = 2;
+// Register bound: the FP32 TMA sweep stages compile spill-free in 128
+// registers per thread (160 without the bound), so that one-warp CTAs of
+// small tiles fit 16 per SM instead of 12 (config 4, staged: 6.76 -> 6.32
+// ms per step); the other paths would spill under it and keep the default.
 template <typename T, int STAGE, int PATH>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, (sizeof(T) == 4 && PATH == kPathTma && STAGE < 3) ? 4 : 1)
     batch_stage_kernel(const BatchInst<T> *__restrict__ inst, const int *__restrict__ perm,
                        const int *__restrict__ tpre, int lo, int hi, int warp_bytes) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
