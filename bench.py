@@ -480,6 +480,14 @@ def run_our_arm(args):
         e1.record(stream)
         e1.synchronize()
         adj_ms[Kc] = slowest(e0.elapsed_time(e1))
+    # the same run when only dL/du0 is wanted: no D / lambda gradients, no per-line sums
+    env.set_field(rho0)
+    barrier()
+    e0.record(stream)
+    env.adjoint_run(DT, n_adj, w.data_ptr(), checkpoint_every=n_adj, coef_grads=False)
+    e1.record(stream)
+    e1.synchronize()
+    adj_field_ms = slowest(e0.elapsed_time(e1))
     env.close()
 
     # the uneven ensemble at N = 1: batched launches against the per-instance loop
@@ -569,6 +577,10 @@ def run_our_arm(args):
             "reverse_ms_per_step": adj_ms[n_adj] / n_adj - ms_step,
             "reverse_over_forward": (adj_ms[n_adj] / n_adj - ms_step) / ms_step,
             "run_over_forward": {f"checkpoint_every_{k}": v / n_adj / ms_step for k, v in adj_ms.items()},
+            "without_D_lambda_gradients": {
+                "run_ms_per_step": adj_field_ms / n_adj,
+                "reverse_over_forward": (adj_field_ms / n_adj - ms_step) / ms_step,
+                "run_over_forward": adj_field_ms / n_adj / ms_step},
         },
         "ensemble": ens,
     }

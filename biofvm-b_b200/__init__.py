@@ -389,22 +389,24 @@ class Env:
         return [tuple(v[3 * a:3 * a + 3]) for a in range(3)], ms
 
     def adjoint_run(self, dt, n_steps, dL_dfinal_ptr: int, flags=STEP_DIFFUSION, checkpoint_every=None,
-                    dL_dinitial_ptr: int = None, final_ptr: int = None, agent_grads=False):
+                    dL_dinitial_ptr: int = None, final_ptr: int = None, agent_grads=False, coef_grads=True):
         """Reverse mode of n_steps steps from the current field (bfb_adjoint_run).
 
         The pointers are device arrays of the env precision in the field layout.
-        Returns a dict of host gradients: D, lambda and, with agent_grads,
+        Returns a dict of host gradients: D and lambda (unless coef_grads is
+        False, which skips the sums they need) and, with agent_grads,
         secretion / uptake / saturation as [n_agents, S] arrays."""
         K = checkpoint_every or max(1, int(round(n_steps ** 0.5)))
-        gD, gL = np.zeros(self.S), np.zeros(self.S)
+        gD, gL = (np.zeros(self.S), np.zeros(self.S)) if coef_grads else (None, None)
         na = getattr(self, "n_agents", 0)
         ga = [np.zeros((na, self.S)) for _ in range(3)] if agent_grads else [None] * 3
         ap = [None if g is None else g.ctypes.data_as(_dp) for g in ga]
         _check(self.L.bfb_adjoint_run(self.h, dt, n_steps, flags, K, ctypes.c_void_p(dL_dfinal_ptr),
                                       None if dL_dinitial_ptr is None else ctypes.c_void_p(dL_dinitial_ptr),
                                       None if final_ptr is None else ctypes.c_void_p(final_ptr),
-                                      gD.ctypes.data_as(_dp), gL.ctypes.data_as(_dp), *ap))
-        out = {"D": gD, "lambda": gL}
+                                      None if gD is None else gD.ctypes.data_as(_dp),
+                                      None if gL is None else gL.ctypes.data_as(_dp), *ap))
+        out = {"D": gD, "lambda": gL} if coef_grads else {}
         if agent_grads:
             out.update(secretion=ga[0], uptake=ga[1], saturation=ga[2])
         return out

@@ -65,10 +65,11 @@ class _Simulate(torch.autograd.Function):
         torch.cuda.synchronize(rho0.device)
         env.set_field_device(rho0.data_ptr(), prec)
         want_agents = ctx.agents is not None and any(t is not None and t.requires_grad for t in (sec, upt, sat))
+        want_coef = ctx.needs_input_grad[6] or ctx.needs_input_grad[7]  # D, lam; else their sums are skipped
         r = env.adjoint_run(ctx.dt, ctx.n, g.data_ptr(), flags=ctx.flags, checkpoint_every=ctx.K,
-                            dL_dinitial_ptr=grad_rho0.data_ptr(), agent_grads=want_agents)
-        gD = torch.from_numpy(r["D"]).to(D.dtype)
-        gL = torch.from_numpy(r["lambda"]).to(lam.dtype)
+                            dL_dinitial_ptr=grad_rho0.data_ptr(), agent_grads=want_agents, coef_grads=want_coef)
+        gD = torch.from_numpy(r["D"]).to(D.dtype) if want_coef else None
+        gL = torch.from_numpy(r["lambda"]).to(lam.dtype) if want_coef else None
         gs = gu = gt = None
         if want_agents:
             gs = torch.from_numpy(r["secretion"]).to(sec.dtype)

@@ -902,6 +902,7 @@ struct Adjoint {
     const double *coef = nullptr;  // [2S]: c1, c2
     double *part_x = nullptr, *part_y = nullptr, *part_z = nullptr;
     long long tiles_z = 0;
+    bool sums = true;  // the per-line sums for dL/dD and dL/dlambda (skipped when neither is asked for)
 
     // tensor maps with the env's row-group counts (so the recompute runs the
     // env's tuned launch shape) and warp tiles of 32 lines (the adjoint
@@ -985,7 +986,7 @@ struct Adjoint {
                 if (wb <= (size_t)kMaxSmem) {
                     adjoint_solve_strided_tma_kernel<T><<<tiles, 32, wb, st>>>(lam.map[axis], mu.map[axis], a, g, crow);
                     BFB_CUDA(cudaGetLastError());
-                    return dots(axis, a, static_cast<const T *>(mu.p), yp, t);
+                    return sums ? dots(axis, a, static_cast<const T *>(mu.p), yp, t) : BFB_OK;
                 }
             }
             const size_t smem = 2 * (size_t)g.n * 32 * sizeof(T);
@@ -1005,7 +1006,7 @@ struct Adjoint {
             default: adjoint_solve_contig_pipe_kernel<T, 0><<<tiles, 32, wb, st>>>(a, gz, kc); break;
             }
             BFB_CUDA(cudaGetLastError());
-            return dots(2, a, static_cast<const T *>(mu.p), yp, t);
+            return sums ? dots(2, a, static_cast<const T *>(mu.p), yp, t) : BFB_OK;
         }
         const size_t smem = 2 * (size_t)gz.R * gz.RS * sizeof(T);
         if (smem > (size_t)kMaxSmem) return fail(BFB_ERR_UNSUPPORTED, "adjoint: rows too long for shared memory");
@@ -1028,6 +1029,7 @@ int adjoint_run(bfb_env_s *env, double dt, int n_steps, int flags, int K, const 
     A.env = env;
     A.dt = dt;
     A.st = st;
+    A.sums = gD || gL;
     A.S = S;
     int vb16[3];
     if ((rc = env_tile_plan(env, sizeof(T), env->nz * S, &A.gx, &A.gy, &A.gz, vb16))) return rc;

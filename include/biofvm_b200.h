@@ -316,7 +316,9 @@ BFB_API int bfb_batch_autotune(bfb_batch batch, double dt, int flags, int trials
  *   dL_dfinal     device, N elements of the env precision (required)
  *   dL_dinitial   device, N elements: dL/d(initial field)         (or NULL)
  *   final_field   device, N elements: the field after n_steps     (or NULL)
- *   dL_dD, dL_dlambda              host, [S] doubles              (or NULL)
+ *   dL_dD, dL_dlambda              host, [S] doubles              (or NULL;
+ *                 with both NULL the per-line sums they need are skipped,
+ *                 about half of the reverse pass's memory traffic)
  *   dL_dsecretion, dL_duptake, dL_dsaturation
  *                 host, [n_agents][S] doubles in bfb_set_agents' list order
  *                 (or NULL); inactive agents get 0. They need the rates of

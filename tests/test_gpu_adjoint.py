@@ -67,7 +67,7 @@ def _setup(bfb, prec, shape, S, rng, dirichlet=True, n_agents=0, dt=0.01, dx=20.
     return env, D, lam, rho0, (dvals, fm * act[None, :]), agents
 
 
-def _gpu_adjoint(bfb, env, rho0, w, n_steps, dt, K, agents, prec=None):
+def _gpu_adjoint(bfb, env, rho0, w, n_steps, dt, K, agents, prec=None, coef_grads=True):
     prec = env.precision if prec is None else prec
     env.set_field(rho0)
     wt = _dev_tensor(w, prec, bfb)
@@ -76,7 +76,7 @@ def _gpu_adjoint(bfb, env, rho0, w, n_steps, dt, K, agents, prec=None):
     flags = bfb.STEP_DIFFUSION | (bfb.STEP_CELLS if agents is not None else 0)
     torch.cuda.synchronize()
     r = env.adjoint_run(dt, n_steps, wt.data_ptr(), flags=flags, checkpoint_every=K, dL_dinitial_ptr=gi.data_ptr(),
-                        final_ptr=fin.data_ptr(), agent_grads=agents is not None)
+                        final_ptr=fin.data_ptr(), agent_grads=agents is not None, coef_grads=coef_grads)
     r["initial"] = gi.double().cpu().numpy()
     r["final"] = fin.double().cpu().numpy()
     return r
@@ -121,6 +121,21 @@ def test_adjoint_is_deterministic(bfb):
     for k in ("initial", "D", "lambda", "secretion", "uptake", "saturation"):
         assert np.array_equal(a[k], b[k]), k
     env.close()
+
+
+def test_adjoint_without_coefficient_gradients(bfb):
+    """With dL/dD and dL/dlambda not asked for (NULL), the reverse pass skips
+    their per-line sums; every other gradient is bit for bit the same."""
+    rng = np.random.default_rng(19)
+    for prec in (bfb.FP64, bfb.FP32):
+        env, D, lam, rho0, dirv, ag = _setup(bfb, prec, (40, 36, 44), 3, rng, n_agents=300)
+        w = rng.standard_normal(rho0.shape)
+        full = _gpu_adjoint(bfb, env, rho0, w, 6, 0.01, 4, ag)
+        part = _gpu_adjoint(bfb, env, rho0, w, 6, 0.01, 4, ag, coef_grads=False)
+        assert "D" not in part and "lambda" not in part
+        for k in ("final", "initial", "secretion", "uptake", "saturation"):
+            assert np.array_equal(full[k], part[k]), k
+        env.close()
 
 
 def _field_fd(bfb, env, rho0, n_steps, dt, flags):
