@@ -145,8 +145,12 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 1) sweep_contig_pipe
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
-    if (tile * g.R >= g.nrows) return;
+    // tiles from the last rows to the first: the y sweep before this one ends
+    // on the last (i, j) rows, whose lines are then still in L2
+    const long long ntiles = (g.nrows + g.R - 1) / g.R;
+    const long long slot = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (slot >= ntiles) return;
+    const long long tile = ntiles - 1 - slot;
     const size_t wbytes = (128 + (size_t)g.R * g.RS * sizeof(T) + 127) / 128 * 128;
     unsigned char *wbase = smem_raw + (size_t)warp * wbytes;
     if (lane == 0) {
