@@ -267,8 +267,9 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
 constexpr int kPathTma = 0, kPathCp16 = 1, kPathCpElem = 2;
 // Register bound: the FP32 TMA sweep stages compile spill-free in 128
 // registers per thread (160 without the bound), so that one-warp CTAs of
-// small tiles fit 16 per SM instead of 12 (config 4, staged: 6.76 -> 6.32
-// ms per step); the other paths would spill under it and keep the default.
+// small tiles fit 16 per SM instead of 12 (256 uneven grids of edges 32-160,
+// staged: 6.76 -> 6.32 ms per step); the other paths would spill under it and
+// keep the default.
 template <typename T, int STAGE, int PATH>
 __global__ void __launch_bounds__(128, (sizeof(T) == 4 && PATH == kPathTma && STAGE < 3) ? 4 : 1)
     batch_stage_kernel(const BatchInst<T> *__restrict__ inst, const int *__restrict__ perm,

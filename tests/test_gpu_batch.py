@@ -22,7 +22,7 @@ def make_instance(bfb, rng, edge_lo, edge_hi, n_agents_max, prec, dt):
     D, lam = log_uniform(rng, 1e2, 1e5, S), log_uniform(rng, 1e-3, 1.0, S)
     rho0 = rng.random((*shape, S))
     fm = np.zeros((6, S), np.uint8)
-    fm[0, 0] = fm[1, 0] = 1  # config-2 style: 38.0 on the x-faces, substrate 0
+    fm[0, 0] = fm[1, 0] = 1  # 38.0 on the x-faces for substrate 0, as the 200^3 agents workload has
     act = np.zeros(S, np.uint8)
     act[0] = 1
     na = int(rng.integers(0, n_agents_max + 1))

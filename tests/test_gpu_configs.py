@@ -1,9 +1,9 @@
 """The named workloads at their full sizes.
 
 FP64 is pinned bit-exact to the oracle at reduced sizes (test_gpu_parity.py
-and the reduced config-2 case here); at full size the FP64 GPU path is the
-FP64 reference, and the FP32 path's relative L-inf / L2 error against it is
-measured on the device and stated after each config's step count.
+and the reduced 200^3-with-agents case here); at full size the FP64 GPU path
+is the FP64 reference, and the FP32 path's relative L-inf / L2 error against
+it is measured on the device and stated after each workload's step count.
 """
 from __future__ import annotations
 

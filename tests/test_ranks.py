@@ -35,7 +35,7 @@ def load_bench():
 
 
 def ensemble_weights(seed=4, n=256):
-    """Field bytes of a config-4-like ensemble: edges U{32..160} per axis, 1-6 substrates, FP32."""
+    """Field bytes of an uneven ensemble of 256 grids: edges U{32..160} per axis, 1-6 substrates, FP32."""
     rng = np.random.default_rng(seed)
     ranks = load_ranks()
     return [ranks.instance_bytes(rng.integers(32, 161, 3), int(rng.integers(1, 7)), 4) for _ in range(n)]
