@@ -138,9 +138,12 @@ __device__ void cells_chunk(const BatchInst<T> &I, int chunk) {
 }
 
 // __launch_bounds__(128, 1): without the minimum-blocks hint the compiler
-// holds this kernel (every tile variant inlined) to 80 registers and spills.
-template <typename T>
-__global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
+// holds this kernel (every tile variant inlined) to 80 registers and spills;
+// with it, it takes 222 (FP32), so one-warp CTAs fit 9 per SM. TMA_ONLY
+// leaves out the cp.async tiles, for batches whose every env takes the TMA
+// tiles: FP32 then compiles spill-free in 128 registers (16 per SM).
+template <typename T, bool TMA_ONLY>
+__global__ void __launch_bounds__(128, (TMA_ONLY && sizeof(T) == 4) ? 4 : 1) batch_step_kernel(BatchParams<T> p) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -229,15 +232,17 @@ __global__ void __launch_bounds__(128, 1) batch_step_kernel(BatchParams<T> p) {
                     }
                     phase ^= (1u << ((I.gz.nz + I.kc - 1) / I.kc)) - 1u;
                     groups += (I.gz.nz + I.kc - 1) / I.kc;
-                } else if (stage == 0) {
-                    if (I.vb16[0]) strided_tile<T, 16, true, false>(I.ax[0], I.gx, tile, sm);
-                    else strided_tile<T, (int)sizeof(T), true, false>(I.ax[0], I.gx, tile, sm);
-                } else if (stage == 1) {
-                    if (I.vb16[1]) strided_tile<T, 16, false, false>(I.ax[1], I.gy, tile, sm);
-                    else strided_tile<T, (int)sizeof(T), false, false>(I.ax[1], I.gy, tile, sm);
-                } else {
-                    if (I.vb16[2]) contig_tile_any<T, 16>(I.ax[2], I.gz, tile, sm);
-                    else contig_tile_any<T, (int)sizeof(T)>(I.ax[2], I.gz, tile, sm);
+                } else if constexpr (!TMA_ONLY) {
+                    if (stage == 0) {
+                        if (I.vb16[0]) strided_tile<T, 16, true, false>(I.ax[0], I.gx, tile, sm);
+                        else strided_tile<T, (int)sizeof(T), true, false>(I.ax[0], I.gx, tile, sm);
+                    } else if (stage == 1) {
+                        if (I.vb16[1]) strided_tile<T, 16, false, false>(I.ax[1], I.gy, tile, sm);
+                        else strided_tile<T, (int)sizeof(T), false, false>(I.ax[1], I.gy, tile, sm);
+                    } else {
+                        if (I.vb16[2]) contig_tile_any<T, 16>(I.ax[2], I.gz, tile, sm);
+                        else contig_tile_any<T, (int)sizeof(T)>(I.ax[2], I.gz, tile, sm);
+                    }
                 }
                 __syncwarp();  // the tile's shared memory is reused by the next tile
             }
@@ -347,6 +352,7 @@ struct bfb_batch_s {
     int tiles_per_item = 2;
     int mode = BFB_BATCH_MODE_STAGED;
     int grid[5] = {0, 0, 0, 0, 0};  // resident CTAs for warps = 1..4
+    bool tma_only = false;          // every env's x, y and z stages take TMA tiles
     // staged mode, per stage s: envs listed by tile size (d_perm[s]), tiles before
     // list entry j (d_tpre[s][j]), and classes of list entries [lo, hi) launched
     // together with `bytes` of shared memory per warp
@@ -527,7 +533,11 @@ static int batch_upload(bfb_batch_s *b, double dt) {
     BFB_CUDA(cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice));
     BFB_CUDA(cudaMemcpy(b->d_tpre, tpre.data(), sizeof(int) * tpre.size(), cudaMemcpyHostToDevice));
     BFB_CUDA(cudaMemcpy(b->d_perm, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice));
-    BFB_CUDA(cudaFuncSetAttribute(batch_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    b->tma_only = true;
+    for (int k = 0; k < b->n; ++k) b->tma_only = b->tma_only && inst[k].tma[0] && inst[k].tma[1] && inst[k].tma[2];
+    const void *step_kernel = b->tma_only ? (const void *)batch_step_kernel<T, true>
+                                          : (const void *)batch_step_kernel<T, false>;
+    BFB_CUDA(cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
     for (const void *k :
          {(const void *)batch_stage_kernel<T, 0, kPathTma>, (const void *)batch_stage_kernel<T, 0, kPathCp16>,
           (const void *)batch_stage_kernel<T, 0, kPathCpElem>, (const void *)batch_stage_kernel<T, 1, kPathTma>,
@@ -544,7 +554,7 @@ static int batch_upload(bfb_batch_s *b, double dt) {
             b->grid[w] = 0;
             continue;
         }
-        BFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel<T>, 32 * w, bytes));
+        BFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel, 32 * w, bytes));
         b->grid[w] = per_sm * sms;
     }
     return BFB_OK;
@@ -637,7 +647,10 @@ static int batch_launch(bfb_batch_s *b, int flags, cudaStream_t s) {
     while (w > 1 && b->grid[w] == 0) --w;  // the widest CTA that fits
     const size_t bytes = (size_t)w * b->warp_bytes;
     const int grid = std::max(1, b->grid[w]);
-    batch_step_kernel<T><<<grid, 32 * w, bytes, s>>>(p);
+    if (b->tma_only)
+        batch_step_kernel<T, true><<<grid, 32 * w, bytes, s>>>(p);
+    else
+        batch_step_kernel<T, false><<<grid, 32 * w, bytes, s>>>(p);
     BFB_CUDA(cudaGetLastError());
     return BFB_OK;
 }
