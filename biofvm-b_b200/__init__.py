@@ -60,7 +60,8 @@ EXPORTS = [
     "bfb_checksum", "bfb_compute_gradients", "bfb_get_gradients", "bfb_write_matlab", "bfb_set_tuning", "bfb_get_tuning", "bfb_autotune", "bfb_batch_create", "bfb_batch_destroy", "bfb_batch_set_option", "bfb_batch_get_option", "bfb_batch_simulate",
     "bfb_batch_simulate_loop", "bfb_batch_synchronize", "bfb_batch_autotune", "bfb_adjoint_run",
     "bfb_checksum_noalloc", "bfb_watchdog_selftest", "bfb_host_register", "bfb_host_unregister",
-    "bfb_batch_set_stream",
+    "bfb_batch_set_stream", "bfb_create_slab", "bfb_slab_info", "bfb_slab_x_forward", "bfb_slab_x_backward",
+    "bfb_slab_yz",
 ]
 
 
@@ -140,6 +141,12 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         "bfb_batch_autotune": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp],
         "bfb_adjoint_run": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _dp, _dp,
                             _dp, _dp, _dp],
+        "bfb_create_slab": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                            ctypes.c_int, ctypes.c_double, ctypes.c_int],
+        "bfb_slab_info": [_vp, _ip, _ip, ctypes.POINTER(ctypes.c_longlong)],
+        "bfb_slab_x_forward": [_vp, ctypes.c_double, _vp, _vp, ctypes.c_longlong, ctypes.c_longlong],
+        "bfb_slab_x_backward": [_vp, ctypes.c_double, _vp, _vp, ctypes.c_longlong, ctypes.c_longlong],
+        "bfb_slab_yz": [_vp, ctypes.c_double],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -410,6 +417,49 @@ class Env:
         if agent_grads:
             out.update(secretion=ga[0], uptake=ga[1], saturation=ga[2])
         return out
+
+
+class SlabEnv(Env):
+    """Planes [x0, x0 + nx_local) of a grid of nx_global x planes, FP64: one
+    rank's share of an x-slab decomposition (``bfb_create_slab``; the reference
+    splits x over MPI ranks, BioFVM_parallel.cpp:108-144). Its x lines continue
+    in the neighbouring slabs; ``slabs.step`` runs the pipelined exchange."""
+
+    def __init__(self, nx_global, x0, nx_local, ny, nz, n_substrates, dx=20.0, device=0):
+        L = load_library()
+        h = _vp()
+        _check(L.bfb_create_slab(ctypes.byref(h), nx_global, x0, nx_local, ny, nz, n_substrates, dx, device))
+        self.h = h
+        self.L = L
+        self.nx, self.ny, self.nz, self.S = nx_local, ny, nz, n_substrates
+        self.precision = FP64
+        self.dx = dx
+        g, x, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        _check(L.bfb_slab_info(h, ctypes.byref(g), ctypes.byref(x), ctypes.byref(n)))
+        self.nx_global, self.x0, self.lines = g.value, x.value, n.value
+
+    @property
+    def first(self):
+        return self.x0 == 0
+
+    @property
+    def last(self):
+        return self.x0 + self.nx == self.nx_global
+
+    def x_forward(self, dt, prev_in_ptr: int, prev_out_ptr: int, line0=0, line1=None):
+        """Forward half of the x sweep over lines [line0, line1): device arrays of
+        ``lines`` doubles (0 for none)."""
+        line1 = self.lines if line1 is None else line1
+        _check(self.L.bfb_slab_x_forward(self.h, dt, ctypes.c_void_p(prev_in_ptr or None),
+                                         ctypes.c_void_p(prev_out_ptr or None), line0, line1))
+
+    def x_backward(self, dt, next_in_ptr: int, next_out_ptr: int, line0=0, line1=None):
+        line1 = self.lines if line1 is None else line1
+        _check(self.L.bfb_slab_x_backward(self.h, dt, ctypes.c_void_p(next_in_ptr or None),
+                                          ctypes.c_void_p(next_out_ptr or None), line0, line1))
+
+    def yz(self, dt):
+        _check(self.L.bfb_slab_yz(self.h, dt))
 
 
 class Batch:

@@ -20,7 +20,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libbiofvm_b200.so"
-SOURCES = ["bfb_capi.cu", "bfb_sweeps.cu", "bfb_tma.cu", "bfb_aux.cu", "bfb_batch.cu", "bfb_noalloc.cu", "bfb_adjoint.cu", "bfb_gradient.cu", "bfb_matlab.cu", "bfb_tmem.cu"]
+SOURCES = ["bfb_capi.cu", "bfb_sweeps.cu", "bfb_tma.cu", "bfb_aux.cu", "bfb_batch.cu", "bfb_noalloc.cu", "bfb_adjoint.cu", "bfb_gradient.cu", "bfb_matlab.cu", "bfb_tmem.cu", "bfb_slab.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",

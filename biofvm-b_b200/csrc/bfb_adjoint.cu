@@ -1268,6 +1268,7 @@ extern "C" BFB_API int bfb_adjoint_run(bfb_env env, double dt, int n_steps, int 
                                        double *dL_dlambda, double *dL_dsecretion, double *dL_duptake,
                                        double *dL_dsaturation) {
     if (!env) return fail(BFB_ERR_INVALID_ARG, "null bfb_env");
+    if (env->nx_global) return fail(BFB_ERR_UNSUPPORTED, "reverse mode runs on whole grids, not x-slab envs");
     if (n_steps < 1 || checkpoint_every < 1 || !(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "bad dt, n_steps or K");
     NvtxRange range("bfb_adjoint_run");
     if (!dL_dfinal) return fail(BFB_ERR_INVALID_ARG, "dL_dfinal is NULL");

@@ -167,7 +167,7 @@ static int upload_factors(bfb_env_s *env, int axis, int n, const std::vector<dou
 
 static int ensure_factors(bfb_env_s *env, double dt) {
     if (env->factors_valid && (env->freeze_factors || env->factor_dt == dt)) return BFB_OK;
-    const int ns[3] = {env->nx, env->ny, env->nz};
+    const int ns[3] = {env->nx_global ? env->nx_global : env->nx, env->ny, env->nz};  // a slab: the whole x line
     std::vector<double> den, c, c1;
     // the factor tables are only read by kernels on env->stream
     BFB_CUDA(cudaStreamSynchronize(env->stream));
@@ -204,7 +204,7 @@ static SweepArgs<T> make_args(bfb_env_s *env, int axis, bool bulk, double dt) {
     a.nz = env->nz;
     a.S = env->S;
     a.Lp = env->Lp;
-    const int ns[3] = {env->nx, env->ny, env->nz};
+    const int ns[3] = {env->nx_global ? env->nx_global : env->nx, env->ny, env->nz};
     const size_t nS = (size_t)ns[axis] * env->S;
     const T *tab = static_cast<const T *>(env->fac_tab[axis]);
     a.fac.t0 = tab;
@@ -266,8 +266,15 @@ static int launch_strided_env(bfb_env_s *env, int axis, bool bulk, double dt, cu
                              env->tma_crow[axis], env->tma_lines[axis], s);
 }
 
+static int refuse_slab(const bfb_env_s *env) {
+    return env->nx_global ? fail(BFB_ERR_UNSUPPORTED, "an x-slab env sweeps x through bfb_slab_x_forward and "
+                                                      "bfb_slab_x_backward")
+                          : BFB_OK;
+}
+
 template <typename T>
 static int run_diffusion(bfb_env_s *env, double dt, bool bulk, cudaStream_t s) {
+    if (int st = refuse_slab(env)) return st;
     int st = launch_strided_env<T>(env, 0, bulk, dt, s);
     if (st) return st;
     st = launch_strided_env<T>(env, 1, false, dt, s);
@@ -302,6 +309,7 @@ static int run_steps_any(bfb_env_s *env, double dt, int n, int flags, cudaStream
 // needs, and the per-axis kernel arguments and tile geometry.
 int env_prepare_step(bfb_env_s *env, double dt, int flags) {
     BFB_CUDA(cudaSetDevice(env->device));
+    if (int st = refuse_slab(env)) return st;
     if (flags & BFB_STEP_DIFFUSION) return ensure_factors(env, dt);
     return BFB_OK;
 }
@@ -743,6 +751,9 @@ static int dirichlet_install(bfb_env_s *env, const std::vector<double> *faces_ho
         for (int d = 0; d < S; ++d) {
             const uint8_t base = face_mask ? face_mask[f * S + d] : 1;
             env->face_mask[f * S + d] = (base && env->activation[d]) ? 1 : 0;
+            // a slab holds the grid's x faces only at its ends of the grid
+            if (env->nx_global && ((f == 0 && env->x0 != 0) || (f == 1 && env->x0 + env->nx != env->nx_global)))
+                env->face_mask[f * S + d] = 0;
         }
     std::vector<uint8_t> bits(S, 0);
     int any = 0;
@@ -921,8 +932,10 @@ BFB_API int bfb_simulate(bfb_env env, double dt, int n_steps, int flags) {
     if (n_steps < 0) return fail(BFB_ERR_INVALID_ARG, "n_steps < 0");
     if (!(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0");
     if (flags & ~(BFB_STEP_BULK | BFB_STEP_DIFFUSION | BFB_STEP_CELLS)) return fail(BFB_ERR_INVALID_ARG, "bad flags");
-    if (flags & BFB_STEP_DIFFUSION)
+    if (flags & BFB_STEP_DIFFUSION) {
+        if ((st = refuse_slab(env))) return st;
         if ((st = ensure_factors(env, dt))) return st;
+    }
     if (n_steps == 0) return BFB_OK;
     NvtxRange range("bfb_simulate");
     if (!env->use_graphs || env->stream == nullptr) return run_steps_any(env, dt, n_steps, flags, env->stream);
@@ -956,6 +969,7 @@ BFB_API int bfb_step_host(bfb_env env, double *host_field, double dt, int n_step
     int st = check_env(env);
     if (st) return st;
     if (!host_field) return fail(BFB_ERR_INVALID_ARG, "host_field is NULL");
+    if ((st = refuse_slab(env))) return st;
     if ((st = ensure_factors(env, dt))) return st;
     NvtxRange range("bfb_step_host");
     cudaStream_t s = env->stream;
@@ -1093,6 +1107,7 @@ BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double
     int st = check_env(env);
     if (st) return st;
     if (!(dt > 0) || trials < 1) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0 and trials >= 1");
+    if ((st = refuse_slab(env))) return st;
     if ((st = ensure_factors(env, dt))) return st;
     BFB_CUDA(cudaStreamSynchronize(env->stream));
     void *scratch = nullptr;
@@ -1114,6 +1129,7 @@ BFB_API int bfb_autotune(bfb_env env, double dt, int trials, int *chosen, double
 BFB_API int bfb_profile_steps(bfb_env env, double dt, int n_steps, int flags, double *ms_out) {
     int st = check_env(env);
     if (st) return st;
+    if ((st = refuse_slab(env))) return st;
     if (!ms_out || n_steps < 1) return fail(BFB_ERR_INVALID_ARG, "ms_out NULL or n_steps < 1");
     if (!(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0");
     if (flags & BFB_STEP_DIFFUSION)
@@ -1180,3 +1196,88 @@ BFB_API int bfb_checksum(bfb_env env, double *out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// x-slab decomposition (BioFVM_parallel.cpp:108-144 splits the x planes over
+// ranks; :832-873 and :948-1255 pipeline the x lines' Thomas solve across
+// them). A slab env is an ordinary env of nx_local planes whose x factor
+// tables are those of the whole line of nx_global planes; its x sweep runs in
+// the two halves below, the y and z sweeps are its own.
+// ---------------------------------------------------------------------------
+BFB_API int bfb_create_slab(bfb_env *out, int nx_global, int x0, int nx_local, int ny, int nz, int n_substrates,
+                            double dx, int device) {
+    if (!out) return fail(BFB_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (nx_global < 2 || x0 < 0 || nx_local < 1 || (long long)x0 + nx_local > nx_global)
+        return fail(BFB_ERR_SIZE, "a slab needs nx_global >= 2 and 0 <= x0 < x0 + nx_local <= nx_global");
+    int st = bfb_create(out, nx_local, ny, nz, n_substrates, dx, BFB_FP64, device);
+    if (st) return st;
+    bfb_env_s *env = *out;
+    env->nx_global = nx_global;
+    env->x0 = x0;
+    env->bbox[0] = x0 * dx;
+    env->bbox[3] = (x0 + nx_local) * dx;
+    // the x factor tables hold the whole line
+    cudaFree(env->fac_tab[0]);
+    cudaFree(env->fac_head[0]);
+    env->fac_tab[0] = env->fac_head[0] = nullptr;
+    cudaError_t e = cudaMalloc(&env->fac_tab[0], env->elem * 4 * (size_t)nx_global * n_substrates);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&env->fac_head[0], env->elem * 4 * (size_t)n_substrates * ((nx_global + 3) / 4 * 4));
+    if (e != cudaSuccess) {
+        bfb_destroy(env);
+        *out = nullptr;
+        return cuda_fail(e, "cudaMalloc");
+    }
+    return BFB_OK;
+}
+
+BFB_API int bfb_slab_info(bfb_env env, int *nx_global, int *x0, long long *lines) {
+    int st = check_env(env);
+    if (st) return st;
+    if (nx_global) *nx_global = env->nx_global ? env->nx_global : env->nx;
+    if (x0) *x0 = env->x0;
+    if (lines) *lines = (long long)env->ny * env->Lp;
+    return BFB_OK;
+}
+
+static int slab_half_args(bfb_env_s *env, double dt, long long line0, long long line1) {
+    if (!env->nx_global) return fail(BFB_ERR_STATE, "not an x-slab env (bfb_create_slab)");
+    if (!(dt > 0)) return fail(BFB_ERR_INVALID_ARG, "dt must be > 0");
+    if (line0 < 0 || line1 < line0 || line1 > (long long)env->ny * env->Lp)
+        return fail(BFB_ERR_INVALID_ARG, "line range outside [0, ny * pitch]");
+    return ensure_factors(env, dt);
+}
+
+BFB_API int bfb_slab_x_forward(bfb_env env, double dt, const double *prev_in, double *prev_out, long long line0,
+                               long long line1) {
+    int st = check_env(env);
+    if (st) return st;
+    if ((st = slab_half_args(env, dt, line0, line1))) return st;
+    if (env->x0 > 0 && !prev_in) return fail(BFB_ERR_INVALID_ARG, "prev_in is NULL past the grid's first plane");
+    NvtxRange range("bfb_slab_x_forward");
+    return launch_slab_x_forward(make_args<double>(env, 0, false, dt), env->x0, env->nx_global, line0, line1,
+                                 env->x0 > 0 ? prev_in : nullptr, prev_out, env->stream);
+}
+
+BFB_API int bfb_slab_x_backward(bfb_env env, double dt, const double *next_in, double *next_out, long long line0,
+                                long long line1) {
+    int st = check_env(env);
+    if (st) return st;
+    if ((st = slab_half_args(env, dt, line0, line1))) return st;
+    const bool last = env->x0 + env->nx == env->nx_global;
+    if (!last && !next_in) return fail(BFB_ERR_INVALID_ARG, "next_in is NULL before the grid's last plane");
+    NvtxRange range("bfb_slab_x_backward");
+    return launch_slab_x_backward(make_args<double>(env, 0, false, dt), env->x0, env->nx_global, line0, line1,
+                                  last ? nullptr : next_in, next_out, env->stream);
+}
+
+BFB_API int bfb_slab_yz(bfb_env env, double dt) {
+    int st = check_env(env);
+    if (st) return st;
+    if ((st = slab_half_args(env, dt, 0, 0))) return st;
+    NvtxRange range("bfb_slab_yz");
+    if ((st = launch_strided_env<double>(env, 1, false, dt, env->stream))) return st;
+    return launch_contig<double>(make_args<double>(env, 2, false, dt), env->tuning.warps[2],
+                                 env->use_tma != 0 && env->tuning.tma[2] != 0, env->stream, env->tuning.chunks[2]);
+}

@@ -178,6 +178,11 @@ struct bfb_env_s {
     // sticky device error flag (a bounded wait in a kernel ran out)
     int *d_err = nullptr;
 
+    // x-slab of a larger grid (bfb_create_slab): planes [x0, x0 + nx) of
+    // nx_global; 0 for a whole grid
+    int nx_global = 0;
+    int x0 = 0;
+
     // reverse-mode workspace (bfb_adjoint.cu): one device block, kept between
     // calls and grown on demand, freed by bfb_destroy
     void *adj_ws = nullptr;

@@ -168,6 +168,18 @@ bool make_tmem_sweep_map(CUtensorMap *out, void *field, int axis, int nx, int ny
 int launch_strided_tmem(const SweepArgs<double> &a, const StridedGeom &g, const CUtensorMap *map,
                         const CUtensorMap *map_out, bool fuse_pre, cudaStream_t s);
 void tmem_prepare_device();
+// The x sweep of an x-slab of a larger grid in two halves (bfb_slab.cu, FP64):
+// the forward half over lines [line0, line1) of the slab's ny*Lp columns,
+// starting from prev_in[line] (the previous slab's last forward value; NULL
+// for the grid's first slab) and giving its own last one in prev_out (may be
+// NULL); the backward half starting from next_in[line] (the next slab's first
+// back-substituted value; NULL for the grid's last slab) and giving its own
+// in next_out (may be NULL). a.nx is the slab's plane count and the factor
+// tables are the whole line's; x0 is the slab's first plane of nglob.
+int launch_slab_x_forward(const SweepArgs<double> &a, int x0, int nglob, long long line0, long long line1,
+                          const double *prev_in, double *prev_out, cudaStream_t s);
+int launch_slab_x_backward(const SweepArgs<double> &a, int x0, int nglob, long long line0, long long line1,
+                           const double *next_in, double *next_out, cudaStream_t s);
 // The strided geometry of a sweep over args a (axis 0: x, 1: y), 32-line tiles.
 template <typename T>
 inline StridedGeom strided_geometry(const SweepArgs<T> &a, int axis) {

@@ -358,6 +358,38 @@ BFB_API int bfb_adjoint_run(bfb_env env, double dt, int n_steps, int flags, int 
 BFB_API int bfb_checksum_noalloc(const void *field_dev, int precision, long long n_voxels, int n_substrates,
                                  double *out_dev, void *stream);
 
+/* ---- x-slab decomposition of one grid over ranks (FP64) -------------------
+ * Replaces the reference's MPI split of the x planes (BioFVM_parallel.cpp:
+ * 108-144, local counts x_nodes/dims[1]) and its pipelined cross-rank x solve
+ * (BioFVM_parallel.cpp:948-1255 with the sends and receives of :832-873). A
+ * slab env holds planes [x0, x0 + nx_local) of a grid of nx_global planes,
+ * one rank (GPU) each; it is an ordinary env (field, Dirichlet, bulk, agents
+ * of its own voxels; its domain box starts at x0*dx) whose x lines continue
+ * in the neighbouring slabs. Its Dirichlet x faces are active only where the
+ * slab holds the grid's face (x0 == 0 for the low face, x0 + nx_local ==
+ * nx_global for the high one). A step is, per rank:
+ *   bfb_slab_x_forward over line ranges, each after receiving prev_in for
+ *     that range from the previous rank and followed by sending prev_out to
+ *     the next;
+ *   bfb_slab_x_backward over the ranges, each after receiving next_in from
+ *     the next rank and followed by sending next_out to the previous;
+ *   bfb_slab_yz.
+ * Lines are the slab's columns, `lines` (bfb_slab_info) = ny * bfb_field_pitch
+ * of them; prev_* / next_* are device arrays of `lines` doubles indexed by
+ * line, of which [line0, line1) are read or written. prev_in is ignored on
+ * the first slab and next_in on the last; prev_out / next_out may be NULL.
+ * The slabs together give the whole grid's step bit for bit. bfb_simulate,
+ * bfb_profile_steps, bfb_autotune, bfb_adjoint_run and batches refuse slab
+ * envs (BFB_ERR_UNSUPPORTED). Work is queued on the env's stream. */
+BFB_API int bfb_create_slab(bfb_env *out, int nx_global, int x0, int nx_local, int ny, int nz, int n_substrates,
+                            double dx, int device);
+BFB_API int bfb_slab_info(bfb_env env, int *nx_global, int *x0, long long *lines);
+BFB_API int bfb_slab_x_forward(bfb_env env, double dt, const double *prev_in, double *prev_out, long long line0,
+                               long long line1);
+BFB_API int bfb_slab_x_backward(bfb_env env, double dt, const double *next_in, double *next_out, long long line0,
+                                long long line1);
+BFB_API int bfb_slab_yz(bfb_env env, double dt);
+
 #ifdef __cplusplus
 }
 #endif
