@@ -692,6 +692,82 @@ def run_ensemble_arm(args):
     return 0
 
 
+def run_slabs_arm(args):
+    """One FP64 grid split into x slabs over the ranks (the reference's MPI
+    decomposition, BioFVM_parallel.cpp:108-144): each rank holds one slab
+    env, the x lines are solved with the pipelined exchange of boundary
+    planes (slabs.step; NCCL send/recv between neighbouring ranks), the y and
+    z sweeps are local. value = the grid's voxel*substrate updates per step /
+    the slowest rank's step time."""
+    import torch
+    rank, world, local = dist_setup(args)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    bfb = load_bfb()
+    slabs = importlib.import_module("biofvm_b_b200.slabs")
+    x0, m = slabs.split_planes(NX, world)[rank]
+    D, lam, _ = coefficients()
+    field = np.random.default_rng(SEED + 1 + rank).random((m, NY, NZ, S))
+    slab = bfb.SlabEnv(NX, x0, m, NY, NZ, S, dx=DX, device=local)
+    slab.set_coefficients(D, lam)
+    slab.set_field(field)
+    stream = torch.cuda.Stream(device=dev)
+    slab.set_stream(stream.cuda_stream)
+    planes = {k: torch.zeros(slab.lines, dtype=torch.float64, device=dev) for k in slabs.PLANES}
+
+    class Planes:
+        def ptr(self, name):
+            return planes[name].data_ptr()
+
+    class Nccl:  # point-to-point messages on the slab's stream
+        def send(self, name, l0, l1, peer):
+            dist.send(planes[name][l0:l1], dst=peer)
+
+        def recv(self, name, l0, l1, peer):
+            dist.recv(planes[name][l0:l1], src=peer)
+
+    blocks = 8
+    warm, K = max(args.warmup, 3), max(1, min(args.steps, 200))
+    with torch.cuda.stream(stream):
+        for _ in range(warm):
+            slabs.step(slab, DT, rank, world, Planes(), Nccl(), blocks)
+        stream.synchronize()
+        rank_barrier(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            slabs.step(slab, DT, rank, world, Planes(), Nccl(), blocks)
+        e1.record(stream)
+        e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
+    total = sum_over_ranks(float(np.sum(slab.checksum())), dev)
+    slab.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    vs = NX * NY * NZ * S
+    line = {
+        "metric": f"voxel*substrate updates/s per LOD step ({NX}^3 voxels x {S} substrates, x slabs)",
+        "value": vs / (ms / K / 1e3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warm,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded U[0,1) field per slab, log-uniform D/lambda)",
+        "config": {"workload": f"LOD diffusion-decay step, {NX}^3 voxels x {S} substrates, dt={DT}, dx={DX}, "
+                               f"split into {world} x slab(s)",
+                   "l2": "inputs larger than L2", "parallelism": f"x slabs over {world} rank(s), {blocks} line blocks"},
+        "gpu_launches": None,
+        "checksum_of_checksums": total,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -706,8 +782,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (for profiler runs, whose timing would mislead the tuner)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the uneven-ensemble block of the default run")
-    ap.add_argument("--workload", default="grid", choices=["grid", "ensemble"],
-                    help="grid: the 256^3 x 8 step (replicas per GPU); ensemble: 256 uneven instances sharded over the GPUs")
+    ap.add_argument("--workload", default="grid", choices=["grid", "ensemble", "slabs"],
+                    help="grid: the 256^3 x 8 step (replicas per GPU); ensemble: 256 uneven instances sharded over "
+                         "the GPUs; slabs: one FP64 grid split into x slabs over the GPUs")
     args = ap.parse_args()
     global NX, NY, NZ, S
     NX = NY = NZ = args.grid
@@ -716,6 +793,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "ensemble":
         return run_ensemble_arm(args)
+    if args.workload == "slabs":
+        return run_slabs_arm(args)
     return run_our_arm(args)
 
 
