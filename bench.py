@@ -731,7 +731,7 @@ def run_slabs_arm(args):
         def recv(self, name, l0, l1, peer):
             dist.recv(planes[name][l0:l1], src=peer)
 
-    blocks = 8
+    blocks = 8 if world > 1 else 1  # blocks only pipeline the ranks
     warm, K = max(args.warmup, 3), max(1, min(args.steps, 200))
     with torch.cuda.stream(stream):
         for _ in range(warm):

@@ -22,6 +22,13 @@ namespace bfb {
 
 namespace {
 
+// Rows whose loads are in flight together, per half (measured at 256^3 x 8,
+// one slab: forward 4 rows 0.379 ms, 8 rows 0.747, 16 rows 0.881; backward
+// 16 rows 0.378 ms, 4 rows 0.436). The forward's four-operation chain per row
+// gains nothing from deeper blocks and loses occupancy to their registers.
+constexpr int kSlabFwdBlock = 4;
+constexpr int kSlabBwdBlock = 16;
+
 struct SlabColumn {
     int cj, ck, d;
     bool real;
@@ -63,7 +70,18 @@ __global__ void __launch_bounds__(256) slab_x_forward_kernel(SweepArgs<double> a
     } else {
         L.prev = prev_in[cl];
     }
-#pragma unroll 4
+    // rows in blocks: a block's loads are issued before its stores (a store
+    // may alias a later row, so the compiler keeps program order), so the
+    // loads of a block are in flight together
+    for (; r + kSlabFwdBlock <= nloc; r += kSlabFwdBlock) {
+        double v[kSlabFwdBlock];
+#pragma unroll
+        for (int u = 0; u < kSlabFwdBlock; ++u) v[u] = xin(r + u);
+#pragma unroll
+        for (int u = 0; u < kSlabFwdBlock; ++u) v[u] = L.fwd<false>(v[u], x0 + r + u);
+#pragma unroll
+        for (int u = 0; u < kSlabFwdBlock; ++u) f[(size_t)(r + u) * P] = v[u];
+    }
     for (; r < nloc; ++r) f[(size_t)r * P] = L.fwd<false>(xin(r), x0 + r);
     if (prev_out) prev_out[cl] = L.prev;
 }
@@ -94,12 +112,19 @@ __global__ void __launch_bounds__(256) slab_x_backward_kernel(SweepArgs<double> 
     } else {
         L.next = next_in[cl];
     }
-#pragma unroll 4
-    for (; r >= 0; --r) {
-        double y = L.bwd<false>(f[(size_t)r * P], x0 + r);
-        if ((lo_dir && x0 + r == 0) || col_dir) y = dir_value(a.dir, r, c.cj, c.ck, c.d);  // stored, not carried
-        f[(size_t)r * P] = y;
+    auto out = [&](int q, double y) -> double {  // the stored value; the recurrence carries y
+        return ((lo_dir && x0 + q == 0) || col_dir) ? dir_value(a.dir, q, c.cj, c.ck, c.d) : y;
+    };
+    for (; r - kSlabBwdBlock + 1 >= 0; r -= kSlabBwdBlock) {
+        double v[kSlabBwdBlock];
+#pragma unroll
+        for (int u = 0; u < kSlabBwdBlock; ++u) v[u] = f[(size_t)(r - u) * P];
+#pragma unroll
+        for (int u = 0; u < kSlabBwdBlock; ++u) v[u] = L.bwd<false>(v[u], x0 + r - u);
+#pragma unroll
+        for (int u = 0; u < kSlabBwdBlock; ++u) f[(size_t)(r - u) * P] = out(r - u, v[u]);
     }
+    for (; r >= 0; --r) f[(size_t)r * P] = out(r, L.bwd<false>(f[(size_t)r * P], x0 + r));
     if (next_out) next_out[cl] = L.next;
 }
 
