@@ -442,6 +442,28 @@ static int go_contig(const SweepArgs<T> &a, const ContigGeom &g, int warps, size
     return BFB_OK;
 }
 
+// Rows per bulk-copy z tile for FP64: a tile holds whole rows, so few tiles
+// fit an SM; where fewer rows per tile keep at least 1/16 more lines resident
+// per SM (one-warp CTAs; 228 KB of shared memory per SM, 1 KB reserved per
+// CTA), the tile takes that many. A stride free of bank conflicts for R rows
+// is free of them for fewer.
+static int z_rows_for_residency(int R, int RS, int S, int eb) {
+    const long long smem_sm = 228 * 1024, reserve = 1024;
+    auto lines = [&](int r) -> long long {
+        const long long wb = (128 + (long long)r * RS * eb + 127) / 128 * 128;
+        return smem_sm / (wb + reserve) * r * S;
+    };
+    const long long base = lines(R);
+    int best = R;
+    long long best_l = base;
+    for (int r = R - 1; r >= 1 && r * S >= 16; --r)  // at least half the warp busy
+        if (lines(r) > best_l) {
+            best_l = lines(r);
+            best = r;
+        }
+    return best_l >= base + base / 16 ? best : R;
+}
+
 template <typename T>
 int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s, int chunks) {
     ContigGeom g;
@@ -465,6 +487,7 @@ int launch_contig(const SweepArgs<T> &a, int warps, bool use_tma, cudaStream_t s
         // conflict-free stride where it is one, else contig_aligned_geom's
         ContigGeom gt = g;
         const bool ok = ((long long)g.RS * eb) % 16 == 0 || contig_aligned_geom(a.nz, a.S, a.Lp, eb, &gt.R, &gt.RS);
+        if (ok && eb == 8) gt.R = z_rows_for_residency(gt.R, gt.RS, a.S, eb);
         if (ok && (L * eb) * gt.R < (1 << 20)) {
             const int st = launch_contig_tma<T>(a, gt, warps, s, chunks);
             if (st != kNotApplicable) return st;
